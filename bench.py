@@ -1,0 +1,333 @@
+#!/usr/bin/env python
+"""Throughput of the B200 DirectSHT forward transform (points*ell/s).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2] [--impl ours|reference]
+
+A step is one forward transform (DirectSHT.__call__ semantics: polar rotation included)
+of one synthetic point set already resident in HBM.  The default workload is the
+survey-like single map: Nl=1024, Nx=2048, N=1e7 points with cos(theta) uniform in
+[cos 1.2, cos 0.3], phi uniform in [0, 1.5 pi), lognormal(0, 0.5) weights.  Under
+torchrun every rank transforms its own point set (independent requests, no collective on
+the data path); the timed region is bracketed by a barrier and a device synchronise and
+the slowest rank's time is reported.  Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as ct
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "c2": dict(Nl=1024, Nx=2048, N=10_000_000, kind="c2", wkind="lognormal",
+               name="survey-like single map: Nl=1024, Nx=2048, N=1e7, cos(theta)~U[cos1.2,cos0.3], "
+                    "phi~U[0,1.5pi), w~lognormal(0,0.5) f64"),
+    "c1": dict(Nl=256, Nx=512, N=100_000, kind="full", wkind="ones",
+               name="full sky: Nl=256, Nx=512, N=1e5, cos(theta)~U[-1,1], phi~U[0,2pi), w=1 f64"),
+}
+
+
+def make_points(spec, seed):
+    rng = np.random.default_rng(seed)
+    N = spec["N"]
+    if spec["kind"] == "c2":
+        cost = rng.uniform(np.cos(1.2), np.cos(0.3), N)
+        phi = rng.uniform(0.0, 1.5 * np.pi, N)
+    else:
+        cost = rng.uniform(-1.0, 1.0, N)
+        phi = rng.uniform(0.0, 2 * np.pi, N)
+    theta = np.arccos(cost)
+    if spec["wkind"] == "lognormal":
+        w = rng.lognormal(0.0, 0.5, N)
+    elif spec["wkind"] == "uniform":
+        w = rng.uniform(0.5, 1.5, N)
+    else:
+        w = np.ones(N)
+    return theta, phi, w
+
+
+# ---------------------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm), "power_w_max": max(power) if power else None}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+# ---------------------------------------------------------------------------------------
+def cpu_reference_run(spec, sample_n, steps, warmup, seed=0):
+    """The reference's own C/OpenMP transform (csht/sht_helper.c, built into oracle/_ref)
+    on a bounded sample of the workload's points.  The polar points are rotated before the
+    timed region and their alm rotated back after it (healpy's part in the reference)."""
+    from oracle import dsht_oracle as O
+    from oracle import ref_csht
+    if not ref_csht.available():
+        return None
+    th, ph, w = make_points(dict(spec, N=sample_n), seed + 1000)
+    t0 = time.time()
+    ref = ref_csht.RefCSHT(spec["Nl"], spec["Nx"])
+    t_tables = time.time() - t0
+    pol = np.abs(np.cos(th)) >= 0.75
+    tr, pr = O.rotate_points(th[pol], ph[pol])
+    equ = ~pol
+    times = []
+    for it in range(warmup + steps):
+        t0 = time.perf_counter()
+        ref.basic(tr, pr, w[pol])
+        ref.basic(th[equ], ph[equ], w[equ])
+        t1 = time.perf_counter()
+        if it >= warmup:
+            times.append(t1 - t0)
+    sec = float(np.mean(times))
+    return {"value": sample_n * spec["Nl"] / sec, "unit": "points*ell/s", "cores": os.cpu_count(),
+            "kind": "reference", "seconds_per_step": sec, "table_build_s": t_tables,
+            "sample": f"{sample_n} points of the same distribution through csht/sht_helper.c do_transform "
+                      f"(OpenMP, {os.cpu_count()} threads) at Nl={spec['Nl']}, Nx={spec['Nx']}; rotations untimed"}
+
+
+def run_reference_arm(args, spec):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+    r = cpu_reference_run(spec, args.ref_sample, args.steps, args.warmup)
+    if r is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/sht_helper.so (csht) not built"}))
+        return 0
+    line = {"metric": "points*ell/s", "value": r["value"], "unit": "points*ell/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["seconds_per_step"] * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": spec["name"], "Nl": spec["Nl"], "Nx": spec["Nx"], "N": args.ref_sample,
+                       "maps": 1},
+            "cpu_baseline": {"value": r["value"], "unit": r["unit"], "cores": r["cores"], "kind": r["kind"],
+                             "sample": r["sample"]},
+            "e2e": {"value": r["value"], "unit": "points*ell/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------------------
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--cpu-sample", type=int, default=200_000)
+    ap.add_argument("--ref-sample", type=int, default=200_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    args.warmup = max(args.warmup, 3)
+    spec = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        return run_reference_arm(args, spec)
+
+    import torch
+    import torch.distributed as dist
+    from directsht_b200 import DirectSHT
+    from directsht_b200 import _lib as L
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    lib = L.load()
+    Nl, Nx, N = spec["Nl"], spec["Nx"], spec["N"]
+    th, ph, w = make_points(spec, seed=rank)
+    t0 = time.time()
+    d = DirectSHT(Nl, Nx, device=dev)
+    t_plan = time.time() - t0
+    thd, phd, wd = (torch.from_numpy(a).to(dev) for a in (th, ph, w))
+    alm = torch.empty(d.Nlm, dtype=torch.complex128, device=dev)
+    nbytes = ct.c_size_t()
+    L.check(lib.dsht_workspace_size(d._plan, N, ct.byref(nbytes)))
+    ws = torch.empty(nbytes.value, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = ct.c_void_p(stream.cuda_stream)
+
+    def step():
+        L.check(lib.dsht_execute(d._plan, L.ptr(thd), L.ptr(phd), L.ptr(wd), N, L.DSHT_MODE_CALL, L.ptr(alm),
+                                 L.ptr(ws), ws.numel(), sp))
+
+    for _ in range(args.warmup):
+        step()
+    L.check(lib.dsht_profile_enable(d._plan, 1))
+    stage_ms = (ct.c_double * 5)()
+    calls = ct.c_int64()
+    L.check(lib.dsht_profile_read(d._plan, stage_ms, ct.byref(calls), 1))
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = lib.dsht_launch_count()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    ev[0].record(stream)
+    for k in range(args.steps):
+        step()
+        ev[k + 1].record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches = lib.dsht_launch_count() - launches0
+    clk = clocks.stop()
+    per_step = np.array([ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)])
+    total_ms = ev[0].elapsed_time(ev[-1])
+    L.check(lib.dsht_profile_read(d._plan, stage_ms, ct.byref(calls), 1))
+    L.check(lib.dsht_profile_enable(d._plan, 0))
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_step = total_ms / args.steps
+    value = world * N * Nl / (ms_step / 1e3)
+
+    # Dominant stage and its roofline.
+    stages = {n: stage_ms[i] / max(calls.value, 1) for i, n in enumerate(L.STAGES)}
+    hbm_peak, bf16_peak, peak_src = measured_peaks()
+    top = max(stages, key=stages.get)
+    if top == "contract":
+        alg_bytes = 16.0 * d.Nlm * Nx
+        achieved = alg_bytes / (stages[top] * 1e-3) / 1e9
+        roof = {"kernel": "contract_fp64_kernel", "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
+                "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
+                "peak_source": peak_src, "algorithmic": "16 B of FP64 table per (l, m, node)"}
+    else:
+        alg_flops = 24.0 * N * Nl
+        peak = 40.0  # nominal B200 FP64 TFLOP/s; no measured FP64 figure exists on this pool
+        achieved = alg_flops / (stages[top] * 1e-3) / 1e12
+        roof = {"kernel": "bin_sums_fp64_kernel" if top == "bin_sums" else top, "bound": "fp64",
+                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                "peak_source": "nominal", "algorithmic": "24 flop per (point, m): 8 FMA sums + 4 FMA angle step"}
+
+    # End to end through the host-pointer C ABI entry, pinned host buffers.
+    e2e = None
+    if args.e2e_steps > 0:
+        hp = [torch.from_numpy(a).pin_memory() for a in (th, ph, w)]
+        out = torch.empty(2 * d.Nlm, dtype=torch.float64).pin_memory()
+        dp = ct.POINTER(ct.c_double)
+
+        def e2e_step():
+            L.check(lib.dsht_execute_host(d._plan, ct.cast(hp[0].data_ptr(), dp), ct.cast(hp[1].data_ptr(), dp),
+                                          ct.cast(hp[2].data_ptr(), dp), N, L.DSHT_MODE_CALL,
+                                          ct.cast(out.data_ptr(), dp)))
+
+        e2e_step()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        torch.cuda.synchronize()
+        e2e_s = (time.perf_counter() - t0) / args.e2e_steps
+        if world > 1:
+            t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e = {"value": world * N * Nl / e2e_s, "unit": "points*ell/s", "ms_per_step": e2e_s * 1e3,
+               "h2d_bytes_per_step": 24 * N, "d2h_bytes_per_step": 16 * d.Nlm,
+               "path": "dsht_execute_host (C ABI, pinned host buffers), wall clock per call"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_reference_run(spec, args.cpu_sample, 1, 0)
+        except Exception as exc:  # reported, not fatal
+            cpu = {"value": None, "error": str(exc)}
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        line = {
+            "metric": "points*ell/s", "value": value, "unit": "points*ell/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": spec["name"], "Nl": Nl, "Nx": Nx, "N": N, "maps": 1, "precision": "fp64",
+                       "l2": "inputs (240 MB) and tables (17 GB) exceed L2 every step",
+                       "parallelism": f"replicas x{world}"},
+            "p50_ms": float(np.percentile(per_step, 50)), "p99_ms": float(np.percentile(per_step, 99)),
+            "stages_ms": stages, "plan_build_s": t_plan, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": int(launches), "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

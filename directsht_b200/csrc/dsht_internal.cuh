@@ -1,0 +1,99 @@
+// Internal declarations shared by the DirectSHT B200 kernels.
+//
+// Data layout in HBM (Nlm = Nl(Nl+1)/2, rows in Healpy order m(2Nl-1-m)/2 + l):
+//   tables   Yv, Yd      double [Nlm][Nx]          (sht/sht.py:50-56 layout, numpy path)
+//   points   key         uint32 [N]                set*(Nx-1) + bin, or DSHT_KEY_DROP
+//            sorted      double [5][N]             (phi, w h0, w h1, w h2, w h3) by key
+//   pieces   <= 1 bin each, <= piece_max points    (key, start, len)
+//   partial  double [piece][8][Nl]                 (k, re/im) bin sums for every m
+//   fold     double [Nl][4 q][Nx][4]               q = {equ even, equ odd, pol even, pol odd}
+//                                                  entries (A re, A im, B re, B im)
+//   alm      double2 [Nlm]                         complex128, Healpy order
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+
+#include "../../include/dsht.h"
+
+#define DSHT_KEY_DROP 0xffffffffu
+
+namespace dsht {
+
+// Number of point sets: {equatorial, rotated polar} x {cos >= 0, cos < 0}.
+constexpr int kSets = 4;
+// Error-flag bits written by the point kernel.
+constexpr unsigned kFlagThetaRange = 1u;   // basic_sht assertion (sht/sht.py:171-172)
+constexpr unsigned kFlagPolarRange = 2u;   // rotated polar point still outside (-xmax, xmax)
+constexpr unsigned kFlagHasPolar = 4u;     // at least one point went through the rotation
+
+struct Geometry {
+  int Nl, Nx;
+  double xmax;
+  double dx;          // xmax / (Nx-1), the numpy grid step  (sht/sht.py:48)
+  double acos_xmax;   // numpy arccos(xmax), arccos(-xmax) (sht/sht.py:171)
+  double acos_mxmax;
+  int64_t Nlm;
+  int nbins;          // Nx - 1 right-open bins
+  int nkeys;          // kSets * nbins
+};
+
+// Workspace carve-up for one execute call.
+struct Workspace {
+  uint32_t* key;        // [N]
+  uint32_t* idx_sorted; // [N] original index of each sorted slot (unused by the fused path)
+  double* pay;          // [5][N]
+  uint32_t* count;      // [nkeys + 1]
+  uint32_t* offset;     // [nkeys + 1]
+  uint32_t* cursor;     // [nkeys]
+  int* piece_first;     // [nkeys + 1]  first piece of each key (exclusive scan)
+  int* piece_key;       // [pmax]
+  int64_t* piece_start; // [pmax]
+  int* piece_len;       // [pmax]
+  int* npieces;         // [1]
+  unsigned* flags;      // [1]
+  double* partial;      // [pmax][8][Nl]
+  double* fold;         // [Nl][4][Nx][4]
+  uint8_t* tile_live;   // [4 q][ntile]
+  double* alm_equ;      // [Nlm][2]
+  double* alm_pol;      // [Nlm][2]
+  int64_t npts;         // N, the stride of pay
+  int64_t pmax;
+  int piece_max;
+  size_t bytes;
+};
+
+size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* base, Workspace* ws);
+int default_piece_max(const Geometry& g, int64_t N);
+
+// Kernels launched by api.cu (each file owns its launch helpers).
+void launch_tables(const Geometry& g, double* Yv, double* Yd, cudaStream_t s);
+void launch_points(const Geometry& g, const double* theta, const double* phi, const double* w,
+                   int64_t N, int mode, const Workspace& ws, cudaStream_t s);
+void launch_bin_sums_fp64(const Geometry& g, const Workspace& ws, cudaStream_t s);
+void launch_fold(const Geometry& g, const Workspace& ws, cudaStream_t s);
+void launch_contract_fp64(const Geometry& g, const double* Yv, const double* Yd,
+                          const Workspace& ws, cudaStream_t s);
+void launch_rotate_back(const Geometry& g, const double* alm_rot, const double* alm_add,
+                        double* alm_out, const unsigned* flags, cudaStream_t s);
+
+// Healpy index of (l, m).
+__host__ __device__ inline int64_t hp_index(int l, int m, int Nl) {
+  return ((int64_t)m * (2 * Nl - 1 - m)) / 2 + l;
+}
+
+}  // namespace dsht
+
+#define DSHT_CUDA_OK(expr)                                   \
+  do {                                                       \
+    cudaError_t _e = (expr);                                 \
+    if (_e != cudaSuccess) return dsht::set_cuda_error(_e, #expr, __FILE__, __LINE__); \
+  } while (0)
+
+namespace dsht {
+int set_error(int code, const char* fmt, ...);
+// Adds n to the process-wide count of kernels this library launched.
+void count_launches(int n);
+int set_cuda_error(cudaError_t e, const char* what, const char* file, int line);
+}  // namespace dsht

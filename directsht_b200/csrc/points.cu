@@ -1,0 +1,254 @@
+// Per-point classification, x-bin search, Hermite weights and the counting sort by bin.
+//
+// Each point goes to one of four sets: equatorial with cos(theta) >= 0 / < 0, or polar
+// (|cos theta| >= xmax, sht/sht.py:128-130) rotated by +90 deg about y and split by the
+// sign of the rotated cos.  The bin is numpy's digitize(|x|, x_nodes) - 1 (right-open,
+// sht/sht.py:212) and t = (|x| - x_j)/dx (sht/sht.py:221); the payload is phi and
+// w * {(2t+1)(1-t)^2, t(1-t)^2, t^2(3-2t), t^2(t-1)} (sht/sht.py:239-240).
+//
+// Sort: key = set*(Nx-1) + bin.  count (shared-memory histogram per block, flushed with
+// one global add per live key), one-block exclusive scan that also cuts every key into
+// pieces of at most piece_max points, then a scatter in which each block reserves a
+// contiguous range per key with one global add.  HBM bound: 24 B read twice and 44 B
+// written per point.
+#include "dsht_internal.cuh"
+
+namespace dsht {
+namespace {
+
+constexpr int kPointThreads = 256;
+constexpr int kScatterTile = 16384;  // points per block in the scatter pass
+
+struct PointOut {
+  uint32_t key;
+  double phi;
+  double t;
+  unsigned flag;
+};
+
+__device__ __forceinline__ PointOut classify(const Geometry& g, int mode, double th, double ph) {
+  PointOut o;
+  o.flag = 0;
+  o.key = DSHT_KEY_DROP;
+  o.phi = ph;
+  o.t = 0.0;
+  const double c = cos(th);
+  double x;        // signed x used for binning
+  int set;
+  if (mode == DSHT_MODE_CALL) {
+    const double xv = fabs(c);
+    if (xv >= g.xmax) {
+      // Rotate n = (s cos p, s sin p, c) to (c, s sin p, -s cos p).
+      double sp, cp;
+      sincos(ph, &sp, &cp);
+      const double st = sin(th);
+      const double nx = st * cp, ny = st * sp;
+      const double xr = -nx;
+      double pr = atan2(ny, c);
+      if (pr < 0.0) pr += 2.0 * M_PI;
+      o.phi = pr;
+      const double tr = acos(fmin(fmax(xr, -1.0), 1.0));
+      if (!(tr > g.acos_xmax && tr < g.acos_mxmax)) {
+        o.flag = kFlagPolarRange;
+        return o;
+      }
+      x = cos(tr);  // the reference takes cos of the rotated theta (sht/sht.py:190)
+      set = 2;
+      o.flag = kFlagHasPolar;
+    } else if (xv < g.xmax) {
+      if (!(th >= 0.0 && th > g.acos_xmax && th < g.acos_mxmax)) {
+        o.flag = kFlagThetaRange;
+        return o;
+      }
+      x = c;
+      set = 0;
+    } else {
+      return o;  // NaN theta: in neither set (sht/sht.py:129-130)
+    }
+  } else {
+    if (!(th >= 0.0 && th > g.acos_xmax && th < g.acos_mxmax)) {
+      o.flag = kFlagThetaRange;
+      return o;
+    }
+    x = c;
+    set = 0;
+  }
+  if (!(x >= 0.0)) set += 1;          // x < 0 half (sht/sht.py:193)
+  const double ax = fabs(x);
+  // digitize: x_j <= ax < x_{j+1} with x_j = j * dx exactly as numpy builds the grid.
+  int j = (int)(ax / g.dx);
+  if (j > g.nbins - 1) j = g.nbins - 1;
+  if (j < 0) j = 0;
+  if (ax < (double)j * g.dx) j -= 1;
+  else if (j + 1 <= g.nbins && ax >= (double)(j + 1) * g.dx) j += 1;
+  if (j < 0 || j >= g.nbins) {
+    o.flag = (set >= 2) ? kFlagPolarRange : kFlagThetaRange;
+    return o;
+  }
+  o.t = __ddiv_rn(__dadd_rn(ax, -(double)j * g.dx), g.dx);
+  o.key = (uint32_t)(set * g.nbins + j);
+  return o;
+}
+
+__global__ void __launch_bounds__(kPointThreads)
+count_kernel(Geometry g, int mode, const double* __restrict__ theta, const double* __restrict__ phi,
+             int64_t N, uint32_t* __restrict__ keys, uint32_t* __restrict__ count,
+             unsigned* __restrict__ flags) {
+  extern __shared__ uint32_t hist[];
+  for (int k = threadIdx.x; k < g.nkeys; k += blockDim.x) hist[k] = 0;
+  __syncthreads();
+  unsigned fl = 0;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
+    PointOut o = classify(g, mode, theta[i], phi[i]);
+    keys[i] = o.key;
+    fl |= o.flag;
+    if (o.key != DSHT_KEY_DROP) atomicAdd(&hist[o.key], 1u);
+  }
+  if (fl) atomicOr(flags, fl);
+  __syncthreads();
+  for (int k = threadIdx.x; k < g.nkeys; k += blockDim.x)
+    if (hist[k]) atomicAdd(&count[k], hist[k]);
+}
+
+// Single-block exclusive scans: key offsets, pieces per key, and the piece list.
+constexpr int kScanThreads = 1024;
+
+__device__ __forceinline__ uint32_t block_scan_excl(uint32_t v, uint32_t* warp_tot, uint32_t* total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_tot[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    uint32_t t = (lane < (int)(blockDim.x >> 5)) ? warp_tot[lane] : 0u;
+    uint32_t s = t;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    warp_tot[lane] = s - t;
+    if (lane == 31) *total = s;
+  }
+  __syncthreads();
+  uint32_t r = x - v + warp_tot[wid];
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+scan_kernel(int nkeys, int nbins, int piece_max, int64_t pmax, const uint32_t* __restrict__ count,
+            uint32_t* __restrict__ offset, uint32_t* __restrict__ cursor, int* __restrict__ piece_first,
+            int* __restrict__ piece_key, int64_t* __restrict__ piece_start, int* __restrict__ piece_len,
+            int* __restrict__ npieces) {
+  __shared__ uint32_t warp_tot[32];
+  __shared__ uint32_t total;
+  __shared__ uint32_t carry_off, carry_pc;
+  if (threadIdx.x == 0) { carry_off = 0; carry_pc = 0; }
+  __syncthreads();
+  for (int base = 0; base < nkeys; base += blockDim.x) {
+    const int k = base + threadIdx.x;
+    const uint32_t c = (k < nkeys) ? count[k] : 0u;
+    const uint32_t pc = (c + piece_max - 1) / piece_max;
+    uint32_t o = block_scan_excl(c, warp_tot, &total);
+    const uint32_t tot_c = total;
+    uint32_t p = block_scan_excl(pc, warp_tot, &total);
+    const uint32_t tot_p = total;
+    o += carry_off;
+    p += carry_pc;
+    if (k < nkeys) {
+      offset[k] = o;
+      cursor[k] = o;
+      piece_first[k] = (int)p;
+      for (uint32_t q = 0; q < pc; ++q) {
+        const int64_t pi = (int64_t)p + q;
+        if (pi < pmax) {
+          piece_key[pi] = k;
+          piece_start[pi] = (int64_t)o + (int64_t)q * piece_max;
+          const uint32_t rem = c - q * piece_max;
+          piece_len[pi] = (int)(rem < (uint32_t)piece_max ? rem : (uint32_t)piece_max);
+        }
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) { carry_off += tot_c; carry_pc += tot_p; }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    offset[nkeys] = carry_off;
+    piece_first[nkeys] = (int)carry_pc;
+    *npieces = (int)carry_pc;
+  }
+}
+
+__global__ void __launch_bounds__(kPointThreads)
+scatter_kernel(Geometry g, int mode, const double* __restrict__ theta, const double* __restrict__ phi,
+               const double* __restrict__ w, int64_t N, const uint32_t* __restrict__ keys,
+               uint32_t* __restrict__ cursor, double* __restrict__ pay) {
+  extern __shared__ uint32_t loc[];  // [nkeys] local counts, then local bases
+  const int64_t lo = (int64_t)blockIdx.x * kScatterTile;
+  const int64_t hi = min(lo + (int64_t)kScatterTile, N);
+  for (int k = threadIdx.x; k < g.nkeys; k += blockDim.x) loc[k] = 0;
+  __syncthreads();
+  for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    const uint32_t k = keys[i];
+    if (k != DSHT_KEY_DROP) atomicAdd(&loc[k], 1u);
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < g.nkeys; k += blockDim.x) {
+    const uint32_t c = loc[k];
+    if (c) loc[k] = atomicAdd(&cursor[k], c);
+  }
+  __syncthreads();
+  for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    const uint32_t k = keys[i];
+    if (k == DSHT_KEY_DROP) continue;
+    const uint32_t pos = atomicAdd(&loc[k], 1u);
+    PointOut o = classify(g, mode, theta[i], phi[i]);
+    // Same rounding order as the numpy expressions of sht/sht.py:239-240.
+    const double t = o.t, wi = w[i];
+    const double omt = __dadd_rn(1.0, -t);
+    const double omt2 = __dmul_rn(omt, omt);
+    const double t2 = __dmul_rn(t, t);
+    pay[pos] = o.phi;
+    pay[(size_t)N + pos] = __dmul_rn(wi, __dmul_rn(__dadd_rn(__dmul_rn(2.0, t), 1.0), omt2));
+    pay[2 * (size_t)N + pos] = __dmul_rn(wi, __dmul_rn(t, omt2));
+    pay[3 * (size_t)N + pos] = __dmul_rn(wi, __dmul_rn(t2, __dadd_rn(3.0, -__dmul_rn(2.0, t))));
+    pay[4 * (size_t)N + pos] = __dmul_rn(wi, __dmul_rn(t2, __dadd_rn(t, -1.0)));
+  }
+}
+
+}  // namespace
+
+void launch_points(const Geometry& g, const double* theta, const double* phi, const double* w,
+                   int64_t N, int mode, const Workspace& ws, cudaStream_t s) {
+  cudaMemsetAsync(ws.count, 0, sizeof(uint32_t) * (g.nkeys + 1), s);
+  cudaMemsetAsync(ws.flags, 0, sizeof(unsigned), s);
+  const size_t hsmem = sizeof(uint32_t) * g.nkeys;
+  cudaFuncSetAttribute(count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem);
+  cudaFuncSetAttribute(scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem);
+  if (N > 0) {
+    int64_t blocks = (N + kPointThreads * 8 - 1) / (kPointThreads * 8);
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    count_kernel<<<(unsigned)blocks, kPointThreads, hsmem, s>>>(g, mode, theta, phi, N, ws.key,
+                                                               ws.count, ws.flags);
+    count_launches(1);
+  }
+  scan_kernel<<<1, kScanThreads, 0, s>>>(g.nkeys, g.nbins, ws.piece_max, ws.pmax, ws.count, ws.offset,
+                                         ws.cursor, ws.piece_first, ws.piece_key, ws.piece_start,
+                                         ws.piece_len, ws.npieces);
+  count_launches(1);
+  if (N > 0) {
+    const int64_t blocks = (N + kScatterTile - 1) / kScatterTile;
+    scatter_kernel<<<(unsigned)blocks, kPointThreads, hsmem, s>>>(g, mode, theta, phi, w, N, ws.key,
+                                                                 ws.cursor, ws.pay);
+    count_launches(1);
+  }
+}
+
+}  // namespace dsht

@@ -1,0 +1,175 @@
+"""Drop-in ``DirectSHT`` backed by the sm_100a kernels of libdsht_b200.so.
+
+Mirrors the reference's ``sht/sht.py:30-283`` interface: the constructor arguments,
+``indx``, ``get_Ylm``/``get_dYlm``, ``alm2cl``, ``__call__`` and ``basic_sht``, with the
+same Healpy alm ordering, return types and exceptions.  Inputs may be numpy arrays
+(results come back as numpy) or CUDA torch tensors (results stay on the device).
+PyTorch supplies device memory and the current stream; all arithmetic runs in the
+library's CUDA kernels.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import time
+
+import numpy as np
+import torch
+
+from . import _lib as L
+
+
+def _as_device_f64(a, device) -> torch.Tensor:
+    if isinstance(a, torch.Tensor):
+        return a.to(device=device, dtype=torch.float64).contiguous()
+    arr = np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+    return torch.from_numpy(arr).to(device=device, non_blocking=False)
+
+
+class DirectSHT:
+    """Brute-force spherical harmonic transforms on a B200 (``sht/sht.py:30``)."""
+
+    def __init__(self, Nell, Nx, xmax=0.75, dflt_type="float64", null_unphysical=True, device=None):
+        """Build the FP64 Ylm/dYlm tables on the GPU (``sht/sht.py:32-56``).
+
+        :param Nell: number of ells (and m's).
+        :param Nx: number of x = |cos theta| grid points in [0, xmax].
+        :param xmax: largest |cos theta| handled without rotation.
+        :param dflt_type: dtype of the host copy of the x grid (the tables are FP64).
+        :param null_unphysical: accepted for compatibility; rows l < m are never stored.
+        :param device: CUDA device (default: the current one).
+        """
+        self._lib = L.load()
+        if not torch.cuda.is_available():
+            raise RuntimeError("DirectSHT (directsht_b200) needs a CUDA device; there is no CPU fallback")
+        self.device = torch.device("cuda", torch.cuda.current_device() if device is None
+                                   else torch.device(device).index or 0)
+        self.Nell, self.Nx, self.xmax = int(Nell), int(Nx), float(xmax)
+        self.Nlm = (self.Nell * (self.Nell + 1)) // 2
+        xx = np.arange(Nx, dtype=dflt_type)
+        xx *= xmax / float(Nx - 1)
+        self.x = xx
+        self._plan = ct.c_void_p()
+        with torch.cuda.device(self.device):
+            L.check(self._lib.dsht_plan_create(self.Nell, self.Nx, self.xmax, 0, ct.byref(self._plan)))
+        self._Yv = None
+        self._Yd = None
+        self.verbose_timing = None
+
+    def __del__(self):
+        plan = getattr(self, "_plan", None)
+        if plan is not None and plan.value:
+            try:
+                with torch.cuda.device(self.device):
+                    self._lib.dsht_plan_destroy(plan)
+            except Exception:
+                pass
+            self._plan = None
+
+    # -- tables ---------------------------------------------------------------------
+    def indx(self, ell, m):
+        """Healpy index (``sht/sht.py:58-67``)."""
+        return (m * (2 * self.Nell - 1 - m)) // 2 + ell
+
+    def _row(self, which, ell, m):
+        out = np.empty(self.Nx, dtype=np.float64)
+        with torch.cuda.device(self.device):
+            L.check(self._lib.dsht_get_row(self._plan, which, int(ell), int(m), L.dptr(out)))
+        return out
+
+    def get_Ylm(self, ell, m):
+        """Ylm(x_i, 0) on the grid (``sht/sht.py:69-80``)."""
+        return self._row(0, ell, m)
+
+    def get_dYlm(self, ell, m):
+        """d/dx Ylm(x_i, 0) on the grid (``sht/sht.py:82-93``)."""
+        return self._row(1, ell, m)
+
+    def _table(self, which):
+        out = np.empty((self.Nlm, self.Nx), dtype=np.float64)
+        with torch.cuda.device(self.device):
+            L.check(self._lib.dsht_get_table(self._plan, which, L.dptr(out)))
+        return out
+
+    @property
+    def Yv(self):
+        """Host copy of the Ylm table, (Nlm, Nx) in Healpy row order (made on first use)."""
+        if self._Yv is None:
+            self._Yv = self._table(0)
+        return self._Yv
+
+    @property
+    def Yd(self):
+        """Host copy of the dYlm/dx table (made on first use)."""
+        if self._Yd is None:
+            self._Yd = self._table(1)
+        return self._Yd
+
+    def alm2cl(self, alm):
+        """1/(2l+1) sum_m |alm|^2 (``sht/sht.py:95-109``)."""
+        if isinstance(alm, torch.Tensor):
+            alm = alm.detach().cpu().numpy()
+        a = np.ascontiguousarray(np.asarray(alm, dtype=np.complex128))
+        cl = np.zeros(self.Nell)
+        L.check(self._lib.dsht_alm2cl(self.Nell, a.view(np.float64).ctypes.data_as(ct.POINTER(ct.c_double)),
+                                      L.dptr(cl)))
+        return cl
+
+    # -- transforms -----------------------------------------------------------------
+    def _execute(self, t, p, w, mode):
+        on_device = isinstance(t, torch.Tensor) and t.is_cuda
+        n = len(t)
+        with torch.cuda.device(self.device):
+            td = _as_device_f64(t, self.device)
+            pd = _as_device_f64(p, self.device)
+            wd = _as_device_f64(w, self.device)
+            alm = torch.empty(self.Nlm, dtype=torch.complex128, device=self.device)
+            nbytes = ct.c_size_t()
+            L.check(self._lib.dsht_workspace_size(self._plan, n, ct.byref(nbytes)))
+            ws = torch.empty(max(int(nbytes.value), 1), dtype=torch.uint8, device=self.device)
+            stream = torch.cuda.current_stream(self.device).cuda_stream
+            rc = self._lib.dsht_execute(self._plan, L.ptr(td), L.ptr(pd), L.ptr(wd), n, mode, L.ptr(alm),
+                                        L.ptr(ws), ws.numel(), ct.c_void_p(stream))
+        return rc, (alm if on_device else alm.cpu().numpy())
+
+    def __call__(self, t, p, w):
+        """alm of weighted points at (theta, phi) (``sht/sht.py:112-150``).
+
+        Points with |cos theta| >= xmax are rotated by 90 degrees, transformed and
+        their alm rotated back, all on the GPU.  Returns complex128 alm in Healpy order.
+        """
+        if not (len(t) == len(p) and len(p) == len(w)):
+            raise AssertionError("theta,phi,wt must be the same length.")
+        rc, alm = self._execute(t, p, w, L.DSHT_MODE_CALL)
+        if rc == L.DSHT_ERR_POLAR_RANGE:
+            # sht/sht.py:141-148: the polar transform failed; the reference prints and
+            # returns the (still zero) alm without the equatorial part.
+            print(f"AssertionError in basic_sht: theta must be in [ACos[xmax],ACos[-xmax]).")
+            if self.xmax < np.sin(np.pi / 4):
+                print("Warning: xmax is smaller than sin(pi/4), so some points may"
+                      " still lie in the polar cap after rotation by 90 degrees."
+                      " Trying increasing it.")
+            return alm * 0
+        if rc == L.DSHT_ERR_THETA_RANGE:
+            raise AssertionError("theta must be in [ACos[xmax],ACos[-xmax]).")
+        L.check(rc)
+        return alm
+
+    def basic_sht(self, theta, phi, wt, reg_factor=1.0, verbose=True):
+        """alm of points with |cos theta| < xmax, no rotation (``sht/sht.py:153-283``).
+
+        Like the reference, multiplies ``wt`` in place by ``reg_factor`` and divides the
+        result by it.
+        """
+        if not (len(theta) == len(phi) and len(phi) == len(wt)):
+            raise AssertionError("theta,phi,wt must be the same length.")
+        t0 = time.time()
+        wt *= reg_factor
+        rc, alm = self._execute(theta, phi, wt, L.DSHT_MODE_BASIC)
+        if rc == L.DSHT_ERR_THETA_RANGE:
+            raise AssertionError("theta must be in [ACos[xmax],ACos[-xmax]).")
+        if rc == L.DSHT_ERR_EMPTY:
+            raise ValueError("The theta array seems to be empty!")
+        L.check(rc)
+        if verbose:
+            print(f"basic_sht on the GPU took {time.time() - t0} seconds.", flush=True)
+        return alm / reg_factor

@@ -1,0 +1,140 @@
+/*
+ * dsht.h -- C ABI of the B200-native DirectSHT forward transform (libdsht_b200.so).
+ *
+ * Computes a_lm = sum_i w_i conj(Y_lm(theta_i, phi_i)) for weighted points on the sphere
+ * with the reference's spline scheme: FP64 Ylm/dYlm tables on Nx uniform nodes in
+ * x = |cos theta| in [0, xmax], cubic Hermite interpolation, per-bin per-m sums, and a
+ * per-m contraction; points with |cos theta| >= xmax are rotated by +90 deg about y,
+ * transformed, and their alm rotated back.  Output alm are complex128 (interleaved
+ * re, im) in Healpy order alm[m(2Nl-1-m)/2 + l], l < Nl, m <= l.
+ *
+ * Reference interfaces replaced (martinjameswhite/directsht):
+ *   dsht_plan_create      DirectSHT.__init__            sht/sht.py:32-56
+ *   dsht_execute          DirectSHT.__call__ / basic_sht sht/sht.py:112-150, :153-283
+ *   dsht_get_row          DirectSHT.get_Ylm / get_dYlm  sht/sht.py:69-93
+ *   dsht_alm2cl           DirectSHT.alm2cl              sht/sht.py:95-109
+ *   dsht_index            DirectSHT.indx                sht/sht.py:58-67
+ *   dsht_make_table       make_table   (ctypes)         csht/sht_helper.c:18, csht/sht.py:39-42
+ *   dsht_do_transform     do_transform (ctypes)         csht/sht_helper.c:176, csht/sht.py:111-115
+ *
+ * All functions return DSHT_OK (0) or a DSHT_ERR_* code; dsht_last_error() gives the
+ * message of the last failure on the calling thread.  Device pointers are owned by the
+ * caller; a plan owns its tables.  A plan may be shared read-only by several threads;
+ * calls on one plan with the plan-owned workspace must not overlap.
+ */
+#ifndef DSHT_H_
+#define DSHT_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct dsht_plan_s* dsht_plan_t;
+
+enum {
+  DSHT_OK = 0,
+  DSHT_ERR_INVALID = 1,      /* bad argument (sizes, null pointers)                  */
+  DSHT_ERR_CUDA = 2,         /* CUDA runtime failure                                  */
+  DSHT_ERR_NOMEM = 3,        /* device allocation or workspace too small              */
+  DSHT_ERR_THETA_RANGE = 4,  /* basic_sht assertion: theta outside (acos xmax, acos -xmax)
+                                (sht/sht.py:171-172) -> AssertionError                 */
+  DSHT_ERR_EMPTY = 5,        /* basic_sht with no points (sht/sht.py:205-206) -> ValueError */
+  DSHT_ERR_POLAR_RANGE = 6   /* a rotated polar point is still polar (xmax < sin(pi/4));
+                                the reference then returns zeros (sht/sht.py:141-148)   */
+};
+
+/* Execution modes of dsht_execute. */
+enum {
+  DSHT_MODE_CALL = 0,   /* DirectSHT.__call__: polar/equatorial split + rotation   */
+  DSHT_MODE_BASIC = 1   /* DirectSHT.basic_sht: every point must be equatorial     */
+};
+
+/* Plan flags. */
+enum {
+  DSHT_PLAN_DEFAULT = 0
+};
+
+/* Build the x grid and the FP64 Ylm/dYlm tables on the current CUDA device.
+ * Replaces DirectSHT.__init__ (sht/sht.py:32-56). Nl >= 1, Nx >= 2, 0 < xmax < 1. */
+int dsht_plan_create(int Nl, int Nx, double xmax, int flags, dsht_plan_t* plan);
+int dsht_plan_destroy(dsht_plan_t plan);
+
+/* Sizes of a plan. */
+int dsht_plan_info(dsht_plan_t plan, int* Nl, int* Nx, double* xmax, int64_t* Nlm);
+
+/* Healpy index m(2Nl-1-m)/2 + l (sht/sht.py:58-67). */
+int64_t dsht_index(int Nl, int ell, int m);
+
+/* Bytes of device workspace dsht_execute needs for N points. */
+int dsht_workspace_size(dsht_plan_t plan, int64_t N, size_t* bytes);
+
+/* Forward transform of N points given by DEVICE pointers theta, phi, w (float64).
+ * alm: DEVICE pointer to 2*Nlm doubles (complex128), overwritten.
+ * workspace: DEVICE buffer of at least dsht_workspace_size bytes, or NULL to use a
+ * buffer the plan owns (grown on demand).  stream: a cudaStream_t (NULL = default).
+ * Stream-ordered; range errors are detected on the device and reported when the call
+ * synchronises, which it does once at the end (to read the error flags).
+ * Replaces DirectSHT.__call__ (mode CALL) and DirectSHT.basic_sht (mode BASIC). */
+int dsht_execute(dsht_plan_t plan, const double* theta, const double* phi, const double* w,
+                 int64_t N, int mode, double* alm, void* workspace, size_t workspace_bytes,
+                 void* stream);
+
+/* alm_out = alm_add + R(alm_rot): alm of points rotated by +90 deg about y rotated back to
+ * the original frame with Wigner d(pi/2) (DEVICE pointers, 2*Nlm doubles each; alm_add may be
+ * NULL for zeros, alm_out may alias alm_add).  Replaces healpy's
+ * Rotator(rot=(0,90,0), eulertype='ZYZ', inv=True).rotate_alm at sht/sht.py:138-139. */
+int dsht_rotate_back(dsht_plan_t plan, const double* alm_rot, const double* alm_add, double* alm_out,
+                     void* stream);
+
+/* Same with HOST pointers (pageable or pinned); copies in, runs, copies alm out. */
+int dsht_execute_host(dsht_plan_t plan, const double* theta, const double* phi,
+                      const double* w, int64_t N, int mode, double* alm_host);
+
+/* One row of the tables to HOST memory: which = 0 -> Ylm(x_j, 0), 1 -> dYlm/dx.
+ * out: Nx doubles.  Replaces DirectSHT.get_Ylm / get_dYlm (sht/sht.py:69-93). */
+int dsht_get_row(dsht_plan_t plan, int which, int ell, int m, double* out);
+
+/* Whole table (Nlm x Nx doubles) to a HOST buffer. */
+int dsht_get_table(dsht_plan_t plan, int which, double* out);
+
+/* Pseudo-spectrum cl[l] = (|a_l0|^2 + 2 sum_{m>0} |a_lm|^2)/(2l+1) of a HOST alm vector.
+ * Replaces DirectSHT.alm2cl (sht/sht.py:95-109). */
+int dsht_alm2cl(int Nl, const double* alm, double* cl);
+
+/* Drop-ins for the reference's ctypes library csht/sht_helper.so (HOST arrays).
+ * dsht_make_table fills Yv, Yd (Nlm*Nx doubles each) like make_table
+ * (csht/sht_helper.c:18-116).  dsht_do_transform takes points of one sign of cos(theta)
+ * (cost = cos(theta)), accumulates nothing across calls, and writes
+ * carr = sum w Y cos(m phi), sarr = sum w Y sin(m phi) per Healpy index with
+ * |cos theta| interpolated and no parity factor, like do_transform
+ * (csht/sht_helper.c:176-286); Yv/Yd are not read: the tables of a plan cached per
+ * (Nl, Nx, xmax) on the device are used.  Return 0 on success, like the reference. */
+int dsht_make_table(int Nl, int Nx, double xmax, double* Yv, double* Yd);
+int dsht_do_transform(int Nl, int Nx, double xmax, double* Yv, double* Yd, int Np,
+                      double* cost, double* phi, double* wt, double* carr, double* sarr);
+
+/* Stage timers (CUDA events recorded on the execute stream around every stage).
+ * Stages: 0 points+sort, 1 bin sums, 2 fold, 3 contraction, 4 rotation. */
+enum { DSHT_STAGE_POINTS = 0, DSHT_STAGE_BIN_SUMS = 1, DSHT_STAGE_FOLD = 2, DSHT_STAGE_CONTRACT = 3,
+       DSHT_STAGE_ROTATE = 4, DSHT_STAGE_COUNT = 5 };
+int dsht_profile_enable(dsht_plan_t plan, int enable);
+/* Accumulated milliseconds per stage and number of profiled executes; reset=1 clears. */
+int dsht_profile_read(dsht_plan_t plan, double* ms, int64_t* calls, int reset);
+
+/* Kernels this library has launched in this process (all devices). */
+int64_t dsht_launch_count(void);
+
+/* Message of the last error on this thread ("" if none). */
+const char* dsht_last_error(void);
+
+/* Library version string. */
+const char* dsht_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DSHT_H_ */
