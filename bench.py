@@ -31,6 +31,9 @@ WORKLOADS = {
     "c2": dict(Nl=1024, Nx=2048, N=10_000_000, kind="c2", wkind="lognormal",
                name="survey-like single map: Nl=1024, Nx=2048, N=1e7, cos(theta)~U[cos1.2,cos0.3], "
                     "phi~U[0,1.5pi), w~lognormal(0,0.5) f64"),
+    # Smaller tables for Nsight Compute captures of the same kernels (inputs still exceed L2).
+    "c2prof": dict(Nl=1024, Nx=256, N=4_000_000, kind="c2", wkind="lognormal",
+                   name="profiling case: Nl=1024, Nx=256, N=4e6, C2 point distribution"),
     "c1": dict(Nl=256, Nx=512, N=100_000, kind="full", wkind="ones",
                name="full sky: Nl=256, Nx=512, N=1e5, cos(theta)~U[-1,1], phi~U[0,2pi), w=1 f64"),
 }
