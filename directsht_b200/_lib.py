@@ -36,6 +36,8 @@ SIGNATURES = {
     "dsht_index": (ct.c_int64, [ct.c_int, ct.c_int, ct.c_int]),
     "dsht_workspace_size": (ct.c_int, [_vp, ct.c_int64, ct.POINTER(ct.c_size_t)]),
     "dsht_execute": (ct.c_int, [_vp, _vp, _vp, _vp, ct.c_int64, ct.c_int, _vp, _vp, ct.c_size_t, _vp]),
+    "dsht_execute_noalloc": (ct.c_int, [_vp, _vp, _vp, _vp, ct.c_int64, ct.c_int, _vp, _vp]),
+    "dsht_noalloc_scratch_bytes": (ct.c_size_t, []),
     "dsht_execute_host": (ct.c_int, [_vp, _dp, _dp, _dp, ct.c_int64, ct.c_int, _dp]),
     "dsht_rotate_back": (ct.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "dsht_get_row": (ct.c_int, [_vp, ct.c_int, ct.c_int, ct.c_int, _dp]),

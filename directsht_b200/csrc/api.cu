@@ -13,27 +13,6 @@
 
 #include "dsht_internal.cuh"
 
-struct dsht_plan_s {
-  dsht::Geometry g;
-  int device = 0;
-  double* Yv = nullptr;
-  double* Yd = nullptr;
-  // Plan-owned buffers, grown on demand (used when the caller passes no workspace and by
-  // the host-pointer entry points).
-  void* ws = nullptr;
-  size_t ws_bytes = 0;
-  double* in = nullptr;  // [3][N] device copies of host inputs
-  int64_t in_n = 0;
-  double* alm = nullptr;  // [2 Nlm]
-  unsigned* h_flags = nullptr;  // pinned
-  // Stage timers.
-  bool prof = false;
-  cudaEvent_t ev[DSHT_STAGE_COUNT + 1] = {};
-  double prof_ms[DSHT_STAGE_COUNT] = {};
-  int64_t prof_calls = 0;
-  std::mutex mu;
-};
-
 namespace dsht {
 
 static thread_local std::string g_last_error;
@@ -102,7 +81,7 @@ size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* ba
   return off;
 }
 
-static Geometry make_geometry(int Nl, int Nx, double xmax) {
+Geometry make_geometry(int Nl, int Nx, double xmax) {
   Geometry g{};
   g.Nl = Nl;
   g.Nx = Nx;
@@ -117,7 +96,7 @@ static Geometry make_geometry(int Nl, int Nx, double xmax) {
 }
 
 // Runs the whole pipeline on `s`; leaves the device flags in ws.flags.
-static int run_pipeline(dsht_plan_s* p, const double* theta, const double* phi, const double* w, int64_t N,
+int run_pipeline(dsht_plan_s* p, const double* theta, const double* phi, const double* w, int64_t N,
                         int mode, double* alm, const Workspace& ws, cudaStream_t s) {
   const Geometry& g = p->g;
   auto mark = [&](int i) {
@@ -143,7 +122,7 @@ static int run_pipeline(dsht_plan_s* p, const double* theta, const double* phi, 
 }
 
 // After the stream has been synchronised: fold the stage events into the totals.
-static void collect_profile(dsht_plan_s* p) {
+void collect_profile(dsht_plan_s* p) {
   if (!p->prof) return;
   for (int i = 0; i < DSHT_STAGE_COUNT; ++i) {
     float ms = 0.f;
@@ -152,7 +131,7 @@ static void collect_profile(dsht_plan_s* p) {
   p->prof_calls += 1;
 }
 
-static int flags_to_status(unsigned f, int mode) {
+int flags_to_status(unsigned f, int mode) {
   if (f & kFlagPolarRange)
     return set_error(DSHT_ERR_POLAR_RANGE,
                      "theta must be in [ACos[xmax],ACos[-xmax]). (a polar point is still polar after the "

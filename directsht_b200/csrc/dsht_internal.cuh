@@ -85,6 +85,40 @@ __host__ __device__ inline int64_t hp_index(int l, int m, int Nl) {
 
 }  // namespace dsht
 
+// A plan: geometry, its FP64 tables, and buffers it owns (see api.cu).
+#include <mutex>
+struct dsht_plan_s {
+  dsht::Geometry g;
+  int device = 0;
+  double* Yv = nullptr;
+  double* Yd = nullptr;
+  // Plan-owned buffers, grown on demand (used when the caller passes no workspace and by
+  // the host-pointer entry points).
+  void* ws = nullptr;
+  size_t ws_bytes = 0;
+  double* in = nullptr;  // [3][N] device copies of host inputs
+  int64_t in_n = 0;
+  double* alm = nullptr;  // [2 Nlm]
+  unsigned* h_flags = nullptr;  // pinned
+  // Stage timers.
+  bool prof = false;
+  cudaEvent_t ev[DSHT_STAGE_COUNT + 1] = {};
+  double prof_ms[DSHT_STAGE_COUNT] = {};
+  int64_t prof_calls = 0;
+  std::mutex mu;
+};
+
+namespace dsht {
+Geometry make_geometry(int Nl, int Nx, double xmax);
+// Enqueue the whole transform on `s` (flags are left in ws.flags; no synchronisation).
+int run_pipeline(dsht_plan_s* p, const double* theta, const double* phi, const double* w, int64_t N, int mode,
+                 double* alm, const Workspace& ws, cudaStream_t s);
+// After the stream has been synchronised: fold the stage events into the plan's totals.
+void collect_profile(dsht_plan_s* p);
+// Map device flag bits to a DSHT status code (and set the error message).
+int flags_to_status(unsigned f, int mode);
+}  // namespace dsht
+
 #define DSHT_CUDA_OK(expr)                                   \
   do {                                                       \
     cudaError_t _e = (expr);                                 \

@@ -89,6 +89,21 @@ int dsht_execute(dsht_plan_t plan, const double* theta, const double* phi, const
 int dsht_rotate_back(dsht_plan_t plan, const double* alm_rot, const double* alm_add, double* alm_out,
                      void* stream);
 
+/* dsht_execute without any allocation.  No counterpart in the reference.  For callers that
+ * cannot allocate device memory when they run a transform: a framework that has reserved
+ * nearly all GPU memory for its own pool, a plugin host that forbids plugins to allocate,
+ * or a latency-critical loop that cannot afford the device-wide synchronisation of
+ * cudaMalloc/cudaFree.  Same arguments and results as dsht_execute (DEVICE pointers), but
+ * all scratch lives in one fixed device array of dsht_noalloc_scratch_bytes() = 64 MiB
+ * that every GPU loading this library holds until exit; problems whose workspace is larger
+ * (e.g. beyond Nl=256, Nx=512, N=1e5) return DSHT_ERR_NOMEM.  The first call on a device
+ * looks up the array's device address and should come before any stream capture.  All
+ * calls share the array (it keeps the last call's contents; what must start at zero is
+ * cleared), so calls that overlap on the GPU race and must be serialised by the caller. */
+int dsht_execute_noalloc(dsht_plan_t plan, const double* theta, const double* phi, const double* w,
+                         int64_t N, int mode, double* alm, void* stream);
+size_t dsht_noalloc_scratch_bytes(void);
+
 /* Same with HOST pointers (pageable or pinned); copies in, runs, copies alm out. */
 int dsht_execute_host(dsht_plan_t plan, const double* theta, const double* phi,
                       const double* w, int64_t N, int mode, double* alm_host);
