@@ -186,6 +186,8 @@ def main(argv=None):
     ap.add_argument("--cpu-sample", type=int, default=200_000)
     ap.add_argument("--ref-sample", type=int, default=200_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--no-fp64-compare", action="store_true")
     args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3)
     spec = WORKLOADS[args.workload]
@@ -220,62 +222,104 @@ def main(argv=None):
     stream = torch.cuda.current_stream(dev)
     sp = ct.c_void_p(stream.cuda_stream)
 
-    def step():
-        L.check(lib.dsht_execute(d._plan, L.ptr(thd), L.ptr(phd), L.ptr(wd), N, L.DSHT_MODE_CALL, L.ptr(alm),
+    def step(out):
+        L.check(lib.dsht_execute(d._plan, L.ptr(thd), L.ptr(phd), L.ptr(wd), N, L.DSHT_MODE_CALL, L.ptr(out),
                                  L.ptr(ws), ws.numel(), sp))
 
-    for _ in range(args.warmup):
-        step()
-    L.check(lib.dsht_profile_enable(d._plan, 1))
-    stage_ms = (ct.c_double * 5)()
-    calls = ct.c_int64()
-    L.check(lib.dsht_profile_read(d._plan, stage_ms, ct.byref(calls), 1))
+    def timed(precision, sample_clocks):
+        """W warm-up steps, then K timed steps between barriers; per-stage CUDA-event times."""
+        d.set_precision(precision)
+        for _ in range(args.warmup):
+            step(alm)
+        L.check(lib.dsht_profile_enable(d._plan, 1))
+        stage_ms = (ct.c_double * 5)()
+        calls = ct.c_int64()
+        L.check(lib.dsht_profile_read(d._plan, stage_ms, ct.byref(calls), 1))
+        clocks = ClockSampler(local) if sample_clocks else None
+        if clocks:
+            clocks.start()
+            time.sleep(0.3)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        launches0 = lib.dsht_launch_count()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+        ev[0].record(stream)
+        for k in range(args.steps):
+            step(alm)
+            ev[k + 1].record(stream)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        launches = lib.dsht_launch_count() - launches0
+        clk = clocks.stop() if clocks else None
+        per_step = np.array([ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)])
+        total_ms = ev[0].elapsed_time(ev[-1])
+        L.check(lib.dsht_profile_read(d._plan, stage_ms, ct.byref(calls), 1))
+        L.check(lib.dsht_profile_enable(d._plan, 0))
+        if world > 1:
+            t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total_ms = float(t.item())
+        ms_step = total_ms / args.steps
+        stages = {n: stage_ms[i] / max(calls.value, 1) for i, n in enumerate(L.STAGES)}
+        return {"ms_per_step": ms_step, "value": world * N * Nl / (ms_step / 1e3), "per_step": per_step,
+                "stages": stages, "launches": int(launches), "clocks": clk, "alm": alm.clone()}
 
-    clocks = ClockSampler(local)
-    clocks.start()
-    time.sleep(0.3)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    launches0 = lib.dsht_launch_count()
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
-    ev[0].record(stream)
-    for k in range(args.steps):
-        step()
-        ev[k + 1].record(stream)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    launches = lib.dsht_launch_count() - launches0
-    clk = clocks.stop()
-    per_step = np.array([ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)])
-    total_ms = ev[0].elapsed_time(ev[-1])
-    L.check(lib.dsht_profile_read(d._plan, stage_ms, ct.byref(calls), 1))
-    L.check(lib.dsht_profile_enable(d._plan, 0))
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    ms_step = total_ms / args.steps
-    value = world * N * Nl / (ms_step / 1e3)
+    main = timed(args.precision, sample_clocks=True)
+    other = None
+    if args.precision == "mixed" and not args.no_fp64_compare:
+        other = timed("fp64", sample_clocks=False)
+        d.set_precision(args.precision)
+    value, ms_step, per_step, stages = main["value"], main["ms_per_step"], main["per_step"], main["stages"]
+    launches, clk = main["launches"], main["clocks"]
+    max_rel_err = None
+    if other is not None:
+        ref = other["alm"]
+        max_rel_err = float((main["alm"] - ref).abs().max() / ref.abs().max())
 
-    # Dominant stage and its roofline.
-    stages = {n: stage_ms[i] / max(calls.value, 1) for i, n in enumerate(L.STAGES)}
+    # Roofline of every stage; the dominant one is reported.
     hbm_peak, bf16_peak, peak_src = measured_peaks()
+    C = 8
+    while C < (Nl + 15) // 16:
+        C *= 2
+
+    def stage_roof(name, ms):
+        if ms <= 0:
+            return None
+        if name == "contract":
+            alg = 16.0 * d.Nlm * Nx
+            a = alg / (ms * 1e-3) / 1e9
+            return {"kernel": "contract_fp64_kernel", "bound": "hbm", "achieved": a, "peak": hbm_peak,
+                    "unit": "GB/s", "frac": a / hbm_peak, "peak_source": peak_src,
+                    "algorithmic": "16 B of FP64 table per (l, m, node) per step"}
+        if name == "points":
+            alg = 64.0 * N
+            a = alg / (ms * 1e-3) / 1e9
+            return {"kernel": "count/scan/scatter (counting sort)", "bound": "hbm", "achieved": a,
+                    "peak": hbm_peak, "unit": "GB/s", "frac": a / hbm_peak, "peak_source": peak_src,
+                    "algorithmic": "24 B of inputs read + 40 B of sorted payload written per point"}
+        if name == "bin_sums" and args.precision == "mixed":
+            alg = 2.0 * 128 * (2 * C) * 6 * N
+            pk = 2 * bf16_peak
+            a = alg / (ms * 1e-3) / 1e12
+            return {"kernel": "bin_sums_tc_kernel (tcgen05 kind::i8)", "bound": "tensor", "achieved": a,
+                    "peak": pk, "unit": "TOP/s", "frac": a / pk,
+                    "peak_source": f"derived: 2 x {peak_src} bf16 (dense int8 rate is twice bf16 on B200)",
+                    "algorithmic": f"6 int8 slice products of a 128 x {2 * C} x P GEMM per piece, 2 op per MAC"}
+        if name == "bin_sums":
+            alg = 24.0 * N * Nl
+            a = alg / (ms * 1e-3) / 1e12
+            return {"kernel": "bin_sums_fp64_kernel", "bound": "fp64", "achieved": a, "peak": 40.0,
+                    "unit": "TFLOP/s", "frac": a / 40.0, "peak_source": "nominal (no measured FP64 figure)",
+                    "algorithmic": "24 flop per (point, m): 8 FMA sums + 4 FMA angle step"}
+        return None
+
+    roofs = {n: stage_roof(n, ms) for n, ms in stages.items()}
     top = max(stages, key=stages.get)
-    if top == "contract":
-        alg_bytes = 16.0 * d.Nlm * Nx
-        achieved = alg_bytes / (stages[top] * 1e-3) / 1e9
-        roof = {"kernel": "contract_fp64_kernel", "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
-                "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
-                "peak_source": peak_src, "algorithmic": "16 B of FP64 table per (l, m, node)"}
-    else:
-        alg_flops = 24.0 * N * Nl
-        peak = 40.0  # nominal B200 FP64 TFLOP/s; no measured FP64 figure exists on this pool
-        achieved = alg_flops / (stages[top] * 1e-3) / 1e12
-        roof = {"kernel": "bin_sums_fp64_kernel" if top == "bin_sums" else top, "bound": "fp64",
-                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
-                "peak_source": "nominal", "algorithmic": "24 flop per (point, m): 8 FMA sums + 4 FMA angle step"}
+    roof = dict(roofs[top] or {"kernel": top, "bound": None})
+    roof["traffic"] = None
+    roof["stage_ms"] = stages[top]
 
     # End to end through the host-pointer C ABI entry, pinned host buffers.
     e2e = None
@@ -320,14 +364,22 @@ def main(argv=None):
         line = {
             "metric": "points*ell/s", "value": value, "unit": "points*ell/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": spec["name"], "Nl": Nl, "Nx": Nx, "N": N, "maps": 1, "precision": "fp64",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "i8 tensor sums + f64" if args.precision == "mixed" else "f64", "data": "synthetic",
+            "config": {"workload": spec["name"], "Nl": Nl, "Nx": Nx, "N": N, "maps": 1,
+                       "precision": args.precision,
                        "l2": "inputs (240 MB) and tables (17 GB) exceed L2 every step",
                        "parallelism": f"replicas x{world}"},
             "p50_ms": float(np.percentile(per_step, 50)), "p99_ms": float(np.percentile(per_step, 99)),
-            "stages_ms": stages, "plan_build_s": t_plan, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+            "stages_ms": stages, "plan_build_s": t_plan, "roofline": roof,
+            "stage_rooflines": {k: v for k, v in roofs.items() if v}, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(launches), "clocks": clk,
         }
+        if other is not None:
+            line["fp64_plain"] = {"value": other["value"], "ms_per_step": other["ms_per_step"],
+                                  "stages_ms": other["stages"]}
+            line["speedup_vs_fp64_plain"] = value / other["value"]
+            line["max_rel_err_vs_fp64"] = max_rel_err
         print(json.dumps(line), flush=True)
     return 0
 

@@ -23,6 +23,9 @@ DSHT_ERR_POLAR_RANGE = 6
 DSHT_MODE_CALL = 0
 DSHT_MODE_BASIC = 1
 
+DSHT_PREC_FP64 = 0
+DSHT_PREC_MIXED = 1
+
 STAGES = ("points", "bin_sums", "fold", "contract", "rotate")
 
 # Every symbol include/dsht.h declares, with (restype, argtypes).
@@ -46,9 +49,12 @@ SIGNATURES = {
     "dsht_make_table": (ct.c_int, [ct.c_int, ct.c_int, ct.c_double, _dp, _dp]),
     "dsht_do_transform": (ct.c_int, [ct.c_int, ct.c_int, ct.c_double, _dp, _dp, ct.c_int, _dp, _dp, _dp, _dp,
                                      _dp]),
+    "dsht_set_precision": (ct.c_int, [_vp, ct.c_int]),
+    "dsht_get_precision": (ct.c_int, [_vp, ct.POINTER(ct.c_int)]),
     "dsht_profile_enable": (ct.c_int, [_vp, ct.c_int]),
     "dsht_profile_read": (ct.c_int, [_vp, _dp, ct.POINTER(ct.c_int64), ct.c_int]),
     "dsht_launch_count": (ct.c_int64, []),
+    "dsht_mixed_min_points": (ct.c_int64, []),
     "dsht_last_error": (ct.c_char_p, []),
     "dsht_version": (ct.c_char_p, []),
 }

@@ -40,7 +40,7 @@ static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 int default_piece_max(const Geometry& g, int64_t N) {
   int64_t p = (N + 2047) / 2048;
   if (p < 512) p = 512;
-  if (p > 4096) p = 4096;
+  if (p > 2048) p = 2048;
   return (int)p;
 }
 
@@ -58,7 +58,8 @@ size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* ba
   Workspace w{};
   w.key = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * n));
   w.idx_sorted = nullptr;
-  w.pay = reinterpret_cast<double*>(take(sizeof(double) * 5 * n));
+  w.rec = reinterpret_cast<double*>(take(sizeof(double) * 3 * n));
+  w.pay = reinterpret_cast<double*>(take(sizeof(double) * 6 * n));
   w.count = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * (g.nkeys + 1)));
   w.offset = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * (g.nkeys + 1)));
   w.cursor = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * (g.nkeys + 1)));
@@ -105,9 +106,17 @@ int run_pipeline(dsht_plan_s* p, const double* theta, const double* phi, const d
   mark(0);
   launch_points(g, theta, phi, w, N, mode, ws, s);
   mark(1);
-  launch_bin_sums_fp64(g, ws, s);
+  Workspace w2 = ws;
+  if (p->precision == DSHT_PREC_MIXED && N >= DSHT_MIXED_MIN_POINTS) {
+    int rc = launch_bin_sums_tc(g, ws, s);
+    if (rc) return rc;
+    w2.partial_f32 = 1;
+  } else {
+    launch_bin_sums_fp64(g, ws, s);
+    w2.partial_f32 = 0;
+  }
   mark(2);
-  launch_fold(g, ws, s);
+  launch_fold(g, w2, s);
   mark(3);
   launch_contract_fp64(g, p->Yv, p->Yd, ws, s);
   mark(4);
@@ -132,6 +141,8 @@ void collect_profile(dsht_plan_s* p) {
 }
 
 int flags_to_status(unsigned f, int mode) {
+  if (f & kFlagTimeout)
+    return set_error(DSHT_ERR_CUDA, "a tensor-core pipeline wait timed out; results are invalid");
   if (f & kFlagPolarRange)
     return set_error(DSHT_ERR_POLAR_RANGE,
                      "theta must be in [ACos[xmax],ACos[-xmax]). (a polar point is still polar after the "
@@ -209,6 +220,23 @@ int dsht_plan_destroy(dsht_plan_t p) {
   return DSHT_OK;
 }
 
+int dsht_set_precision(dsht_plan_t p, int precision) {
+  if (!p) return set_error(DSHT_ERR_INVALID, "plan is NULL");
+  if (precision != DSHT_PREC_FP64 && precision != DSHT_PREC_MIXED)
+    return set_error(DSHT_ERR_INVALID, "unknown precision %d", precision);
+  if (precision == DSHT_PREC_MIXED && p->g.Nl > 2048)
+    return set_error(DSHT_ERR_INVALID, "mixed precision supports Nl <= 2048 (Nl=%d)", p->g.Nl);
+  std::lock_guard<std::mutex> lock(p->mu);
+  p->precision = precision;
+  return DSHT_OK;
+}
+
+int dsht_get_precision(dsht_plan_t p, int* precision) {
+  if (!p || !precision) return set_error(DSHT_ERR_INVALID, "invalid arguments");
+  *precision = p->precision;
+  return DSHT_OK;
+}
+
 int dsht_profile_enable(dsht_plan_t p, int enable) {
   if (!p) return set_error(DSHT_ERR_INVALID, "plan is NULL");
   std::lock_guard<std::mutex> lock(p->mu);
@@ -232,6 +260,8 @@ int dsht_profile_read(dsht_plan_t p, double* ms, int64_t* calls, int reset) {
 }
 
 int64_t dsht_launch_count(void) { return g_launches.load(); }
+
+int64_t dsht_mixed_min_points(void) { return DSHT_MIXED_MIN_POINTS; }
 
 int dsht_plan_info(dsht_plan_t p, int* Nl, int* Nx, double* xmax, int64_t* Nlm) {
   if (!p) return set_error(DSHT_ERR_INVALID, "plan is NULL");

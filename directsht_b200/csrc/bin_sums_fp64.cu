@@ -8,7 +8,8 @@
 // atomics: the piece's partial sums are written once, coalesced.  cos/sin(m phi) come
 // from an angle-addition recurrence in registers: per point the thread starts from
 // e^{i m0 phi} = T2[t/16] * T1[t%16] (two small power tables per point staged in shared
-// memory) and steps by e^{i phi} 7 times.  Compute bound on the FP64 pipe:
+// memory, built from cos/sin of phi by squaring) and steps by e^{i phi} 7 times.
+// Compute bound on the FP64 pipe:
 // 12 DFMA per (point, m).
 #include "dsht_internal.cuh"
 
@@ -41,12 +42,6 @@ bin_sums_fp64_kernel(int Nl, int64_t N, const double* __restrict__ pay, const in
   const int tid = threadIdx.x;
   const int mblk = blockIdx.y;
   const int m0 = mblk * kMBlock + kMPerThread * tid;
-  const double* phi = pay;
-  const double* g0 = pay + N;
-  const double* g1 = pay + 2 * N;
-  const double* g2 = pay + 3 * N;
-  const double* g3 = pay + 4 * N;
-
   for (int piece = blockIdx.x; piece < npieces; piece += gridDim.x) {
     const int64_t start = piece_start[piece];
     const int len = piece_len[piece];
@@ -64,11 +59,12 @@ bin_sums_fp64_kernel(int Nl, int64_t N, const double* __restrict__ pay, const in
         const int p = tid >> 1, half = tid & 1;
         if (p < np) {
           const int64_t i = start + base + p;
-          const double ph = phi[i];
+          const double* rp = pay + 6 * i;
+          const cplx e1 = {rp[0], rp[1]};
+          cplx e8 = cmul(e1, e1);
+          e8 = cmul(e8, e8);
+          e8 = cmul(e8, e8);
           if (half == 0) {
-            double s, c;
-            sincos(8.0 * ph, &s, &c);
-            const cplx e8 = {c, s};
             cplx z = {1.0, 0.0};
             sT1[p][0] = z;
 #pragma unroll
@@ -77,26 +73,22 @@ bin_sums_fp64_kernel(int Nl, int64_t N, const double* __restrict__ pay, const in
               sT1[p][a] = z;
             }
           } else {
-            double s, c;
-            sincos(128.0 * ph, &s, &c);
-            const cplx e128 = {c, s};
+            cplx e128 = e8;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) e128 = cmul(e128, e128);
             cplx z = {1.0, 0.0};
-            if (mblk > 0) {
-              sincos((double)(mblk * kMBlock) * ph, &s, &c);
-              z = {c, s};
-            }
+            for (int k = 0; k < mblk * 8; ++k) z = cmul(z, e128);  // e^{i 1024 mblk phi}
             sT2[p][0] = z;
 #pragma unroll
             for (int b = 1; b < 8; ++b) {
               z = cmul(z, e128);
               sT2[p][b] = z;
             }
-            sincos(ph, &s, &c);
-            sE1[p] = {c, s};
-            sG[p][0] = g0[i];
-            sG[p][1] = g1[i];
-            sG[p][2] = g2[i];
-            sG[p][3] = g3[i];
+            sE1[p] = e1;
+            sG[p][0] = rp[2];
+            sG[p][1] = rp[3];
+            sG[p][2] = rp[4];
+            sG[p][3] = rp[5];
           }
         }
       }

@@ -3,7 +3,8 @@
 // Data layout in HBM (Nlm = Nl(Nl+1)/2, rows in Healpy order m(2Nl-1-m)/2 + l):
 //   tables   Yv, Yd      double [Nlm][Nx]          (sht/sht.py:50-56 layout, numpy path)
 //   points   key         uint32 [N]                set*(Nx-1) + bin, or DSHT_KEY_DROP
-//            sorted      double [5][N]             (phi, w h0, w h1, w h2, w h3) by key
+//            record      double [N][3]             (cos phi, sin phi, t) in input order
+//            sorted      double [N][6]             (cos phi, sin phi, w h0..w h3) by key
 //   pieces   <= 1 bin each, <= piece_max points    (key, start, len)
 //   partial  double [piece][8][Nl]                 (k, re/im) bin sums for every m
 //   fold     double [Nl][4 q][Nx][4]               q = {equ even, equ odd, pol even, pol odd}
@@ -27,6 +28,7 @@ constexpr int kSets = 4;
 constexpr unsigned kFlagThetaRange = 1u;   // basic_sht assertion (sht/sht.py:171-172)
 constexpr unsigned kFlagPolarRange = 2u;   // rotated polar point still outside (-xmax, xmax)
 constexpr unsigned kFlagHasPolar = 4u;     // at least one point went through the rotation
+constexpr unsigned kFlagTimeout = 8u;      // a bounded wait in a tensor-core kernel gave up
 
 struct Geometry {
   int Nl, Nx;
@@ -43,7 +45,8 @@ struct Geometry {
 struct Workspace {
   uint32_t* key;        // [N]
   uint32_t* idx_sorted; // [N] original index of each sorted slot (unused by the fused path)
-  double* pay;          // [5][N]
+  double* rec;          // [N][3]
+  double* pay;          // [N][6]
   uint32_t* count;      // [nkeys + 1]
   uint32_t* offset;     // [nkeys + 1]
   uint32_t* cursor;     // [nkeys]
@@ -59,6 +62,7 @@ struct Workspace {
   double* alm_equ;      // [Nlm][2]
   double* alm_pol;      // [Nlm][2]
   int64_t npts;         // N, the stride of pay
+  int partial_f32;      // partial sums stored as float (tensor-core path) instead of double
   int64_t pmax;
   int piece_max;
   size_t bytes;
@@ -72,6 +76,8 @@ void launch_tables(const Geometry& g, double* Yv, double* Yd, cudaStream_t s);
 void launch_points(const Geometry& g, const double* theta, const double* phi, const double* w,
                    int64_t N, int mode, const Workspace& ws, cudaStream_t s);
 void launch_bin_sums_fp64(const Geometry& g, const Workspace& ws, cudaStream_t s);
+int launch_bin_sums_tc(const Geometry& g, const Workspace& ws, cudaStream_t s);
+int tc_inner_factor(int Nl);
 void launch_fold(const Geometry& g, const Workspace& ws, cudaStream_t s);
 void launch_contract_fp64(const Geometry& g, const double* Yv, const double* Yd,
                           const Workspace& ws, cudaStream_t s);
@@ -100,6 +106,7 @@ struct dsht_plan_s {
   int64_t in_n = 0;
   double* alm = nullptr;  // [2 Nlm]
   unsigned* h_flags = nullptr;  // pinned
+  int precision = DSHT_PREC_FP64;
   // Stage timers.
   bool prof = false;
   cudaEvent_t ev[DSHT_STAGE_COUNT + 1] = {};

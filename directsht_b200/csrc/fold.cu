@@ -7,6 +7,7 @@
 // The x < 0 half enters with (-1)^(l-m) (sht/sht.py:279); rows with l-m even use
 // A+ + A-, odd rows A+ - A-, for the equatorial and the rotated polar sets.
 // Output fold[m][q][j] = (A re, A im, B re, B im), q = {equ even, equ odd, pol even, pol odd}.
+// Partial sums are FP64 (plain path) or FP32 (tensor-core path); they are added in FP64.
 #include "dsht_internal.cuh"
 
 namespace dsht {
@@ -14,9 +15,10 @@ namespace {
 
 constexpr int kFoldThreads = 128;
 
+template <typename T>
 __global__ void __launch_bounds__(kFoldThreads)
 fold_kernel(int Nl, int Nx, int nbins, double dx, const int* __restrict__ piece_first,
-            const double* __restrict__ partial, double* __restrict__ fold) {
+            const T* __restrict__ partial, double* __restrict__ fold) {
   const int j = blockIdx.x;
   const int m = blockIdx.y * blockDim.x + threadIdx.x;
   if (m >= Nl) return;
@@ -27,7 +29,7 @@ fold_kernel(int Nl, int Nx, int nbins, double dx, const int* __restrict__ piece_
     if (j < nbins) {  // bin j: its left node carries V0, V1
       const int key = s * nbins + j;
       for (int p = piece_first[key]; p < piece_first[key + 1]; ++p) {
-        const double* v = partial + (size_t)p * 8 * Nl + m;
+        const T* v = partial + (size_t)p * 8 * Nl + m;
         ar += v[0];
         ai -= v[(size_t)Nl];
         br += v[(size_t)2 * Nl];
@@ -37,7 +39,7 @@ fold_kernel(int Nl, int Nx, int nbins, double dx, const int* __restrict__ piece_
     if (j >= 1) {  // bin j-1: its right node carries V2, V3
       const int key = s * nbins + j - 1;
       for (int p = piece_first[key]; p < piece_first[key + 1]; ++p) {
-        const double* v = partial + (size_t)p * 8 * Nl + m;
+        const T* v = partial + (size_t)p * 8 * Nl + m;
         ar += v[(size_t)4 * Nl];
         ai -= v[(size_t)5 * Nl];
         br += v[(size_t)6 * Nl];
@@ -77,7 +79,12 @@ int contract_tile();
 
 void launch_fold(const Geometry& g, const Workspace& ws, cudaStream_t s) {
   dim3 grid(g.Nx, (g.Nl + kFoldThreads - 1) / kFoldThreads);
-  fold_kernel<<<grid, kFoldThreads, 0, s>>>(g.Nl, g.Nx, g.nbins, g.dx, ws.piece_first, ws.partial, ws.fold);
+  if (ws.partial_f32)
+    fold_kernel<float><<<grid, kFoldThreads, 0, s>>>(g.Nl, g.Nx, g.nbins, g.dx, ws.piece_first,
+                                                    reinterpret_cast<const float*>(ws.partial), ws.fold);
+  else
+    fold_kernel<double><<<grid, kFoldThreads, 0, s>>>(g.Nl, g.Nx, g.nbins, g.dx, ws.piece_first, ws.partial,
+                                                     ws.fold);
   count_launches(1);
   const int tile = contract_tile();
   const int ntile = (g.Nx + tile - 1) / tile;

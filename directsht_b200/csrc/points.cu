@@ -3,14 +3,16 @@
 // Each point goes to one of four sets: equatorial with cos(theta) >= 0 / < 0, or polar
 // (|cos theta| >= xmax, sht/sht.py:128-130) rotated by +90 deg about y and split by the
 // sign of the rotated cos.  The bin is numpy's digitize(|x|, x_nodes) - 1 (right-open,
-// sht/sht.py:212) and t = (|x| - x_j)/dx (sht/sht.py:221); the payload is phi and
-// w * {(2t+1)(1-t)^2, t(1-t)^2, t^2(3-2t), t^2(t-1)} (sht/sht.py:239-240).
+// sht/sht.py:212) and t = (|x| - x_j)/dx (sht/sht.py:221); the payload is cos phi, sin phi
+// and w * {(2t+1)(1-t)^2, t(1-t)^2, t^2(3-2t), t^2(t-1)} (sht/sht.py:239-240).
 //
-// Sort: key = set*(Nx-1) + bin.  count (shared-memory histogram per block, flushed with
-// one global add per live key), one-block exclusive scan that also cuts every key into
-// pieces of at most piece_max points, then a scatter in which each block reserves a
-// contiguous range per key with one global add.  HBM bound: 24 B read twice and 44 B
-// written per point.
+// Sort: key = set*(Nx-1) + bin.  The count pass classifies every point once (key, cos phi,
+// sin phi, t in input order) and histograms the keys in shared memory (one global add per
+// live key and block); a one-block exclusive scan cuts every key into pieces of at most
+// piece_max points; the scatter pass reserves a contiguous range per key and block with
+// one global add and writes each point's 48-byte record (cos phi, sin phi, w h0..w h3) to
+// its sorted slot.  HBM bound: about 16 B read + 28 B written (count), 36 B read + 48 B
+// written (scatter) per point.
 #include "dsht_internal.cuh"
 
 namespace dsht {
@@ -21,16 +23,19 @@ constexpr int kScatterTile = 16384;  // points per block in the scatter pass
 
 struct PointOut {
   uint32_t key;
-  double phi;
+  double cphi, sphi;  // cos, sin of the (rotated) azimuth
   double t;
   unsigned flag;
 };
 
+// kAngles: also compute cos/sin of the azimuth (the count pass only needs the key).
+template <bool kAngles>
 __device__ __forceinline__ PointOut classify(const Geometry& g, int mode, double th, double ph) {
   PointOut o;
   o.flag = 0;
   o.key = DSHT_KEY_DROP;
-  o.phi = ph;
+  o.cphi = 1.0;
+  o.sphi = 0.0;
   o.t = 0.0;
   const double c = cos(th);
   double x;        // signed x used for binning
@@ -44,9 +49,12 @@ __device__ __forceinline__ PointOut classify(const Geometry& g, int mode, double
       const double st = sin(th);
       const double nx = st * cp, ny = st * sp;
       const double xr = -nx;
-      double pr = atan2(ny, c);
-      if (pr < 0.0) pr += 2.0 * M_PI;
-      o.phi = pr;
+      // azimuth of the rotated point: atan2(ny, c), kept as its cosine and sine
+      const double rho = sqrt(ny * ny + c * c);
+      if (rho > 0.0) {
+        o.cphi = c / rho;
+        o.sphi = ny / rho;
+      }
       const double tr = acos(fmin(fmax(xr, -1.0), 1.0));
       if (!(tr > g.acos_xmax && tr < g.acos_mxmax)) {
         o.flag = kFlagPolarRange;
@@ -62,6 +70,7 @@ __device__ __forceinline__ PointOut classify(const Geometry& g, int mode, double
       }
       x = c;
       set = 0;
+      if (kAngles) sincos(ph, &o.sphi, &o.cphi);
     } else {
       return o;  // NaN theta: in neither set (sht/sht.py:129-130)
     }
@@ -72,6 +81,7 @@ __device__ __forceinline__ PointOut classify(const Geometry& g, int mode, double
     }
     x = c;
     set = 0;
+    if (kAngles) sincos(ph, &o.sphi, &o.cphi);
   }
   if (!(x >= 0.0)) set += 1;          // x < 0 half (sht/sht.py:193)
   const double ax = fabs(x);
@@ -92,7 +102,7 @@ __device__ __forceinline__ PointOut classify(const Geometry& g, int mode, double
 
 __global__ void __launch_bounds__(kPointThreads)
 count_kernel(Geometry g, int mode, const double* __restrict__ theta, const double* __restrict__ phi,
-             int64_t N, uint32_t* __restrict__ keys, uint32_t* __restrict__ count,
+             int64_t N, uint32_t* __restrict__ keys, double* __restrict__ rec, uint32_t* __restrict__ count,
              unsigned* __restrict__ flags) {
   extern __shared__ uint32_t hist[];
   for (int k = threadIdx.x; k < g.nkeys; k += blockDim.x) hist[k] = 0;
@@ -100,8 +110,11 @@ count_kernel(Geometry g, int mode, const double* __restrict__ theta, const doubl
   unsigned fl = 0;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
-    PointOut o = classify(g, mode, theta[i], phi[i]);
+    PointOut o = classify<true>(g, mode, theta[i], phi[i]);
     keys[i] = o.key;
+    rec[3 * i] = o.cphi;
+    rec[3 * i + 1] = o.sphi;
+    rec[3 * i + 2] = o.t;
     fl |= o.flag;
     if (o.key != DSHT_KEY_DROP) atomicAdd(&hist[o.key], 1u);
   }
@@ -187,9 +200,8 @@ scan_kernel(int nkeys, int nbins, int piece_max, int64_t pmax, const uint32_t* _
 }
 
 __global__ void __launch_bounds__(kPointThreads)
-scatter_kernel(Geometry g, int mode, const double* __restrict__ theta, const double* __restrict__ phi,
-               const double* __restrict__ w, int64_t N, const uint32_t* __restrict__ keys,
-               uint32_t* __restrict__ cursor, double* __restrict__ pay) {
+scatter_kernel(Geometry g, const double* __restrict__ w, int64_t N, const uint32_t* __restrict__ keys,
+               const double* __restrict__ rec, uint32_t* __restrict__ cursor, double* __restrict__ pay) {
   extern __shared__ uint32_t loc[];  // [nkeys] local counts, then local bases
   const int64_t lo = (int64_t)blockIdx.x * kScatterTile;
   const int64_t hi = min(lo + (int64_t)kScatterTile, N);
@@ -209,17 +221,17 @@ scatter_kernel(Geometry g, int mode, const double* __restrict__ theta, const dou
     const uint32_t k = keys[i];
     if (k == DSHT_KEY_DROP) continue;
     const uint32_t pos = atomicAdd(&loc[k], 1u);
-    PointOut o = classify(g, mode, theta[i], phi[i]);
     // Same rounding order as the numpy expressions of sht/sht.py:239-240.
-    const double t = o.t, wi = w[i];
+    const double t = rec[3 * i + 2], wi = w[i];
     const double omt = __dadd_rn(1.0, -t);
     const double omt2 = __dmul_rn(omt, omt);
     const double t2 = __dmul_rn(t, t);
-    pay[pos] = o.phi;
-    pay[(size_t)N + pos] = __dmul_rn(wi, __dmul_rn(__dadd_rn(__dmul_rn(2.0, t), 1.0), omt2));
-    pay[2 * (size_t)N + pos] = __dmul_rn(wi, __dmul_rn(t, omt2));
-    pay[3 * (size_t)N + pos] = __dmul_rn(wi, __dmul_rn(t2, __dadd_rn(3.0, -__dmul_rn(2.0, t))));
-    pay[4 * (size_t)N + pos] = __dmul_rn(wi, __dmul_rn(t2, __dadd_rn(t, -1.0)));
+    double2* out = reinterpret_cast<double2*>(pay + (size_t)6 * pos);
+    out[0] = make_double2(rec[3 * i], rec[3 * i + 1]);
+    out[1] = make_double2(__dmul_rn(wi, __dmul_rn(__dadd_rn(__dmul_rn(2.0, t), 1.0), omt2)),
+                          __dmul_rn(wi, __dmul_rn(t, omt2)));
+    out[2] = make_double2(__dmul_rn(wi, __dmul_rn(t2, __dadd_rn(3.0, -__dmul_rn(2.0, t)))),
+                          __dmul_rn(wi, __dmul_rn(t2, __dadd_rn(t, -1.0))));
   }
 }
 
@@ -235,7 +247,7 @@ void launch_points(const Geometry& g, const double* theta, const double* phi, co
   if (N > 0) {
     int64_t blocks = (N + kPointThreads * 8 - 1) / (kPointThreads * 8);
     if (blocks > 148 * 8) blocks = 148 * 8;
-    count_kernel<<<(unsigned)blocks, kPointThreads, hsmem, s>>>(g, mode, theta, phi, N, ws.key,
+    count_kernel<<<(unsigned)blocks, kPointThreads, hsmem, s>>>(g, mode, theta, phi, N, ws.key, ws.rec,
                                                                ws.count, ws.flags);
     count_launches(1);
   }
@@ -245,8 +257,8 @@ void launch_points(const Geometry& g, const double* theta, const double* phi, co
   count_launches(1);
   if (N > 0) {
     const int64_t blocks = (N + kScatterTile - 1) / kScatterTile;
-    scatter_kernel<<<(unsigned)blocks, kPointThreads, hsmem, s>>>(g, mode, theta, phi, w, N, ws.key,
-                                                                 ws.cursor, ws.pay);
+    scatter_kernel<<<(unsigned)blocks, kPointThreads, hsmem, s>>>(g, w, N, ws.key, ws.rec, ws.cursor,
+                                                                 ws.pay);
     count_launches(1);
   }
 }

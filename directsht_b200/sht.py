@@ -28,7 +28,8 @@ def _as_device_f64(a, device) -> torch.Tensor:
 class DirectSHT:
     """Brute-force spherical harmonic transforms on a B200 (``sht/sht.py:30``)."""
 
-    def __init__(self, Nell, Nx, xmax=0.75, dflt_type="float64", null_unphysical=True, device=None):
+    def __init__(self, Nell, Nx, xmax=0.75, dflt_type="float64", null_unphysical=True, device=None,
+                 precision="fp64"):
         """Build the FP64 Ylm/dYlm tables on the GPU (``sht/sht.py:32-56``).
 
         :param Nell: number of ells (and m's).
@@ -37,6 +38,8 @@ class DirectSHT:
         :param dflt_type: dtype of the host copy of the x grid (the tables are FP64).
         :param null_unphysical: accepted for compatibility; rows l < m are never stored.
         :param device: CUDA device (default: the current one).
+        :param precision: "fp64" (FP64 per-bin sums, agrees with the reference to ~1e-15) or
+            "mixed" (tensor-core per-bin sums on fp16 hi/lo operands, <= 1e-7 x max|alm|).
         """
         self._lib = L.load()
         if not torch.cuda.is_available():
@@ -51,6 +54,8 @@ class DirectSHT:
         self._plan = ct.c_void_p()
         with torch.cuda.device(self.device):
             L.check(self._lib.dsht_plan_create(self.Nell, self.Nx, self.xmax, 0, ct.byref(self._plan)))
+        self.precision = None
+        self.set_precision(precision)
         self._Yv = None
         self._Yd = None
         self.verbose_timing = None
@@ -64,6 +69,14 @@ class DirectSHT:
             except Exception:
                 pass
             self._plan = None
+
+    def set_precision(self, precision):
+        """Switch the per-bin sums between "fp64" and "mixed" (tables stay FP64)."""
+        code = {"fp64": L.DSHT_PREC_FP64, "mixed": L.DSHT_PREC_MIXED}.get(precision)
+        if code is None:
+            raise ValueError(f"precision must be 'fp64' or 'mixed', not {precision!r}")
+        L.check(self._lib.dsht_set_precision(self._plan, code))
+        self.precision = precision
 
     # -- tables ---------------------------------------------------------------------
     def indx(self, ell, m):

@@ -57,6 +57,25 @@ enum {
   DSHT_PLAN_DEFAULT = 0
 };
 
+/* Arithmetic of the per-bin sums (the scatter) of a plan.
+ *   DSHT_PREC_FP64  : FP64 CUDA-core sums; agrees with the reference's numpy path to
+ *                     about 1e-15 (tested at <= 1e-12 x max|alm|).
+ *   DSHT_PREC_MIXED : tcgen05 tensor-core sums: operands quantised to 21-bit fixed point,
+ *                     split in three int8 slices, six slice products accumulated exactly in
+ *                     S32 and combined in FP64 (unbiased, about 1.3e-7 rms per product;
+ *                     tested at <= 1e-7 x max|alm|); Nl <= 2048.  Transforms of fewer than
+ *                     DSHT_MIXED_MIN_POINTS points use the FP64 sums: they cost little, and
+ *                     the quantisation error of a handful of points does not average down.
+ * The tables, the contraction and the rotation stay FP64 in both. */
+enum {
+  DSHT_PREC_FP64 = 0,
+  DSHT_PREC_MIXED = 1
+};
+#define DSHT_MIXED_MIN_POINTS 1024
+int64_t dsht_mixed_min_points(void);
+int dsht_set_precision(dsht_plan_t plan, int precision);
+int dsht_get_precision(dsht_plan_t plan, int* precision);
+
 /* Build the x grid and the FP64 Ylm/dYlm tables on the current CUDA device.
  * Replaces DirectSHT.__init__ (sht/sht.py:32-56). Nl >= 1, Nx >= 2, 0 < xmax < 1. */
 int dsht_plan_create(int Nl, int Nx, double xmax, int flags, dsht_plan_t* plan);
