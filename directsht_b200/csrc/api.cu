@@ -72,6 +72,7 @@ size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* ba
   w.partial = reinterpret_cast<double*>(take(sizeof(double) * 8 * (size_t)g.Nl * pmax));
   w.fold = reinterpret_cast<double*>(take(sizeof(double) * 16 * (size_t)g.Nl * g.Nx));
   w.tile_live = reinterpret_cast<uint8_t*>(take(2 * (size_t)ntile));
+  w.tile_live2 = reinterpret_cast<uint8_t*>(take(2 * (size_t)((g.Nx + 255) / 256)));
   w.alm_equ = reinterpret_cast<double*>(take(sizeof(double) * 2 * (size_t)g.Nlm));
   w.alm_pol = reinterpret_cast<double*>(take(sizeof(double) * 2 * (size_t)g.Nlm));
   w.npts = n;
@@ -107,7 +108,9 @@ int run_pipeline(dsht_plan_s* p, const double* theta, const double* phi, const d
   launch_points(g, theta, phi, w, N, mode, ws, s);
   mark(1);
   Workspace w2 = ws;
-  if (p->precision == DSHT_PREC_MIXED && N >= DSHT_MIXED_MIN_POINTS) {
+  // Small transforms run the FP64 stages even on a mixed-precision plan.
+  const bool mixed = p->precision == DSHT_PREC_MIXED && N >= DSHT_MIXED_MIN_POINTS;
+  if (mixed) {
     int rc = launch_bin_sums_tc(g, ws, s);
     if (rc) return rc;
     w2.partial_f32 = 1;
@@ -118,7 +121,12 @@ int run_pipeline(dsht_plan_s* p, const double* theta, const double* phi, const d
   mark(2);
   launch_fold(g, w2, s);
   mark(3);
-  launch_contract_fp64(g, p->Yv, p->Yd, ws, s);
+  if (mixed && p->tm32)
+    launch_contract_stream<float>(g, p->tmYv32, p->tmYd32, ws, s);
+  else if (p->tm64)
+    launch_contract_stream<double>(g, p->tmYv, p->tmYd, ws, s);
+  else
+    launch_contract_fp64(g, p->Yv, p->Yd, ws, s);
   mark(4);
   if (mode == DSHT_MODE_CALL) {
     launch_rotate_back(g, ws.alm_pol, ws.alm_equ, alm, ws.flags, s);
@@ -202,6 +210,10 @@ int dsht_plan_create(int Nl, int Nx, double xmax, int flags, dsht_plan_t* plan) 
     delete p;
     return set_cuda_error(e, "table build", __FILE__, __LINE__);
   }
+  if (contract_stream_ok(p->g, sizeof(double)) &&
+      make_table_tmap(&p->tmYv, p->Yv, sizeof(double), Nx, p->g.Nlm) == DSHT_OK &&
+      make_table_tmap(&p->tmYd, p->Yd, sizeof(double), Nx, p->g.Nlm) == DSHT_OK)
+    p->tm64 = true;
   *plan = p;
   return DSHT_OK;
 }
@@ -212,6 +224,8 @@ int dsht_plan_destroy(dsht_plan_t p) {
     if (e) cudaEventDestroy(e);
   cudaFree(p->Yv);
   cudaFree(p->Yd);
+  cudaFree(p->Yv32);
+  cudaFree(p->Yd32);
   cudaFree(p->ws);
   cudaFree(p->in);
   cudaFree(p->alm);
@@ -227,6 +241,26 @@ int dsht_set_precision(dsht_plan_t p, int precision) {
   if (precision == DSHT_PREC_MIXED && p->g.Nl > 2048)
     return set_error(DSHT_ERR_INVALID, "mixed precision supports Nl <= 2048 (Nl=%d)", p->g.Nl);
   std::lock_guard<std::mutex> lock(p->mu);
+  if (precision == DSHT_PREC_MIXED && !p->Yv32) {
+    const size_t tb = sizeof(float) * (size_t)p->g.Nlm * p->g.Nx;
+    cudaError_t e = cudaMalloc(&p->Yv32, tb);
+    if (e == cudaSuccess) e = cudaMalloc(&p->Yd32, tb);
+    if (e != cudaSuccess) {  // no room for the FP32 copies: stream the FP64 tables instead
+      cudaFree(p->Yv32);
+      cudaFree(p->Yd32);
+      p->Yv32 = nullptr;
+      p->Yd32 = nullptr;
+      cudaGetLastError();
+      p->precision = precision;
+      return DSHT_OK;
+    }
+    launch_tables_to_f32(p->g, p->Yv, p->Yd, p->Yv32, p->Yd32, 0);
+    DSHT_CUDA_OK(cudaDeviceSynchronize());
+    if (contract_stream_ok(p->g, sizeof(float)) &&
+        make_table_tmap(&p->tmYv32, p->Yv32, sizeof(float), p->g.Nx, p->g.Nlm) == DSHT_OK &&
+        make_table_tmap(&p->tmYd32, p->Yd32, sizeof(float), p->g.Nx, p->g.Nlm) == DSHT_OK)
+      p->tm32 = true;
+  }
   p->precision = precision;
   return DSHT_OK;
 }

@@ -12,6 +12,7 @@
 //   alm      double2 [Nlm]                         complex128, Healpy order
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stddef.h>
@@ -58,7 +59,8 @@ struct Workspace {
   unsigned* flags;      // [1]
   double* partial;      // [pmax][8][Nl]
   double* fold;         // [Nl][4][Nx][4]
-  uint8_t* tile_live;   // [4 q][ntile]
+  uint8_t* tile_live;   // [2][ceil(Nx/128)] tiles of the fallback contraction
+  uint8_t* tile_live2;  // [2][ceil(Nx/256)] tiles of the streaming contraction
   double* alm_equ;      // [Nlm][2]
   double* alm_pol;      // [Nlm][2]
   int64_t npts;         // N, the stride of pay
@@ -81,6 +83,14 @@ int tc_inner_factor(int Nl);
 void launch_fold(const Geometry& g, const Workspace& ws, cudaStream_t s);
 void launch_contract_fp64(const Geometry& g, const double* Yv, const double* Yd,
                           const Workspace& ws, cudaStream_t s);
+bool contract_stream_ok(const Geometry& g, size_t elem_bytes);
+template <typename T>
+void launch_contract_stream(const Geometry& g, const CUtensorMap& tmv, const CUtensorMap& tmd, const Workspace& ws,
+                            cudaStream_t s);
+// 2D tensor map over a (Nlm x Nx) table for the streaming contraction's TMA loads.
+int make_table_tmap(CUtensorMap* tm, const void* base, size_t elem_bytes, int Nx, int64_t Nlm);
+void launch_tables_to_f32(const Geometry& g, const double* Yv, const double* Yd, float* Yv32, float* Yd32,
+                          cudaStream_t s);
 void launch_rotate_back(const Geometry& g, const double* alm_rot, const double* alm_add,
                         double* alm_out, const unsigned* flags, cudaStream_t s);
 
@@ -98,6 +108,10 @@ struct dsht_plan_s {
   int device = 0;
   double* Yv = nullptr;
   double* Yd = nullptr;
+  float* Yv32 = nullptr;  // FP32 copies streamed by mixed-precision executes (made on first use)
+  float* Yd32 = nullptr;
+  alignas(64) CUtensorMap tmYv, tmYd, tmYv32, tmYd32;
+  bool tm64 = false, tm32 = false;
   // Plan-owned buffers, grown on demand (used when the caller passes no workspace and by
   // the host-pointer entry points).
   void* ws = nullptr;

@@ -90,6 +90,9 @@ void launch_fold(const Geometry& g, const Workspace& ws, cudaStream_t s) {
   const int ntile = (g.Nx + tile - 1) / tile;
   tile_live_kernel<<<(ntile + 127) / 128, 128, 0, s>>>(g.nbins, ntile, tile, ws.count, ws.tile_live);
   count_launches(1);
+  const int ntile2 = (g.Nx + 255) / 256;
+  tile_live_kernel<<<(ntile2 + 127) / 128, 128, 0, s>>>(g.nbins, ntile2, 256, ws.count, ws.tile_live2);
+  count_launches(1);
 }
 
 }  // namespace dsht

@@ -109,7 +109,22 @@ table_kernel(int Nl, int Nx, double step, double* __restrict__ Yv, double* __res
   }
 }
 
+__global__ void to_f32_kernel(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
+                              float* __restrict__ a32, float* __restrict__ b32) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    a32[i] = (float)a[i];
+    b32[i] = (float)b[i];
+  }
+}
+
 }  // namespace
+
+void launch_tables_to_f32(const Geometry& g, const double* Yv, const double* Yd, float* Yv32, float* Yd32,
+                          cudaStream_t s) {
+  const int64_t n = g.Nlm * (int64_t)g.Nx;
+  to_f32_kernel<<<148 * 16, 256, 0, s>>>(n, Yv, Yd, Yv32, Yd32);
+  count_launches(1);
+}
 
 void launch_tables(const Geometry& g, double* Yv, double* Yd, cudaStream_t s) {
   const size_t smem = (size_t)g.Nl * sizeof(Coef) + (size_t)(g.Nl + 1) * sizeof(double);
