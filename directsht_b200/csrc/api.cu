@@ -118,13 +118,14 @@ int run_pipeline(dsht_plan_s* p, const double* theta, const double* phi, const d
     launch_bin_sums_fp64(g, ws, s);
     w2.partial_f32 = 0;
   }
+  w2.fold_f32 = (mixed && p->tm32) ? 1 : 0;
   mark(2);
   launch_fold(g, w2, s);
   mark(3);
   if (mixed && p->tm32)
-    launch_contract_stream<float>(g, p->tmYv32, p->tmYd32, ws, s);
+    launch_contract_stream(g, true, p->tmYv32, p->tmYd32, ws, s);
   else if (p->tm64)
-    launch_contract_stream<double>(g, p->tmYv, p->tmYd, ws, s);
+    launch_contract_stream(g, false, p->tmYv, p->tmYd, ws, s);
   else
     launch_contract_fp64(g, p->Yv, p->Yd, ws, s);
   mark(4);

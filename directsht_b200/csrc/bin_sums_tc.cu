@@ -116,7 +116,7 @@ struct Layout {
   static constexpr int kXchStride = 65;                       // floats per exchange row
   static constexpr int kAnchorBytes = kBK * (8 + (CH / 2 + 1) * 8 + 17 * 8 + 4 * 4);
   static constexpr int kXchBytes = kM * kXchStride * 4;
-  static constexpr int kUnion = kAnchorBytes > kXchBytes ? kAnchorBytes : kXchBytes;
+  static constexpr int kUnion = 2 * kAnchorBytes > kXchBytes ? 2 * kAnchorBytes : kXchBytes;
   static constexpr int kUnionOff = kStages * kStage;
   static constexpr int kMiscOff = kUnionOff + ((kUnion + 1023) / 1024) * 1024;
   static constexpr int kBytes = kMiscOff + 256 + 1024;        // + alignment slack
@@ -142,10 +142,12 @@ bin_sums_tc_kernel(int Nl, int Cf, int64_t Npay, const double* __restrict__ pay,
   // Row strides are padded by one entry so that lanes holding consecutive points hit
   // different banks.
   constexpr int kEcStride = CH / 2 + 1, kEaStride = 17;
-  float2* e1 = reinterpret_cast<float2*>(uni);                   // [64]          e^{i phi}
-  float2* ec = e1 + kBK;                                         // [64][CH/2+1]  e^{i (cbase + 2u) phi}
-  float2* ea = ec + kBK * kEcStride;                             // [64][17]      e^{i Cf a phi}
-  float* gk = reinterpret_cast<float*>(ea + kBK * kEaStride);    // [64][4]       g_k / scale
+  // Two anchor buffers (block b uses buffer b & 1), each laid out as
+  //   e1 [64] e^{i phi} | ec [64][CH/2+1] e^{i (cbase + 2u) phi} | ea [64][17] e^{i Cf a phi} | gk [64][4]
+  auto e1_of = [&](int buf) { return reinterpret_cast<float2*>(uni + buf * Lay::kAnchorBytes); };
+  auto ec_of = [&](int buf) { return e1_of(buf) + kBK; };
+  auto ea_of = [&](int buf) { return ec_of(buf) + kBK * kEcStride; };
+  auto gk_of = [&](int buf) { return reinterpret_cast<float*>(ea_of(buf) + kBK * kEaStride); };
   float* xch = reinterpret_cast<float*>(uni);                    // [128][65]   epilogue exchange
   uint8_t* misc = smem + Lay::kMiscOff;
   uint64_t* full = reinterpret_cast<uint64_t*>(misc);            // [S]
@@ -198,58 +200,75 @@ bin_sums_tc_kernel(int Nl, int Cf, int64_t Npay, const double* __restrict__ pay,
       if (!(scale > 0.0) || !isfinite(scale)) scale = 1.0;
       const double inv_scale = 1.0 / scale;
 
+      // ---- phase 1: anchors of block b (FP64 math, FP32 storage) into buffer b & 1 ----
+      // Threads 0-127: ec of point t%64, entries [h CH/4, (h+1) CH/4), h = t/64.
+      // Threads 128-255: ea of point t%64, entries [8h, 8h+8), and e1, g for h = 1.
+      // Lanes of a warp hold consecutive points (warp-uniform branches); every thread runs
+      // two interleaved recurrences so that FP64 latency overlaps.
+      auto phase1 = [&](int b) {
+        if (*abort_flag) return;
+        const int buf = b & 1;
+        float2* e1 = e1_of(buf);
+        float2* ec = ec_of(buf);
+        float2* ea = ea_of(buf);
+        float* gk = gk_of(buf);
+        const int np = min(kBK, len - b * kBK);
+        const int p = tid & 63, hq = (tid >> 6) & 1;
+        const bool is_ec = tid < 128;
+        if (p < np) {
+          const int64_t i = start + (int64_t)b * kBK + p;
+          const cplx z1 = {pay[6 * i], pay[6 * i + 1]};
+          if (is_ec) {
+            constexpr int H = CH / 8;  // entries per chain
+            const int u0 = hq * (CH / 4);
+            const cplx st = cmul(z1, z1);
+            cplx za = cpow(z1, cbase + 2 * u0);
+            cplx zb = cmul(za, cpow(st, H));
+            for (int u = 0; u < H; ++u) {
+              ec[p * kEcStride + u0 + u] = make_float2((float)za.re, (float)za.im);
+              ec[p * kEcStride + u0 + H + u] = make_float2((float)zb.re, (float)zb.im);
+              za = cmul(za, st);
+              zb = cmul(zb, st);
+            }
+          } else {
+            const int a0 = 8 * hq;
+            const cplx st = cpow(z1, Cf);
+            cplx za = cpow(st, a0);
+            cplx zb = cmul(za, cpow(st, 4));
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+              ea[p * kEaStride + a0 + a] = make_float2((float)za.re, (float)za.im);
+              ea[p * kEaStride + a0 + 4 + a] = make_float2((float)zb.re, (float)zb.im);
+              za = cmul(za, st);
+              zb = cmul(zb, st);
+            }
+            if (hq == 1) {
+              e1[p] = make_float2((float)z1.re, (float)z1.im);
+#pragma unroll
+              for (int k = 0; k < 4; ++k) gk[p * 4 + k] = (float)(pay[6 * i + 2 + k] * inv_scale);
+            }
+          }
+        } else {  // padding points contribute zero
+          if (is_ec) {
+            for (int u = hq * (CH / 4); u < (hq + 1) * (CH / 4); ++u) ec[p * kEcStride + u] = make_float2(0.f, 0.f);
+          } else {
+            for (int a = 8 * hq; a < 8 * hq + 8; ++a) ea[p * kEaStride + a] = make_float2(0.f, 0.f);
+            if (hq == 1) {
+              e1[p] = make_float2(0.f, 0.f);
+#pragma unroll
+              for (int k = 0; k < 4; ++k) gk[p * 4 + k] = 0.f;
+            }
+          }
+        }
+      };
+
+      phase1(0);
+      bar_producers();
       for (int b = 0; b < nblk; ++b) {
         const uint32_t g = blk_count + b;
         const int stage = g % S;
         const uint32_t use = g / S;
-        const int np = min(kBK, len - b * kBK);
-        // ---- phase 1: anchors (FP64 math, FP32 storage) --------------------------------
-        // Threads 0-127: ec of point t%64, entries [h CH/4, (h+1) CH/4), h = t/64.
-        // Threads 128-255: ea of point t%64, entries [8h, 8h+8), and e1, g for h = 1.
-        // Lanes of a warp hold consecutive points, so every branch is warp-uniform.
-        if (!*abort_flag) {
-          const int p = tid & 63, hq = (tid >> 6) & 1;
-          const bool is_ec = tid < 128;
-          if (p < np) {
-            const int64_t i = start + (int64_t)b * kBK + p;
-            const cplx z1 = {pay[6 * i], pay[6 * i + 1]};
-            if (is_ec) {
-              const int u0 = hq * (CH / 4);
-              cplx z = cpow(z1, cbase + 2 * u0);
-              const cplx st = cmul(z1, z1);
-              for (int u = u0; u < u0 + CH / 4; ++u) {
-                ec[p * kEcStride + u] = make_float2((float)z.re, (float)z.im);
-                z = cmul(z, st);
-              }
-            } else {
-              const int a0 = 8 * hq;
-              const cplx st = cpow(z1, Cf);
-              cplx z = cpow(st, a0);
-#pragma unroll
-              for (int a = 0; a < 8; ++a) {
-                ea[p * kEaStride + a0 + a] = make_float2((float)z.re, (float)z.im);
-                z = cmul(z, st);
-              }
-              if (hq == 1) {
-                e1[p] = make_float2((float)z1.re, (float)z1.im);
-#pragma unroll
-                for (int k = 0; k < 4; ++k) gk[p * 4 + k] = (float)(pay[6 * i + 2 + k] * inv_scale);
-              }
-            }
-          } else {  // padding points contribute zero
-            if (is_ec) {
-              for (int u = hq * (CH / 4); u < (hq + 1) * (CH / 4); ++u) ec[p * kEcStride + u] = make_float2(0.f, 0.f);
-            } else {
-              for (int a = 8 * hq; a < 8 * hq + 8; ++a) ea[p * kEaStride + a] = make_float2(0.f, 0.f);
-              if (hq == 1) {
-                e1[p] = make_float2(0.f, 0.f);
-#pragma unroll
-                for (int k = 0; k < 4; ++k) gk[p * 4 + k] = 0.f;
-              }
-            }
-          }
-        }
-        bar_producers();
+        if (b + 1 < nblk) phase1(b + 1);  // overlaps with the other warps' slicing
         // ---- wait until the MMAs that last read this stage are done -------------------
         if (use > 0 && !*abort_flag) {
           if (!tc::mbar_wait(&empty[stage], (use - 1) & 1, abort_flag)) {
@@ -257,9 +276,14 @@ bin_sums_tc_kernel(int Nl, int Cf, int64_t Npay, const double* __restrict__ pay,
             atomicOr(err_flags, kFlagTimeout);
           }
         }
-        // ---- phase 2: int8 slice tiles (FP32 + integer work only) ----------------------
+        // ---- phase 2: int8 slice tiles of block b from buffer b & 1 ---------------------
         uint8_t* st_base = smem + stage * Lay::kStage;
         if (!*abort_flag) {
+          const int buf = b & 1;
+          const float2* e1 = e1_of(buf);
+          const float2* ec = ec_of(buf);
+          const float2* ea = ea_of(buf);
+          const float* gk = gk_of(buf);
           constexpr int nB = 4 * (CH / 2);  // (16-point chunk h, c pair)
           constexpr int nA = 4 * 32;        // (16-point chunk h, k, a pair)
           for (int u = tid; u < nB + nA; u += kProducers) {
@@ -323,7 +347,7 @@ bin_sums_tc_kernel(int Nl, int Cf, int64_t Npay, const double* __restrict__ pay,
                   v2 = gg * z1.x;
                   v3 = gg * z1.y;
                 }
-                if (odd) {  // odd lanes write the odd row of the pair first (bank spread)
+                if (odd) {
                   const float t0 = v0, t1 = v1;
                   v0 = v2;
                   v1 = v3;
@@ -337,16 +361,22 @@ bin_sums_tc_kernel(int Nl, int Cf, int64_t Npay, const double* __restrict__ pay,
               }
 #pragma unroll
               for (int e = 0; e < 4; ++e) {
-                w[e][0][t] = pack4<2>(X[e][0], X[e][1], X[e][2], X[e][3]);
-                w[e][1][t] = pack4<1>(X[e][0], X[e][1], X[e][2], X[e][3]);
-                w[e][2][t] = pack4<0>(X[e][0], X[e][1], X[e][2], X[e][3]);
+                // 4 x 4 byte transpose: slice s of the four points is byte (2 - s) of X.
+                const uint32_t t0 = __byte_perm((uint32_t)X[e][0], (uint32_t)X[e][1], 0x5140);
+                const uint32_t t1 = __byte_perm((uint32_t)X[e][0], (uint32_t)X[e][1], 0x7362);
+                const uint32_t u0 = __byte_perm((uint32_t)X[e][2], (uint32_t)X[e][3], 0x5140);
+                const uint32_t u1 = __byte_perm((uint32_t)X[e][2], (uint32_t)X[e][3], 0x7362);
+                w[e][0][t] = __byte_perm(t1, u1, 0x5410);
+                w[e][1][t] = __byte_perm(t0, u0, 0x7632);
+                w[e][2][t] = __byte_perm(t0, u0, 0x5410);
               }
             }
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
+              uint8_t* rowp = base + rows[e] * 64 + ((h ^ ((rows[e] >> 1) & 3)) << 4);
 #pragma unroll
               for (int sl = 0; sl < 3; ++sl)
-                *tile_chunk(base + sl * tile_bytes, rows[e], h) =
+                *reinterpret_cast<uint4*>(rowp + sl * tile_bytes) =
                     make_uint4(w[e][sl][0], w[e][sl][1], w[e][sl][2], w[e][sl][3]);
             }
           }
@@ -354,7 +384,7 @@ bin_sums_tc_kernel(int Nl, int Cf, int64_t Npay, const double* __restrict__ pay,
         tc::fence_async_smem();
         __syncwarp();
         if (lane == 0) tc::mbar_arrive(&full[stage]);
-        bar_producers();  // the anchors of this block are no longer read
+        bar_producers();  // anchors of block b consumed, anchors of block b+1 complete
       }
 
       // ---- epilogue: warps 0-3 own TMEM lanes 0-127 -----------------------------------

@@ -4,15 +4,17 @@
 //   alm_equ[lm] = sum_j Yv[lm,j] A_q[m,j] + Yd[lm,j] B_q[m,j],  q = equ even/odd by (l-m)%2
 //   alm_pol[lm] = same with the polar q                     (sht/sht.py:266-279)
 //
-// Persistent CTAs walk work items (m, 16 consecutive rows l).  Warp 0 (one thread) is the
+// Persistent CTAs walk work items (m, R consecutive rows l).  Warp 0 (one thread) is the
 // producer: for every live tile of 256 nodes it issues one 2D tensor-map TMA load per table
-// (a 16-row x 256-node box of Yv and of Yd) and one bulk copy per fold row (4 q), all
-// completing on the stage's mbarrier.
-// Warps 1-8 consume: each owns two rows of equal parity and the 256 nodes of the tile
-// (8 per lane), accumulating in FP64; the fold values in shared memory feed both rows.
-// HBM bound: sizeof(T) x 2 bytes of table per (l, m, node).  T = double (FP64 plans) or
-// float (FP32 copy of the tables used by mixed-precision plans).
+// (an R-row x 256-node box of Yv and of Yd) and one bulk copy per fold row (4 q), all
+// completing on the stage's mbarrier.  Warps 1-8 consume: each owns R/8 rows of equal
+// parity and the 256 nodes of the tile (8 per lane); the fold values in shared memory
+// feed all its rows.  FP64 plans: double tables and fold, R = 16, FP64 FMAs.  Mixed plans:
+// FP32 tables and fold, R = 32, FP32 FMAs within a tile, FP64 sums across tiles.
+// HBM bound: 2 sizeof(T) bytes of table per (l, m, node).
 #include <cudaTypedefs.h>
+
+#include <type_traits>
 
 #include "dsht_internal.cuh"
 #include "tc_ptx.cuh"
@@ -20,7 +22,6 @@
 namespace dsht {
 namespace {
 
-constexpr int kRows = 16;
 constexpr int kTJ = 256;                  // nodes per tile
 constexpr int kConsumers = 8;             // warps 1..8
 constexpr int kThreads = 32 * (1 + kConsumers);
@@ -51,6 +52,7 @@ __device__ __forceinline__ void mbar_arrive_tx(uint64_t* bar, uint32_t bytes) {
 }
 
 // Work items in m order: group index g < groups(m) = ceil((Nl - m) / kRows).
+template <int kRows>
 __device__ __forceinline__ void item_of(int64_t item, int Nl, int* m_out, int* g_out) {
   // cumulative groups before m: G(m) = sum_{m' < m} ceil((Nl - m') / kRows); binary search.
   int lo = 0, hi = Nl;  // find largest m with G(m) <= item
@@ -71,20 +73,33 @@ __device__ __forceinline__ void item_of(int64_t item, int Nl, int* m_out, int* g
   *g_out = (int)(item - G(lo));
 }
 
-template <typename T>
+// FP64 plans: double tables, double4 fold entries, 16 rows per item, FP64 FMAs.
+// Mixed plans: float tables, float4 fold entries, 32 rows per item, FP32 FMAs within a
+// tile and FP64 accumulation across tiles.
+template <bool kMixed>
 struct StageLayout {
-  static constexpr int kTab = kRows * kTJ * sizeof(T);   // one of Yv, Yd
-  static constexpr int kFold = 4 * kTJ * 32;              // 4 q x kTJ x double4
+  using T = typename std::conditional<kMixed, float, double>::type;
+  using F4 = typename std::conditional<kMixed, float4, double4>::type;
+  static constexpr int kRows = kMixed ? 32 : 16;
+  static constexpr int kRowsPerWarp = kRows / 8;               // same parity, stride 2
+  static constexpr int kTab = kRows * kTJ * sizeof(T);         // one of Yv, Yd
+  static constexpr int kFold = 4 * kTJ * sizeof(F4);           // 4 q x kTJ
   static constexpr int kStage = 2 * kTab + kFold;
   static constexpr int kBytes = kStagesC * kStage + 128 + 128;
 };
 
-template <typename T>
+template <bool kMixed>
 __global__ void __launch_bounds__(kThreads, 1)
 contract_stream_kernel(int Nl, int Nx, int64_t nitems, const __grid_constant__ CUtensorMap tmv,
-                       const __grid_constant__ CUtensorMap tmd, const double* __restrict__ fold, const uint8_t* __restrict__ live, int ntile,
-                       double* __restrict__ alm_equ, double* __restrict__ alm_pol, unsigned* __restrict__ err) {
-  using L = StageLayout<T>;
+                       const __grid_constant__ CUtensorMap tmd, const void* __restrict__ fold_v,
+                       const uint8_t* __restrict__ live, int ntile, double* __restrict__ alm_equ,
+                       double* __restrict__ alm_pol, unsigned* __restrict__ err) {
+  using L = StageLayout<kMixed>;
+  using T = typename L::T;
+  using F4 = typename L::F4;
+  constexpr int kRows = L::kRows;
+  constexpr int RW = L::kRowsPerWarp;
+  const F4* fold = reinterpret_cast<const F4*>(fold_v);
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStagesC * L::kStage);
@@ -107,7 +122,7 @@ contract_stream_kernel(int Nl, int Nx, int64_t nitems, const __grid_constant__ C
       uint32_t n = 0;  // stages issued
       for (int64_t item = blockIdx.x; item < nitems && !*abort_flag; item += gridDim.x) {
         int m, g;
-        item_of(item, Nl, &m, &g);
+        item_of<kRows>(item, Nl, &m, &g);
         const int l0 = m + g * kRows;
         const int64_t row0 = hp_index(l0, m, Nl);
         for (int t = 0; t < ntile; ++t) {
@@ -122,32 +137,34 @@ contract_stream_kernel(int Nl, int Nx, int64_t nitems, const __grid_constant__ C
           const int j0 = t * kTJ;
           const int nj = min(kTJ, Nx - j0);
           uint8_t* st = smem + s * L::kStage;
-          const uint32_t fold_bytes = nj * 32;
+          const uint32_t fold_bytes = nj * sizeof(F4);
           // The table boxes always transfer kRows x kTJ elements (zero fill out of range).
           mbar_arrive_tx(&full[s], 2u * L::kTab + 4u * fold_bytes);
           tma_load_2d(st, &tmv, j0, (int)row0, &full[s]);
           tma_load_2d(st + L::kTab, &tmd, j0, (int)row0, &full[s]);
           for (int q = 0; q < 4; ++q)
-            bulk_g2s(st + 2 * L::kTab + q * kTJ * 32, fold + ((size_t)m * 4 + q) * Nx * 4 + (size_t)j0 * 4,
-                     fold_bytes, &full[s]);
+            bulk_g2s(st + 2 * L::kTab + q * kTJ * sizeof(F4), fold + ((size_t)m * 4 + q) * Nx + j0, fold_bytes,
+                     &full[s]);
           ++n;
         }
       }
     }
     __syncwarp();
   } else {
-    // ---- consumers: warp cw owns rows ra = par + 4 (cw >> 1) and ra + 2 ----------------
+    // ---- consumers: warp cw owns the RW rows par + 2 RW (cw >> 1) + 2 i ---------------
     const int cw = warp - 1;
     const int par = cw & 1;
-    const int ra = par + 4 * (cw >> 1);
+    const int rbase = par + 2 * RW * (cw >> 1);
     uint32_t n = 0;
     for (int64_t item = blockIdx.x; item < nitems; item += gridDim.x) {
       int m, g;
-      item_of(item, Nl, &m, &g);
+      item_of<kRows>(item, Nl, &m, &g);
       const int l0 = m + g * kRows;
-      const int la = l0 + ra, lb = l0 + ra + 2;
-      const bool va = la < Nl, vb = lb < Nl;
-      double ea_r = 0, ea_i = 0, pa_r = 0, pa_i = 0, eb_r = 0, eb_i = 0, pb_r = 0, pb_i = 0;
+      double acc[RW][4];
+#pragma unroll
+      for (int i = 0; i < RW; ++i)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[i][c] = 0.0;
       for (int t = 0; t < ntile; ++t) {
         if (!live[t] && !live[ntile + t]) continue;
         const int s = n % kStagesC;
@@ -160,59 +177,55 @@ contract_stream_kernel(int Nl, int Nx, int64_t nitems, const __grid_constant__ C
         }
         if (ok) {
           const uint8_t* st = smem + s * L::kStage;
-          const T* Ta = reinterpret_cast<const T*>(st) + ra * kTJ;
-          const T* Da = reinterpret_cast<const T*>(st + L::kTab) + ra * kTJ;
-          const double4* Fe = reinterpret_cast<const double4*>(st + 2 * L::kTab) + par * kTJ;
-          const double4* Fp = Fe + 2 * kTJ;
+          const T* Tv = reinterpret_cast<const T*>(st);
+          const T* Td = reinterpret_cast<const T*>(st + L::kTab);
+          const F4* Fe = reinterpret_cast<const F4*>(st + 2 * L::kTab) + par * kTJ;
+          const F4* Fp = Fe + 2 * kTJ;
           const int nj = min(kTJ, Nx - t * kTJ);
+          T part[RW][4];
+#pragma unroll
+          for (int i = 0; i < RW; ++i)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) part[i][c] = (T)0;
 #pragma unroll 4
           for (int jj = lane; jj < nj; jj += 32) {
-            const double4 fe = Fe[jj], fp = Fp[jj];
-            if (va) {
-              const double v = (double)Ta[jj], d = (double)Da[jj];
-              ea_r = fma(v, fe.x, fma(d, fe.z, ea_r));
-              ea_i = fma(v, fe.y, fma(d, fe.w, ea_i));
-              pa_r = fma(v, fp.x, fma(d, fp.z, pa_r));
-              pa_i = fma(v, fp.y, fma(d, fp.w, pa_i));
-            }
-            if (vb) {
-              const double v = (double)Ta[2 * kTJ + jj], d = (double)Da[2 * kTJ + jj];
-              eb_r = fma(v, fe.x, fma(d, fe.z, eb_r));
-              eb_i = fma(v, fe.y, fma(d, fe.w, eb_i));
-              pb_r = fma(v, fp.x, fma(d, fp.z, pb_r));
-              pb_i = fma(v, fp.y, fma(d, fp.w, pb_i));
+            const F4 fe = Fe[jj], fp = Fp[jj];
+#pragma unroll
+            for (int i = 0; i < RW; ++i) {
+              const int r = rbase + 2 * i;
+              const T v = Tv[r * kTJ + jj], d = Td[r * kTJ + jj];
+              part[i][0] = fma(v, fe.x, fma(d, fe.z, part[i][0]));
+              part[i][1] = fma(v, fe.y, fma(d, fe.w, part[i][1]));
+              part[i][2] = fma(v, fp.x, fma(d, fp.z, part[i][2]));
+              part[i][3] = fma(v, fp.y, fma(d, fp.w, part[i][3]));
             }
           }
+#pragma unroll
+          for (int i = 0; i < RW; ++i)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) acc[i][c] += (double)part[i][c];
         }
         __syncwarp();
         if (lane == 0) tc::mbar_arrive(&empty[s]);
         ++n;
       }
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        ea_r += __shfl_xor_sync(0xffffffffu, ea_r, o);
-        ea_i += __shfl_xor_sync(0xffffffffu, ea_i, o);
-        pa_r += __shfl_xor_sync(0xffffffffu, pa_r, o);
-        pa_i += __shfl_xor_sync(0xffffffffu, pa_i, o);
-        eb_r += __shfl_xor_sync(0xffffffffu, eb_r, o);
-        eb_i += __shfl_xor_sync(0xffffffffu, eb_i, o);
-        pb_r += __shfl_xor_sync(0xffffffffu, pb_r, o);
-        pb_i += __shfl_xor_sync(0xffffffffu, pb_i, o);
-      }
+      for (int i = 0; i < RW; ++i)
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) acc[i][c] += __shfl_xor_sync(0xffffffffu, acc[i][c], o);
       if (lane == 0) {
-        if (va) {
-          const int64_t i = hp_index(la, m, Nl);
-          alm_equ[2 * i] = ea_r;
-          alm_equ[2 * i + 1] = ea_i;
-          alm_pol[2 * i] = pa_r;
-          alm_pol[2 * i + 1] = pa_i;
-        }
-        if (vb) {
-          const int64_t i = hp_index(lb, m, Nl);
-          alm_equ[2 * i] = eb_r;
-          alm_equ[2 * i + 1] = eb_i;
-          alm_pol[2 * i] = pb_r;
-          alm_pol[2 * i + 1] = pb_i;
+#pragma unroll
+        for (int i = 0; i < RW; ++i) {
+          const int l = l0 + rbase + 2 * i;
+          if (l < Nl) {
+            const int64_t idx = hp_index(l, m, Nl);
+            alm_equ[2 * idx] = acc[i][0];
+            alm_equ[2 * idx + 1] = acc[i][1];
+            alm_pol[2 * idx] = acc[i][2];
+            alm_pol[2 * idx + 1] = acc[i][3];
+          }
         }
       }
     }
@@ -229,6 +242,7 @@ bool contract_stream_ok(const Geometry& g, size_t elem_bytes) {
 }
 
 int make_table_tmap(CUtensorMap* tm, const void* base, size_t elem_bytes, int Nx, int64_t Nlm) {
+  const int kRows = elem_bytes == 8 ? StageLayout<false>::kRows : StageLayout<true>::kRows;
   static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
   if (!encode) {
     void* fn = nullptr;
@@ -250,26 +264,28 @@ int make_table_tmap(CUtensorMap* tm, const void* base, size_t elem_bytes, int Nx
   return DSHT_OK;
 }
 
-template <typename T>
-void launch_contract_stream(const Geometry& g, const CUtensorMap& tmv, const CUtensorMap& tmd, const Workspace& ws,
-                            cudaStream_t s) {
-  using L = StageLayout<T>;
-  cudaFuncSetAttribute(contract_stream_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kBytes);
+void launch_contract_stream(const Geometry& g, bool mixed, const CUtensorMap& tmv, const CUtensorMap& tmd,
+                            const Workspace& ws, cudaStream_t s) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int ntile = (g.Nx + kTJ - 1) / kTJ;
+  const int rows = mixed ? StageLayout<true>::kRows : StageLayout<false>::kRows;
   int64_t nitems = 0;
-  for (int m = 0; m < g.Nl; ++m) nitems += (g.Nl - m + kRows - 1) / kRows;
+  for (int m = 0; m < g.Nl; ++m) nitems += (g.Nl - m + rows - 1) / rows;
   const int64_t grid = nitems < sms ? nitems : sms;
-  contract_stream_kernel<T><<<(unsigned)grid, kThreads, L::kBytes, s>>>(
-      g.Nl, g.Nx, nitems, tmv, tmd, ws.fold, ws.tile_live2, ntile, ws.alm_equ, ws.alm_pol, ws.flags);
+  if (mixed) {
+    using L = StageLayout<true>;
+    cudaFuncSetAttribute(contract_stream_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kBytes);
+    contract_stream_kernel<true><<<(unsigned)grid, kThreads, L::kBytes, s>>>(
+        g.Nl, g.Nx, nitems, tmv, tmd, ws.fold, ws.tile_live2, ntile, ws.alm_equ, ws.alm_pol, ws.flags);
+  } else {
+    using L = StageLayout<false>;
+    cudaFuncSetAttribute(contract_stream_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kBytes);
+    contract_stream_kernel<false><<<(unsigned)grid, kThreads, L::kBytes, s>>>(
+        g.Nl, g.Nx, nitems, tmv, tmd, ws.fold, ws.tile_live2, ntile, ws.alm_equ, ws.alm_pol, ws.flags);
+  }
   count_launches(1);
 }
-
-template void launch_contract_stream<double>(const Geometry&, const CUtensorMap&, const CUtensorMap&,
-                                             const Workspace&, cudaStream_t);
-template void launch_contract_stream<float>(const Geometry&, const CUtensorMap&, const CUtensorMap&,
-                                            const Workspace&, cudaStream_t);
 
 }  // namespace dsht

@@ -65,6 +65,7 @@ struct Workspace {
   double* alm_pol;      // [Nlm][2]
   int64_t npts;         // N, the stride of pay
   int partial_f32;      // partial sums stored as float (tensor-core path) instead of double
+  int fold_f32;         // fold written as float4 (mixed contraction) instead of double4
   int64_t pmax;
   int piece_max;
   size_t bytes;
@@ -84,9 +85,8 @@ void launch_fold(const Geometry& g, const Workspace& ws, cudaStream_t s);
 void launch_contract_fp64(const Geometry& g, const double* Yv, const double* Yd,
                           const Workspace& ws, cudaStream_t s);
 bool contract_stream_ok(const Geometry& g, size_t elem_bytes);
-template <typename T>
-void launch_contract_stream(const Geometry& g, const CUtensorMap& tmv, const CUtensorMap& tmd, const Workspace& ws,
-                            cudaStream_t s);
+void launch_contract_stream(const Geometry& g, bool mixed, const CUtensorMap& tmv, const CUtensorMap& tmd,
+                            const Workspace& ws, cudaStream_t s);
 // 2D tensor map over a (Nlm x Nx) table for the streaming contraction's TMA loads.
 int make_table_tmap(CUtensorMap* tm, const void* base, size_t elem_bytes, int Nx, int64_t Nlm);
 void launch_tables_to_f32(const Geometry& g, const double* Yv, const double* Yd, float* Yv32, float* Yd32,

@@ -15,10 +15,10 @@ namespace {
 
 constexpr int kFoldThreads = 128;
 
-template <typename T>
+template <typename T, typename F4>
 __global__ void __launch_bounds__(kFoldThreads)
 fold_kernel(int Nl, int Nx, int nbins, double dx, const int* __restrict__ piece_first,
-            const T* __restrict__ partial, double* __restrict__ fold) {
+            const T* __restrict__ partial, F4* __restrict__ fold) {
   const int j = blockIdx.x;
   const int m = blockIdx.y * blockDim.x + threadIdx.x;
   if (m >= Nl) return;
@@ -51,11 +51,14 @@ fold_kernel(int Nl, int Nx, int nbins, double dx, const int* __restrict__ piece_
     B[s][0] = dx * br;
     B[s][1] = dx * bi;
   }
-  double4* out = reinterpret_cast<double4*>(fold) + ((size_t)m * 4) * Nx + j;
-  out[0] = make_double4(A[0][0] + A[1][0], A[0][1] + A[1][1], B[0][0] + B[1][0], B[0][1] + B[1][1]);
-  out[(size_t)Nx] = make_double4(A[0][0] - A[1][0], A[0][1] - A[1][1], B[0][0] - B[1][0], B[0][1] - B[1][1]);
-  out[(size_t)2 * Nx] = make_double4(A[2][0] + A[3][0], A[2][1] + A[3][1], B[2][0] + B[3][0], B[2][1] + B[3][1]);
-  out[(size_t)3 * Nx] = make_double4(A[2][0] - A[3][0], A[2][1] - A[3][1], B[2][0] - B[3][0], B[2][1] - B[3][1]);
+  using E = decltype(F4::x);
+  F4* out = fold + ((size_t)m * 4) * Nx + j;
+  out[0] = F4{(E)(A[0][0] + A[1][0]), (E)(A[0][1] + A[1][1]), (E)(B[0][0] + B[1][0]), (E)(B[0][1] + B[1][1])};
+  out[(size_t)Nx] = F4{(E)(A[0][0] - A[1][0]), (E)(A[0][1] - A[1][1]), (E)(B[0][0] - B[1][0]), (E)(B[0][1] - B[1][1])};
+  out[(size_t)2 * Nx] =
+      F4{(E)(A[2][0] + A[3][0]), (E)(A[2][1] + A[3][1]), (E)(B[2][0] + B[3][0]), (E)(B[2][1] + B[3][1])};
+  out[(size_t)3 * Nx] =
+      F4{(E)(A[2][0] - A[3][0]), (E)(A[2][1] - A[3][1]), (E)(B[2][0] - B[3][0]), (E)(B[2][1] - B[3][1])};
 }
 
 // tile_live[h][t] = 1 when any point of the equatorial (h = 0) or polar (h = 1) sets
@@ -79,12 +82,16 @@ int contract_tile();
 
 void launch_fold(const Geometry& g, const Workspace& ws, cudaStream_t s) {
   dim3 grid(g.Nx, (g.Nl + kFoldThreads - 1) / kFoldThreads);
-  if (ws.partial_f32)
-    fold_kernel<float><<<grid, kFoldThreads, 0, s>>>(g.Nl, g.Nx, g.nbins, g.dx, ws.piece_first,
-                                                    reinterpret_cast<const float*>(ws.partial), ws.fold);
+  const float* pf = reinterpret_cast<const float*>(ws.partial);
+  float4* f32 = reinterpret_cast<float4*>(ws.fold);
+  double4* f64 = reinterpret_cast<double4*>(ws.fold);
+  if (ws.partial_f32 && ws.fold_f32)
+    fold_kernel<float, float4><<<grid, kFoldThreads, 0, s>>>(g.Nl, g.Nx, g.nbins, g.dx, ws.piece_first, pf, f32);
+  else if (ws.partial_f32)
+    fold_kernel<float, double4><<<grid, kFoldThreads, 0, s>>>(g.Nl, g.Nx, g.nbins, g.dx, ws.piece_first, pf, f64);
   else
-    fold_kernel<double><<<grid, kFoldThreads, 0, s>>>(g.Nl, g.Nx, g.nbins, g.dx, ws.piece_first, ws.partial,
-                                                     ws.fold);
+    fold_kernel<double, double4><<<grid, kFoldThreads, 0, s>>>(g.Nl, g.Nx, g.nbins, g.dx, ws.piece_first,
+                                                              ws.partial, f64);
   count_launches(1);
   const int tile = contract_tile();
   const int ntile = (g.Nx + tile - 1) / tile;
