@@ -25,6 +25,7 @@ DSHT_MODE_BASIC = 1
 
 DSHT_PREC_FP64 = 0
 DSHT_PREC_MIXED = 1
+DSHT_PREC_MIXED_F64_TABLES = 2
 
 STAGES = ("points", "bin_sums", "fold", "contract", "rotate")
 

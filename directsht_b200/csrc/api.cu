@@ -109,7 +109,8 @@ int run_pipeline(dsht_plan_s* p, const double* theta, const double* phi, const d
   mark(1);
   Workspace w2 = ws;
   // Small transforms run the FP64 stages even on a mixed-precision plan.
-  const bool mixed = p->precision == DSHT_PREC_MIXED && N >= DSHT_MIXED_MIN_POINTS;
+  const bool mixed = p->precision != DSHT_PREC_FP64 && N >= DSHT_MIXED_MIN_POINTS;
+  const bool f32_tables = mixed && p->precision == DSHT_PREC_MIXED && p->tm32;
   if (mixed) {
     int rc = launch_bin_sums_tc(g, ws, s);
     if (rc) return rc;
@@ -118,11 +119,11 @@ int run_pipeline(dsht_plan_s* p, const double* theta, const double* phi, const d
     launch_bin_sums_fp64(g, ws, s);
     w2.partial_f32 = 0;
   }
-  w2.fold_f32 = (mixed && p->tm32) ? 1 : 0;
+  w2.fold_f32 = f32_tables ? 1 : 0;
   mark(2);
   launch_fold(g, w2, s);
   mark(3);
-  if (mixed && p->tm32)
+  if (f32_tables)
     launch_contract_stream(g, true, p->tmYv32, p->tmYd32, ws, s);
   else if (p->tm64)
     launch_contract_stream(g, false, p->tmYv, p->tmYd, ws, s);
@@ -237,9 +238,9 @@ int dsht_plan_destroy(dsht_plan_t p) {
 
 int dsht_set_precision(dsht_plan_t p, int precision) {
   if (!p) return set_error(DSHT_ERR_INVALID, "plan is NULL");
-  if (precision != DSHT_PREC_FP64 && precision != DSHT_PREC_MIXED)
+  if (precision != DSHT_PREC_FP64 && precision != DSHT_PREC_MIXED && precision != DSHT_PREC_MIXED_F64_TABLES)
     return set_error(DSHT_ERR_INVALID, "unknown precision %d", precision);
-  if (precision == DSHT_PREC_MIXED && p->g.Nl > 2048)
+  if (precision != DSHT_PREC_FP64 && p->g.Nl > 2048)
     return set_error(DSHT_ERR_INVALID, "mixed precision supports Nl <= 2048 (Nl=%d)", p->g.Nl);
   std::lock_guard<std::mutex> lock(p->mu);
   if (precision == DSHT_PREC_MIXED && !p->Yv32) {

@@ -8,9 +8,9 @@
 // producer: for every live tile of 256 nodes it issues one 2D tensor-map TMA load per table
 // (an R-row x 256-node box of Yv and of Yd) and one bulk copy per fold row (4 q), all
 // completing on the stage's mbarrier.  Warps 1-8 consume: each owns R/8 rows of equal
-// parity and the 256 nodes of the tile (8 per lane); the fold values in shared memory
-// feed all its rows.  FP64 plans: double tables and fold, R = 16, FP64 FMAs.  Mixed plans:
-// FP32 tables and fold, R = 32, FP32 FMAs within a tile, FP64 sums across tiles.
+// parity and the 256 nodes of the tile (8 per lane); the FP64 fold values in shared memory
+// feed all its rows.  FP64 tables: double tables and fold, R = 16, FP64 FMAs.  FP32
+// tables: float tables and fold, R = 32, FP32 FMAs within a tile, FP64 sums across tiles.
 // HBM bound: 2 sizeof(T) bytes of table per (l, m, node).
 #include <cudaTypedefs.h>
 
@@ -73,9 +73,9 @@ __device__ __forceinline__ void item_of(int64_t item, int Nl, int* m_out, int* g
   *g_out = (int)(item - G(lo));
 }
 
-// FP64 plans: double tables, double4 fold entries, 16 rows per item, FP64 FMAs.
-// Mixed plans: float tables, float4 fold entries, 32 rows per item, FP32 FMAs within a
-// tile and FP64 accumulation across tiles.
+// FP64 tables: double tables and fold, 16 rows per item, FP64 FMAs.  FP32 tables (the
+// DSHT_PREC_MIXED level): float tables and fold, 32 rows per item, FP32 FMAs within a
+// tile and FP64 sums across tiles -- half the HBM traffic.
 template <bool kMixed>
 struct StageLayout {
   using T = typename std::conditional<kMixed, float, double>::type;

@@ -92,55 +92,89 @@ rotate_back_kernel(int Nl, const double* __restrict__ alm_rot, const double* __r
     }
   }
   __syncthreads();
+  // a'_{l,k} pre-scaled by 2 (the k = 0 term has weight 1 on the real part).
+  for (int k = threadIdx.x; k <= l; k += blockDim.x) {
+    a_re[k] *= (k >= 1) ? 2.0 : 1.0;
+    a_im[k] *= 2.0;
+  }
+  __syncthreads();
+  // Output column m: d_{k,m} for k = l .. 0 by the downward recurrence.  With pi = m & 1,
+  // the terms with k = l, l-2, ... go to Re if pi == 0 and to Im if pi == 1 (l+m+k even
+  // <-> real), so each column adds alternately into acc0 (rows k = l, l-2, ...) and acc1.
+  // acc0/acc1 are kept in the recurrence's scaled units (x 2^-E) and rescaled with it.
   const double big = 0x1p256, small = 0x1p-256;
-  // Two interleaved output columns per thread (independent recurrences).
   const int step = 2 * blockDim.x;
   for (int ma = threadIdx.x; ma <= l; ma += step) {
     const int mb = ma + blockDim.x;
     const bool hb = mb <= l;
-    double cur_a = st_m[ma], nxt_a = 0.0, cur_b = hb ? st_m[mb] : 0.0, nxt_b = 0.0;
+    const double* A0a = (ma & 1) ? a_im : a_re;  // k = l, l-2, ...
+    const double* A1a = (ma & 1) ? a_re : a_im;  // k = l-1, l-3, ...
+    const double* A0b = (mb & 1) ? a_im : a_re;
+    const double* A1b = (mb & 1) ? a_re : a_im;
+    double ca = st_m[ma], na = 0.0, cb = hb ? st_m[mb] : 0.0, nb = 0.0;
     int Ea = st_e[ma], Eb = hb ? st_e[mb] : 0;
-    double sca = (Ea > -1000) ? ldexp(1.0, Ea) : 0.0;
-    double scb = (hb && Eb > -1000) ? ldexp(1.0, Eb) : 0.0;
-    double re_a = 0.0, im_a = 0.0, re_b = 0.0, im_b = 0.0;
+    double s0a = 0.0, s1a = 0.0, s0b = 0.0, s1b = 0.0;
     const double twoa = 2.0 * ma, twob = 2.0 * mb;
-    for (int k = l; k >= 0; --k) {
-      const double da = cur_a * sca, db = cur_b * scb;
-      const double ar = a_re[k], ai = a_im[k];
-      const double wk = (k == 0) ? 1.0 : 2.0;
-      if (((l + ma + k) & 1) == 0) re_a = fma(wk * da, ar, re_a);
-      else if (k > 0) im_a = fma(2.0 * da, ai, im_a);
-      if (((l + mb + k) & 1) == 0) re_b = fma(wk * db, ar, re_b);
-      else if (k > 0) im_b = fma(2.0 * db, ai, im_b);
-      if (k == 0) break;
-      double pa = (twoa * cur_a - c1[k] * nxt_a) * c2[k];
-      double pb = (twob * cur_b - c1[k] * nxt_b) * c2[k];
-      if (fabs(pa) > big) {
-        pa *= small;
-        cur_a *= small;
-        Ea += 256;
-        sca = (Ea > -1000) ? ldexp(1.0, Ea) : 0.0;
+    int k = l;
+    // Pairs (k, k-1) while k >= 1; the single k = 0 term is handled after the loop.
+    for (int it = 0; k >= 2; ++it) {
+      // row k (acc0)
+      s0a = fma(ca, A0a[k], s0a);
+      s0b = fma(cb, A0b[k], s0b);
+      double pa = (twoa * ca - c1[k] * na) * c2[k];
+      double pb = (twob * cb - c1[k] * nb) * c2[k];
+      na = ca;
+      ca = pa;
+      nb = cb;
+      cb = pb;
+      // row k-1 (acc1)
+      s1a = fma(ca, A1a[k - 1], s1a);
+      s1b = fma(cb, A1b[k - 1], s1b);
+      pa = (twoa * ca - c1[k - 1] * na) * c2[k - 1];
+      pb = (twob * cb - c1[k - 1] * nb) * c2[k - 1];
+      na = ca;
+      ca = pa;
+      nb = cb;
+      cb = pb;
+      k -= 2;
+      if ((it & 1) == 1) {  // growth per step is bounded, so checking every 4 steps is safe
+        if (fabs(ca) > big) {
+          ca *= small; na *= small; s0a *= small; s1a *= small; Ea += 256;
+        }
+        if (fabs(cb) > big) {
+          cb *= small; nb *= small; s0b *= small; s1b *= small; Eb += 256;
+        }
       }
-      if (fabs(pb) > big) {
-        pb *= small;
-        cur_b *= small;
-        Eb += 256;
-        scb = (Eb > -1000) ? ldexp(1.0, Eb) : 0.0;
-      }
-      nxt_a = cur_a;
-      cur_a = pa;
-      nxt_b = cur_b;
-      cur_b = pb;
     }
+    // Remaining rows: k == 1 (then 0) or k == 0.
+    if (k == 1) {
+      s0a = fma(ca, A0a[1], s0a);
+      s0b = fma(cb, A0b[1], s0b);
+      const double pa = (twoa * ca - c1[1] * na) * c2[1];
+      const double pb = (twob * cb - c1[1] * nb) * c2[1];
+      na = ca; ca = pa; nb = cb; cb = pb;
+      // k = 0 follows k = 1 in acc1's sequence (l odd): the weight-1 real term counts
+      // when l + m is even, i.e. m odd, and acc1 is then the real part.
+      s1a = fma(ca, ((ma & 1) ? a_re[0] : 0.0), s1a);
+      s1b = fma(cb, ((mb & 1) ? a_re[0] : 0.0), s1b);
+    } else {  // k == 0 in acc0's sequence (l even): counts when m is even (acc0 real)
+      s0a = fma(ca, ((ma & 1) ? 0.0 : a_re[0]), s0a);
+      s0b = fma(cb, ((mb & 1) ? 0.0 : a_re[0]), s0b);
+    }
+    const double fa = (Ea > -1074) ? ldexp(1.0, Ea) : 0.0;
+    const double fb = (Eb > -1074) ? ldexp(1.0, Eb) : 0.0;
+    // acc0 holds Re when m even, Im when m odd (and acc1 the other).
+    const double rea = ((ma & 1) ? s1a : s0a) * fa, ima = ((ma & 1) ? s0a : s1a) * fa;
     {
       const int64_t i = hp_index(l, ma, Nl);
-      alm_out[2 * i] = alm_add[2 * i] + re_a;
-      alm_out[2 * i + 1] = alm_add[2 * i + 1] + im_a;
+      alm_out[2 * i] = alm_add[2 * i] + rea;
+      alm_out[2 * i + 1] = alm_add[2 * i + 1] + ima;
     }
     if (hb) {
+      const double reb = ((mb & 1) ? s1b : s0b) * fb, imb = ((mb & 1) ? s0b : s1b) * fb;
       const int64_t i = hp_index(l, mb, Nl);
-      alm_out[2 * i] = alm_add[2 * i] + re_b;
-      alm_out[2 * i + 1] = alm_add[2 * i + 1] + im_b;
+      alm_out[2 * i] = alm_add[2 * i] + reb;
+      alm_out[2 * i + 1] = alm_add[2 * i + 1] + imb;
     }
   }
 }

@@ -38,8 +38,10 @@ class DirectSHT:
         :param dflt_type: dtype of the host copy of the x grid (the tables are FP64).
         :param null_unphysical: accepted for compatibility; rows l < m are never stored.
         :param device: CUDA device (default: the current one).
-        :param precision: "fp64" (FP64 per-bin sums, agrees with the reference to ~1e-15) or
-            "mixed" (tensor-core per-bin sums on fp16 hi/lo operands, <= 1e-7 x max|alm|).
+        :param precision: "fp64" (agrees with the reference to ~1e-15), "mixed" (tensor-core
+            per-bin sums and FP32 tables: fastest, <= 1e-7 x max|alm| for point sets spread over
+            many x bins) or "mixed_f64_tables" (tensor-core sums, FP64 tables: <= 1e-7 also when
+            the weight concentrates in one bin).
         """
         self._lib = L.load()
         if not torch.cuda.is_available():
@@ -71,10 +73,11 @@ class DirectSHT:
             self._plan = None
 
     def set_precision(self, precision):
-        """Switch the per-bin sums between "fp64" and "mixed" (tables stay FP64)."""
-        code = {"fp64": L.DSHT_PREC_FP64, "mixed": L.DSHT_PREC_MIXED}.get(precision)
+        """Switch between "fp64", "mixed" and "mixed_f64_tables" (see the constructor)."""
+        code = {"fp64": L.DSHT_PREC_FP64, "mixed": L.DSHT_PREC_MIXED,
+                "mixed_f64_tables": L.DSHT_PREC_MIXED_F64_TABLES}.get(precision)
         if code is None:
-            raise ValueError(f"precision must be 'fp64' or 'mixed', not {precision!r}")
+            raise ValueError(f"precision must be 'fp64', 'mixed' or 'mixed_f64_tables', not {precision!r}")
         L.check(self._lib.dsht_set_precision(self._plan, code))
         self.precision = precision
 

@@ -57,19 +57,27 @@ enum {
   DSHT_PLAN_DEFAULT = 0
 };
 
-/* Arithmetic of the per-bin sums (the scatter) of a plan.
- *   DSHT_PREC_FP64  : FP64 CUDA-core sums; agrees with the reference's numpy path to
- *                     about 1e-15 (tested at <= 1e-12 x max|alm|).
- *   DSHT_PREC_MIXED : tcgen05 tensor-core sums: operands quantised to 21-bit fixed point,
- *                     split in three int8 slices, six slice products accumulated exactly in
- *                     S32 and combined in FP64 (unbiased, about 1.3e-7 rms per product;
- *                     tested at <= 1e-7 x max|alm|); Nl <= 2048.  Transforms of fewer than
- *                     DSHT_MIXED_MIN_POINTS points use the FP64 sums: they cost little, and
- *                     the quantisation error of a handful of points does not average down.
- * The tables, the contraction and the rotation stay FP64 in both. */
+/* Arithmetic of a plan's transforms.
+ *   DSHT_PREC_FP64  : FP64 CUDA-core per-bin sums and FP64 tables; agrees with the
+ *                     reference's numpy path to about 1e-15 (tested at <= 1e-12 x max|alm|).
+ *   DSHT_PREC_MIXED : tcgen05 tensor-core per-bin sums (operands quantised to 22-bit fixed
+ *                     point, split into int8 slices, slice products accumulated exactly in
+ *                     S32 and combined in FP64; unbiased, about 5.6e-8 rms per product) and
+ *                     an FP32 copy of the tables streamed by the contraction (half the HBM
+ *                     bytes, FP64 sums).  Within 1e-7 x max|alm| of FP64 for point sets
+ *                     spread over many nodes (4.5e-8 measured on 1e7 points, Nl=1024); the
+ *                     FP32 table rounding can reach a few 1e-7 when most of the weight sits
+ *                     in one x bin.  Also the fixed-point scale of a bin piece is its
+ *                     largest |weight|: weights spanning many decades lose accuracy.
+ *   DSHT_PREC_MIXED_F64_TABLES : the same tensor-core sums with the FP64 tables
+ *                     (within 1e-7 x max|alm| also for concentrated point sets).
+ * Mixed levels need Nl <= 2048; transforms of fewer than DSHT_MIXED_MIN_POINTS points run
+ * the FP64 stages (they cost little, and the quantisation error of a handful of points
+ * does not average down).  The rotation stays FP64 in all levels. */
 enum {
   DSHT_PREC_FP64 = 0,
-  DSHT_PREC_MIXED = 1
+  DSHT_PREC_MIXED = 1,
+  DSHT_PREC_MIXED_F64_TABLES = 2
 };
 #define DSHT_MIXED_MIN_POINTS 1024
 int64_t dsht_mixed_min_points(void);
