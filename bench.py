@@ -112,6 +112,20 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm), "power_w_max": max(power) if power else None}
 
 
+def dram_traffic(stage, precision, N, Nlm, Nx):
+    """DRAM bytes per launch of a stage's kernel from the Nsight Compute capture summarised in
+    profiles/dram_traffic.json (bytes per point or per table entry), scaled to this workload."""
+    p = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        t = json.load(f)
+    e = t.get(f"{stage}:{precision}")
+    if not e:
+        return None
+    return e["bytes_per_point"] * N + e.get("bytes_per_table_entry", 0.0) * Nlm * Nx
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -284,41 +298,52 @@ def main(argv=None):
     while C < (Nl + 15) // 16:
         C *= 2
 
+    f32_tables = args.precision == "mixed"
+
     def stage_roof(name, ms):
+        """Roofline of one stage: algorithmic bytes or ops per launch / measured launch time."""
         if ms <= 0:
             return None
         if name == "contract":
-            alg = 16.0 * d.Nlm * Nx
+            eb = 4 if f32_tables else 8
+            alg = 2.0 * eb * d.Nlm * Nx
             a = alg / (ms * 1e-3) / 1e9
-            return {"kernel": "contract_fp64_kernel", "bound": "hbm", "achieved": a, "peak": hbm_peak,
-                    "unit": "GB/s", "frac": a / hbm_peak, "peak_source": peak_src,
-                    "algorithmic": "16 B of FP64 table per (l, m, node) per step"}
-        if name == "points":
-            alg = 64.0 * N
-            a = alg / (ms * 1e-3) / 1e9
-            return {"kernel": "count/scan/scatter (counting sort)", "bound": "hbm", "achieved": a,
+            return {"kernel": "contract_stream_kernel (TMA 2D tensor-map tiles)", "bound": "hbm", "achieved": a,
                     "peak": hbm_peak, "unit": "GB/s", "frac": a / hbm_peak, "peak_source": peak_src,
-                    "algorithmic": "24 B of inputs read + 40 B of sorted payload written per point"}
-        if name == "bin_sums" and args.precision == "mixed":
-            alg = 2.0 * 128 * (2 * C) * 6 * N
+                    "algorithmic": f"{2 * eb} B of {'FP32' if f32_tables else 'FP64'} table (Yv, Yd) per "
+                                   f"(l, m, node)"}
+        if name == "points":
+            alg = 72.0 * N
+            a = alg / (ms * 1e-3) / 1e9
+            return {"kernel": "count/scan/scatter (counting sort by bin)", "bound": "hbm", "achieved": a,
+                    "peak": hbm_peak, "unit": "GB/s", "frac": a / hbm_peak, "peak_source": peak_src,
+                    "algorithmic": "24 B of inputs read + 48 B of sorted record written per point"}
+        if name == "bin_sums" and args.precision != "fp64":
+            alg = 2.0 * 128 * (2 * C) * 8 * N
             pk = 2 * bf16_peak
             a = alg / (ms * 1e-3) / 1e12
             return {"kernel": "bin_sums_tc_kernel (tcgen05 kind::i8)", "bound": "tensor", "achieved": a,
                     "peak": pk, "unit": "TOP/s", "frac": a / pk,
                     "peak_source": f"derived: 2 x {peak_src} bf16 (dense int8 rate is twice bf16 on B200)",
-                    "algorithmic": f"6 int8 slice products of a 128 x {2 * C} x P GEMM per piece, 2 op per MAC"}
+                    "algorithmic": f"8 int8 slice products of a 128 x {2 * C} x (points) GEMM, 2 op per MAC"}
         if name == "bin_sums":
             alg = 24.0 * N * Nl
             a = alg / (ms * 1e-3) / 1e12
             return {"kernel": "bin_sums_fp64_kernel", "bound": "fp64", "achieved": a, "peak": 40.0,
                     "unit": "TFLOP/s", "frac": a / 40.0, "peak_source": "nominal (no measured FP64 figure)",
                     "algorithmic": "24 flop per (point, m): 8 FMA sums + 4 FMA angle step"}
+        if name == "rotate":
+            alg = 2.0 * 5 * sum((l + 1) ** 2 for l in range(Nl))
+            a = alg / (ms * 1e-3) / 1e12
+            return {"kernel": "rotate_back_kernel", "bound": "fp64", "achieved": a, "peak": 40.0,
+                    "unit": "TFLOP/s", "frac": a / 40.0, "peak_source": "nominal (no measured FP64 figure)",
+                    "algorithmic": "5 FMA per (l, m, m') of the Wigner-d recursion and product"}
         return None
 
     roofs = {n: stage_roof(n, ms) for n, ms in stages.items()}
     top = max(stages, key=stages.get)
     roof = dict(roofs[top] or {"kernel": top, "bound": None})
-    roof["traffic"] = None
+    roof["traffic"] = dram_traffic(top, args.precision, N, d.Nlm, Nx)
     roof["stage_ms"] = stages[top]
 
     # End to end through the host-pointer C ABI entry, pinned host buffers.
