@@ -36,6 +36,8 @@ WORKLOADS = {
                    name="profiling case: Nl=1024, Nx=256, N=4e6, C2 point distribution"),
     "c1": dict(Nl=256, Nx=512, N=100_000, kind="full", wkind="ones",
                name="full sky: Nl=256, Nx=512, N=1e5, cos(theta)~U[-1,1], phi~U[0,2pi), w=1 f64"),
+    "c3": dict(Nl=1024, Nx=2048, N=2_000_000, kind="full", wkind="normal", maps=64,
+               name="multi-map: Nl=1024, Nx=2048, N=2e6 full sky shared by 64 maps w~N(1,0.3^2) f32"),
 }
 
 
@@ -49,7 +51,9 @@ def make_points(spec, seed):
         cost = rng.uniform(-1.0, 1.0, N)
         phi = rng.uniform(0.0, 2 * np.pi, N)
     theta = np.arccos(cost)
-    if spec["wkind"] == "lognormal":
+    if spec["wkind"] == "normal":  # float32 maps, one row per map
+        w = rng.normal(1.0, 0.3, (spec.get("maps", 1), N)).astype(np.float32)
+    elif spec["wkind"] == "lognormal":
         w = rng.lognormal(0.0, 0.5, N)
     elif spec["wkind"] == "uniform":
         w = rng.uniform(0.5, 1.5, N)
@@ -145,6 +149,8 @@ def cpu_reference_run(spec, sample_n, steps, warmup, seed=0):
     if not ref_csht.available():
         return None
     th, ph, w = make_points(dict(spec, N=sample_n), seed + 1000)
+    if w.ndim == 2:  # the reference transforms one map per call; time the first
+        w = w[0].astype(np.float64)
     t0 = time.time()
     ref = ref_csht.RefCSHT(spec["Nl"], spec["Nx"])
     t_tables = time.time() - t0
@@ -162,8 +168,9 @@ def cpu_reference_run(spec, sample_n, steps, warmup, seed=0):
     sec = float(np.mean(times))
     return {"value": sample_n * spec["Nl"] / sec, "unit": "points*ell/s", "cores": os.cpu_count(),
             "kind": "reference", "seconds_per_step": sec, "table_build_s": t_tables,
-            "sample": f"{sample_n} points of the same distribution through csht/sht_helper.c do_transform "
-                      f"(OpenMP, {os.cpu_count()} threads) at Nl={spec['Nl']}, Nx={spec['Nx']}; rotations untimed"}
+            "sample": f"{sample_n} points of the same distribution (one map) through csht/sht_helper.c "
+                      f"do_transform (OpenMP, {os.cpu_count()} threads) at Nl={spec['Nl']}, Nx={spec['Nx']}; "
+                      f"rotations untimed"}
 
 
 def run_reference_arm(args, spec):
@@ -180,7 +187,7 @@ def run_reference_arm(args, spec):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
             "config": {"workload": spec["name"], "Nl": spec["Nl"], "Nx": spec["Nx"], "N": args.ref_sample,
-                       "maps": 1},
+                       "maps": 1, "maps_note": "points*ell/s counts point x map x ell; one map per call"},
             "cpu_baseline": {"value": r["value"], "unit": r["unit"], "cores": r["cores"], "kind": r["kind"],
                              "sample": r["sample"]},
             "e2e": {"value": r["value"], "unit": "points*ell/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -224,21 +231,27 @@ def main(argv=None):
 
     lib = L.load()
     Nl, Nx, N = spec["Nl"], spec["Nx"], spec["N"]
+    maps = spec.get("maps", 1)
     th, ph, w = make_points(spec, seed=rank)
     t0 = time.time()
     d = DirectSHT(Nl, Nx, device=dev)
     t_plan = time.time() - t0
     thd, phd, wd = (torch.from_numpy(a).to(dev) for a in (th, ph, w))
-    alm = torch.empty(d.Nlm, dtype=torch.complex128, device=dev)
+    alm = torch.empty((maps, d.Nlm), dtype=torch.complex128, device=dev)
     nbytes = ct.c_size_t()
-    L.check(lib.dsht_workspace_size(d._plan, N, ct.byref(nbytes)))
+    L.check(lib.dsht_workspace_size_maps(d._plan, N, maps, ct.byref(nbytes)))
     ws = torch.empty(nbytes.value, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
     sp = ct.c_void_p(stream.cuda_stream)
+    w_dtype = L.DSHT_W_F32 if w.dtype == np.float32 else L.DSHT_W_F64
 
-    def step(out):
-        L.check(lib.dsht_execute(d._plan, L.ptr(thd), L.ptr(phd), L.ptr(wd), N, L.DSHT_MODE_CALL, L.ptr(out),
-                                 L.ptr(ws), ws.numel(), sp))
+    def step(out, t=thd, p=phd, ww=wd):
+        if maps == 1 and w_dtype == L.DSHT_W_F64:
+            L.check(lib.dsht_execute(d._plan, L.ptr(t), L.ptr(p), L.ptr(ww), N, L.DSHT_MODE_CALL, L.ptr(out),
+                                     L.ptr(ws), ws.numel(), sp))
+        else:
+            L.check(lib.dsht_execute_maps(d._plan, L.ptr(t), L.ptr(p), L.ptr(ww), w_dtype, N, maps, N,
+                                          L.DSHT_MODE_CALL, L.ptr(out), L.ptr(ws), ws.numel(), sp))
 
     def timed(precision, sample_clocks):
         """W warm-up steps, then K timed steps between barriers; per-stage CUDA-event times."""
@@ -277,7 +290,7 @@ def main(argv=None):
             total_ms = float(t.item())
         ms_step = total_ms / args.steps
         stages = {n: stage_ms[i] / max(calls.value, 1) for i, n in enumerate(L.STAGES)}
-        return {"ms_per_step": ms_step, "value": world * N * Nl / (ms_step / 1e3), "per_step": per_step,
+        return {"ms_per_step": ms_step, "value": world * N * maps * Nl / (ms_step / 1e3), "per_step": per_step,
                 "stages": stages, "launches": int(launches), "clocks": clk, "alm": alm.clone()}
 
     main = timed(args.precision, sample_clocks=True)
@@ -289,8 +302,8 @@ def main(argv=None):
     launches, clk = main["launches"], main["clocks"]
     max_rel_err = None
     if other is not None:
-        ref = other["alm"]
-        max_rel_err = float((main["alm"] - ref).abs().max() / ref.abs().max())
+        ref = other["alm"]  # (maps, Nlm); error relative to each map's max|alm|
+        max_rel_err = float(((main["alm"] - ref).abs().amax(dim=1) / ref.abs().amax(dim=1)).max())
 
     # Roofline of every stage; the dominant one is reported.
     hbm_peak, bf16_peak, peak_src = measured_peaks()
@@ -346,9 +359,9 @@ def main(argv=None):
     roof["traffic"] = dram_traffic(top, args.precision, N, d.Nlm, Nx)
     roof["stage_ms"] = stages[top]
 
-    # End to end through the host-pointer C ABI entry, pinned host buffers.
+    # End to end from pinned host buffers: inputs copied in and alm copied out every step.
     e2e = None
-    if args.e2e_steps > 0:
+    if args.e2e_steps > 0 and maps == 1 and w_dtype == L.DSHT_W_F64:
         hp = [torch.from_numpy(a).pin_memory() for a in (th, ph, w)]
         out = torch.empty(2 * d.Nlm, dtype=torch.float64).pin_memory()
         dp = ct.POINTER(ct.c_double)
@@ -357,7 +370,22 @@ def main(argv=None):
             L.check(lib.dsht_execute_host(d._plan, ct.cast(hp[0].data_ptr(), dp), ct.cast(hp[1].data_ptr(), dp),
                                           ct.cast(hp[2].data_ptr(), dp), N, L.DSHT_MODE_CALL,
                                           ct.cast(out.data_ptr(), dp)))
+        e2e_path = "dsht_execute_host (C ABI, pinned host buffers), wall clock per call"
+        h2d = 24 * N
+    elif args.e2e_steps > 0:
+        hp = [torch.from_numpy(a).pin_memory() for a in (th, ph, w)]
+        dbuf = [torch.empty_like(a, device=dev) for a in hp]
+        out = torch.empty((maps, d.Nlm), dtype=torch.complex128).pin_memory()
 
+        def e2e_step():
+            for h, b in zip(hp, dbuf):
+                b.copy_(h, non_blocking=True)
+            step(alm, *dbuf)
+            out.copy_(alm, non_blocking=True)
+            stream.synchronize()
+        e2e_path = "pinned host -> device copies, dsht_execute_maps (C ABI), alm -> pinned host; wall clock"
+        h2d = sum(a.nbytes for a in (th, ph, w))
+    if args.e2e_steps > 0:
         e2e_step()
         if world > 1:
             dist.barrier()
@@ -371,9 +399,8 @@ def main(argv=None):
             t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             e2e_s = float(t.item())
-        e2e = {"value": world * N * Nl / e2e_s, "unit": "points*ell/s", "ms_per_step": e2e_s * 1e3,
-               "h2d_bytes_per_step": 24 * N, "d2h_bytes_per_step": 16 * d.Nlm,
-               "path": "dsht_execute_host (C ABI, pinned host buffers), wall clock per call"}
+        e2e = {"value": world * N * maps * Nl / e2e_s, "unit": "points*ell/s", "ms_per_step": e2e_s * 1e3,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 16 * d.Nlm * maps, "path": e2e_path}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -391,12 +418,15 @@ def main(argv=None):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": "i8 tensor sums + f64" if args.precision == "mixed" else "f64", "data": "synthetic",
-            "config": {"workload": spec["name"], "Nl": Nl, "Nx": Nx, "N": N, "maps": 1,
+            "config": {"workload": spec["name"], "Nl": Nl, "Nx": Nx, "N": N, "maps": maps,
                        "precision": args.precision,
-                       "l2": "inputs (240 MB) and tables (17 GB) exceed L2 every step",
+                       "l2": f"inputs ({(th.nbytes + ph.nbytes + w.nbytes) / 1e6:.0f} MB) and tables "
+                             f"({16 * d.Nlm * Nx / 1e9:.1f} GB FP64) exceed L2 every step",
                        "parallelism": f"replicas x{world}"},
             "p50_ms": float(np.percentile(per_step, 50)), "p99_ms": float(np.percentile(per_step, 99)),
             "stages_ms": stages, "plan_build_s": t_plan, "roofline": roof,
+            "stages_note": ("one sort (points) for all maps; bin_sums..rotate are those of one map "
+                            "(bin_sums includes its payload gather)") if maps > 1 else "all stages of one step",
             "stage_rooflines": {k: v for k, v in roofs.items() if v}, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(launches), "clocks": clk,
         }

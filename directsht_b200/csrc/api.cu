@@ -44,7 +44,7 @@ int default_piece_max(const Geometry& g, int64_t N) {
   return (int)p;
 }
 
-size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* base, Workspace* ws) {
+size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* base, Workspace* ws, bool maps) {
   size_t off = 0;
   auto take = [&](size_t bytes) -> uint8_t* {
     uint8_t* p = base ? base + off : nullptr;
@@ -57,9 +57,12 @@ size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* ba
   const int ntile = (g.Nx + tile - 1) / tile;
   Workspace w{};
   w.key = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * n));
-  w.idx_sorted = nullptr;
   w.rec = reinterpret_cast<double*>(take(sizeof(double) * 3 * n));
   w.pay = reinterpret_cast<double*>(take(sizeof(double) * 6 * n));
+  if (maps) {
+    w.sidx = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * n));
+    w.st = reinterpret_cast<double*>(take(sizeof(double) * n));
+  }
   w.count = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * (g.nkeys + 1)));
   w.offset = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * (g.nkeys + 1)));
   w.cursor = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * (g.nkeys + 1)));
@@ -97,16 +100,14 @@ Geometry make_geometry(int Nl, int Nx, double xmax) {
   return g;
 }
 
-// Runs the whole pipeline on `s`; leaves the device flags in ws.flags.
-int run_pipeline(dsht_plan_s* p, const double* theta, const double* phi, const double* w, int64_t N,
-                        int mode, double* alm, const Workspace& ws, cudaStream_t s) {
+// The stages after the sort: bin sums, fold, contraction, rotation (stage events 1..5 when
+// `marks` is set).  Reads the sorted payload ws.pay; leaves the device flags in ws.flags.
+int run_after_sort(dsht_plan_s* p, int64_t N, int mode, double* alm, const Workspace& ws, cudaStream_t s,
+                   bool marks) {
   const Geometry& g = p->g;
   auto mark = [&](int i) {
-    if (p->prof) cudaEventRecord(p->ev[i], s);
+    if (marks && p->prof) cudaEventRecord(p->ev[i], s);
   };
-  mark(0);
-  launch_points(g, theta, phi, w, N, mode, ws, s);
-  mark(1);
   Workspace w2 = ws;
   // Small transforms run the FP64 stages even on a mixed-precision plan.
   const bool mixed = p->precision != DSHT_PREC_FP64 && N >= DSHT_MIXED_MIN_POINTS;
@@ -140,14 +141,47 @@ int run_pipeline(dsht_plan_s* p, const double* theta, const double* phi, const d
   return DSHT_OK;
 }
 
+// Runs the whole pipeline on `s`; leaves the device flags in ws.flags.
+int run_pipeline(dsht_plan_s* p, const double* theta, const double* phi, const double* w, int64_t N,
+                        int mode, double* alm, const Workspace& ws, cudaStream_t s) {
+  p->prof_maps = false;
+  if (p->prof) cudaEventRecord(p->ev[0], s);
+  launch_points(p->g, theta, phi, w, 0, N, mode, ws, s);
+  if (p->prof) cudaEventRecord(p->ev[1], s);
+  return run_after_sort(p, N, mode, alm, ws, s, true);
+}
+
+// Several weight maps on one point set: one classification and sort (which also records the
+// input index and t of every sorted slot), then for every further map a gather rebuilds the
+// weighted payload and the later stages run again.  Stage events cover the last map.
+int run_maps(dsht_plan_s* p, const double* theta, const double* phi, const void* w, int w_f32, int64_t N,
+             int nmaps, int64_t w_stride, int mode, double* alm, const Workspace& ws, cudaStream_t s) {
+  const size_t esz = w_f32 ? sizeof(float) : sizeof(double);
+  const size_t nlm2 = 2 * (size_t)p->g.Nlm;
+  p->prof_maps = true;
+  if (p->prof) cudaEventRecord(p->ev[0], s);
+  launch_points(p->g, theta, phi, w, w_f32, N, mode, ws, s);
+  if (p->prof) cudaEventRecord(p->ev[1], s);
+  for (int k = 0; k < nmaps; ++k) {
+    const bool last = k == nmaps - 1;
+    if (last && p->prof) cudaEventRecord(p->ev[DSHT_STAGE_COUNT + 1], s);
+    if (k > 0) launch_gather(p->g, static_cast<const uint8_t*>(w) + esz * (size_t)w_stride * k, w_f32, N, ws, s);
+    int rc = run_after_sort(p, N, mode, alm + nlm2 * k, ws, s, last);
+    if (rc) return rc;
+  }
+  return DSHT_OK;
+}
+
 // After the stream has been synchronised: fold the stage events into the totals.
 void collect_profile(dsht_plan_s* p) {
   if (!p->prof) return;
   for (int i = 0; i < DSHT_STAGE_COUNT; ++i) {
     float ms = 0.f;
-    if (cudaEventElapsedTime(&ms, p->ev[i], p->ev[i + 1]) == cudaSuccess) p->prof_ms[i] += ms;
+    cudaEvent_t a = (p->prof_maps && i == DSHT_STAGE_BIN_SUMS) ? p->ev[DSHT_STAGE_COUNT + 1] : p->ev[i];
+    if (cudaEventElapsedTime(&ms, a, p->ev[i + 1]) == cudaSuccess) p->prof_ms[i] += ms;
   }
   p->prof_calls += 1;
+  p->prof_maps = false;
 }
 
 int flags_to_status(unsigned f, int mode) {
@@ -314,18 +348,23 @@ int dsht_workspace_size(dsht_plan_t p, int64_t N, size_t* bytes) {
   return DSHT_OK;
 }
 
-int dsht_execute(dsht_plan_t p, const double* theta, const double* phi, const double* w, int64_t N, int mode,
-                 double* alm, void* workspace, size_t workspace_bytes, void* stream) {
+static int execute_device(dsht_plan_t p, const double* theta, const double* phi, const void* w, int w_dtype,
+                          int64_t N, int nmaps, int64_t w_stride, int mode, double* alm, void* workspace,
+                          size_t workspace_bytes, void* stream) {
   if (!p || !alm || N < 0 || (N > 0 && (!theta || !phi || !w)))
     return set_error(DSHT_ERR_INVALID, "invalid arguments");
   if (mode != DSHT_MODE_CALL && mode != DSHT_MODE_BASIC) return set_error(DSHT_ERR_INVALID, "bad mode %d", mode);
+  if (w_dtype != DSHT_W_F64 && w_dtype != DSHT_W_F32) return set_error(DSHT_ERR_INVALID, "bad w_dtype %d", w_dtype);
+  if (nmaps < 1 || (nmaps > 1 && w_stride < N))
+    return set_error(DSHT_ERR_INVALID, "invalid maps (nmaps=%d, w_stride=%lld)", nmaps, (long long)w_stride);
   if (N > (int64_t)0xfffffff0LL) return set_error(DSHT_ERR_INVALID, "too many points (%lld)", (long long)N);
   if (N == 0 && mode == DSHT_MODE_BASIC)
     return set_error(DSHT_ERR_EMPTY, "The theta array seems to be empty!");
+  const bool maps = nmaps > 1;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   std::unique_lock<std::mutex> lock(p->mu, std::defer_lock);
   const int piece_max = default_piece_max(p->g, N);
-  const size_t need = workspace_layout(p->g, N, piece_max, nullptr, nullptr);
+  const size_t need = workspace_layout(p->g, N, piece_max, nullptr, nullptr, maps);
   uint8_t* base = reinterpret_cast<uint8_t*>(workspace);
   if (base) {
     if (workspace_bytes < need)
@@ -337,18 +376,38 @@ int dsht_execute(dsht_plan_t p, const double* theta, const double* phi, const do
     base = reinterpret_cast<uint8_t*>(p->ws);
   }
   if (N == 0) {  // __call__ on no points returns zeros (sht/sht.py:127,150)
-    DSHT_CUDA_OK(cudaMemsetAsync(alm, 0, sizeof(double) * 2 * p->g.Nlm, s));
+    DSHT_CUDA_OK(cudaMemsetAsync(alm, 0, sizeof(double) * 2 * p->g.Nlm * nmaps, s));
     return DSHT_OK;
   }
   Workspace ws;
-  workspace_layout(p->g, N, piece_max, base, &ws);
-  int rc = run_pipeline(p, theta, phi, w, N, mode, alm, ws, s);
+  workspace_layout(p->g, N, piece_max, base, &ws, maps);
+  int rc = maps || w_dtype == DSHT_W_F32
+               ? run_maps(p, theta, phi, w, w_dtype == DSHT_W_F32, N, nmaps, w_stride, mode, alm, ws, s)
+               : run_pipeline(p, theta, phi, static_cast<const double*>(w), N, mode, alm, ws, s);
   if (rc) return rc;
   unsigned hf = 0;
   DSHT_CUDA_OK(cudaMemcpyAsync(&hf, ws.flags, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
   DSHT_CUDA_OK(cudaStreamSynchronize(s));
   collect_profile(p);
   return flags_to_status(hf, mode);
+}
+
+int dsht_execute(dsht_plan_t p, const double* theta, const double* phi, const double* w, int64_t N, int mode,
+                 double* alm, void* workspace, size_t workspace_bytes, void* stream) {
+  return execute_device(p, theta, phi, w, DSHT_W_F64, N, 1, N, mode, alm, workspace, workspace_bytes, stream);
+}
+
+int dsht_workspace_size_maps(dsht_plan_t p, int64_t N, int nmaps, size_t* bytes) {
+  if (!p || !bytes || N < 0 || nmaps < 1) return set_error(DSHT_ERR_INVALID, "invalid arguments");
+  *bytes = workspace_layout(p->g, N, default_piece_max(p->g, N), nullptr, nullptr, nmaps > 1);
+  return DSHT_OK;
+}
+
+int dsht_execute_maps(dsht_plan_t p, const double* theta, const double* phi, const void* w, int w_dtype, int64_t N,
+                      int nmaps, int64_t w_stride, int mode, double* alm, void* workspace, size_t workspace_bytes,
+                      void* stream) {
+  return execute_device(p, theta, phi, w, w_dtype, N, nmaps, w_stride, mode, alm, workspace, workspace_bytes,
+                        stream);
 }
 
 int dsht_execute_host(dsht_plan_t p, const double* theta, const double* phi, const double* w, int64_t N, int mode,

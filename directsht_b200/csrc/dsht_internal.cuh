@@ -45,9 +45,10 @@ struct Geometry {
 // Workspace carve-up for one execute call.
 struct Workspace {
   uint32_t* key;        // [N]
-  uint32_t* idx_sorted; // [N] original index of each sorted slot (unused by the fused path)
   double* rec;          // [N][3]
   double* pay;          // [N][6]
+  uint32_t* sidx;       // [N] input index of each sorted slot (multi-map transforms)
+  double* st;           // [N] t of each sorted slot
   uint32_t* count;      // [nkeys + 1]
   uint32_t* offset;     // [nkeys + 1]
   uint32_t* cursor;     // [nkeys]
@@ -71,13 +72,15 @@ struct Workspace {
   size_t bytes;
 };
 
-size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* base, Workspace* ws);
+size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* base, Workspace* ws,
+                        bool maps = false);
 int default_piece_max(const Geometry& g, int64_t N);
 
 // Kernels launched by api.cu (each file owns its launch helpers).
 void launch_tables(const Geometry& g, double* Yv, double* Yd, cudaStream_t s);
-void launch_points(const Geometry& g, const double* theta, const double* phi, const double* w,
+void launch_points(const Geometry& g, const double* theta, const double* phi, const void* w, int w_f32,
                    int64_t N, int mode, const Workspace& ws, cudaStream_t s);
+void launch_gather(const Geometry& g, const void* w, int w_f32, int64_t N, const Workspace& ws, cudaStream_t s);
 void launch_bin_sums_fp64(const Geometry& g, const Workspace& ws, cudaStream_t s);
 int launch_bin_sums_tc(const Geometry& g, const Workspace& ws, cudaStream_t s);
 int tc_inner_factor(int Nl);
@@ -123,7 +126,10 @@ struct dsht_plan_s {
   int precision = DSHT_PREC_FP64;
   // Stage timers.
   bool prof = false;
-  cudaEvent_t ev[DSHT_STAGE_COUNT + 1] = {};
+  // ev[0..5]: stage boundaries; ev[6]: start of the last map's bin sums (multi-map calls,
+  // where stage 0 covers the sort alone and stages 1-4 the last map).
+  cudaEvent_t ev[DSHT_STAGE_COUNT + 2] = {};
+  bool prof_maps = false;
   double prof_ms[DSHT_STAGE_COUNT] = {};
   int64_t prof_calls = 0;
   std::mutex mu;
@@ -134,6 +140,12 @@ Geometry make_geometry(int Nl, int Nx, double xmax);
 // Enqueue the whole transform on `s` (flags are left in ws.flags; no synchronisation).
 int run_pipeline(dsht_plan_s* p, const double* theta, const double* phi, const double* w, int64_t N, int mode,
                  double* alm, const Workspace& ws, cudaStream_t s);
+// The stages after the sort: bin sums, fold, contraction, rotation.
+int run_after_sort(dsht_plan_s* p, int64_t N, int mode, double* alm, const Workspace& ws, cudaStream_t s,
+                   bool marks);
+// Several weight maps (float or double, map k at w + k * w_stride) on one point set.
+int run_maps(dsht_plan_s* p, const double* theta, const double* phi, const void* w, int w_f32, int64_t N,
+             int nmaps, int64_t w_stride, int mode, double* alm, const Workspace& ws, cudaStream_t s);
 // After the stream has been synchronised: fold the stage events into the plan's totals.
 void collect_profile(dsht_plan_s* p);
 // Map device flag bits to a DSHT status code (and set the error message).

@@ -199,9 +199,22 @@ scan_kernel(int nkeys, int nbins, int piece_max, int64_t pmax, const uint32_t* _
   }
 }
 
+// Hermite weights of one point, in the rounding order of sht/sht.py:239-240.
+__device__ __forceinline__ void hermite(double t, double wi, double* out4) {
+  const double omt = __dadd_rn(1.0, -t);
+  const double omt2 = __dmul_rn(omt, omt);
+  const double t2 = __dmul_rn(t, t);
+  out4[0] = __dmul_rn(wi, __dmul_rn(__dadd_rn(__dmul_rn(2.0, t), 1.0), omt2));
+  out4[1] = __dmul_rn(wi, __dmul_rn(t, omt2));
+  out4[2] = __dmul_rn(wi, __dmul_rn(t2, __dadd_rn(3.0, -__dmul_rn(2.0, t))));
+  out4[3] = __dmul_rn(wi, __dmul_rn(t2, __dadd_rn(t, -1.0)));
+}
+
+template <typename WT>
 __global__ void __launch_bounds__(kPointThreads)
-scatter_kernel(Geometry g, const double* __restrict__ w, int64_t N, const uint32_t* __restrict__ keys,
-               const double* __restrict__ rec, uint32_t* __restrict__ cursor, double* __restrict__ pay) {
+scatter_kernel(Geometry g, const WT* __restrict__ w, int64_t N, const uint32_t* __restrict__ keys,
+               const double* __restrict__ rec, uint32_t* __restrict__ cursor, double* __restrict__ pay,
+               uint32_t* __restrict__ sidx, double* __restrict__ st) {
   extern __shared__ uint32_t loc[];  // [nkeys] local counts, then local bases
   const int64_t lo = (int64_t)blockIdx.x * kScatterTile;
   const int64_t hi = min(lo + (int64_t)kScatterTile, N);
@@ -221,29 +234,47 @@ scatter_kernel(Geometry g, const double* __restrict__ w, int64_t N, const uint32
     const uint32_t k = keys[i];
     if (k == DSHT_KEY_DROP) continue;
     const uint32_t pos = atomicAdd(&loc[k], 1u);
-    // Same rounding order as the numpy expressions of sht/sht.py:239-240.
-    const double t = rec[3 * i + 2], wi = w[i];
-    const double omt = __dadd_rn(1.0, -t);
-    const double omt2 = __dmul_rn(omt, omt);
-    const double t2 = __dmul_rn(t, t);
+    const double t = rec[3 * i + 2];
+    double h[4];
+    hermite(t, (double)w[i], h);
     double2* out = reinterpret_cast<double2*>(pay + (size_t)6 * pos);
     out[0] = make_double2(rec[3 * i], rec[3 * i + 1]);
-    out[1] = make_double2(__dmul_rn(wi, __dmul_rn(__dadd_rn(__dmul_rn(2.0, t), 1.0), omt2)),
-                          __dmul_rn(wi, __dmul_rn(t, omt2)));
-    out[2] = make_double2(__dmul_rn(wi, __dmul_rn(t2, __dadd_rn(3.0, -__dmul_rn(2.0, t)))),
-                          __dmul_rn(wi, __dmul_rn(t2, __dadd_rn(t, -1.0))));
+    out[1] = make_double2(h[0], h[1]);
+    out[2] = make_double2(h[2], h[3]);
+    if (sidx) {
+      sidx[pos] = (uint32_t)i;
+      st[pos] = t;
+    }
+  }
+}
+
+// Rebuild the weighted part of the sorted payload for another weight map (multi-map
+// transforms share the sort): g_k(pos) = w[sidx[pos]] h_k(t[pos]).
+template <typename WT>
+__global__ void __launch_bounds__(kPointThreads)
+gather_kernel(int64_t N, const uint32_t* __restrict__ total, const uint32_t* __restrict__ sidx,
+              const double* __restrict__ st, const WT* __restrict__ w, double* __restrict__ pay) {
+  const int64_t n = (int64_t)*total;
+  for (int64_t pos = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; pos < n && pos < N;
+       pos += (int64_t)gridDim.x * blockDim.x) {
+    double h[4];
+    hermite(st[pos], (double)w[sidx[pos]], h);
+    double2* out = reinterpret_cast<double2*>(pay + (size_t)6 * pos);
+    out[1] = make_double2(h[0], h[1]);
+    out[2] = make_double2(h[2], h[3]);
   }
 }
 
 }  // namespace
 
-void launch_points(const Geometry& g, const double* theta, const double* phi, const double* w,
+void launch_points(const Geometry& g, const double* theta, const double* phi, const void* w, int w_f32,
                    int64_t N, int mode, const Workspace& ws, cudaStream_t s) {
   cudaMemsetAsync(ws.count, 0, sizeof(uint32_t) * (g.nkeys + 1), s);
   cudaMemsetAsync(ws.flags, 0, sizeof(unsigned), s);
   const size_t hsmem = sizeof(uint32_t) * g.nkeys;
   cudaFuncSetAttribute(count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem);
-  cudaFuncSetAttribute(scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem);
+  cudaFuncSetAttribute(scatter_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem);
+  cudaFuncSetAttribute(scatter_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem);
   if (N > 0) {
     int64_t blocks = (N + kPointThreads * 8 - 1) / (kPointThreads * 8);
     if (blocks > 148 * 8) blocks = 148 * 8;
@@ -257,10 +288,28 @@ void launch_points(const Geometry& g, const double* theta, const double* phi, co
   count_launches(1);
   if (N > 0) {
     const int64_t blocks = (N + kScatterTile - 1) / kScatterTile;
-    scatter_kernel<<<(unsigned)blocks, kPointThreads, hsmem, s>>>(g, w, N, ws.key, ws.rec, ws.cursor,
-                                                                 ws.pay);
+    if (w_f32)
+      scatter_kernel<float><<<(unsigned)blocks, kPointThreads, hsmem, s>>>(
+          g, reinterpret_cast<const float*>(w), N, ws.key, ws.rec, ws.cursor, ws.pay, ws.sidx, ws.st);
+    else
+      scatter_kernel<double><<<(unsigned)blocks, kPointThreads, hsmem, s>>>(
+          g, reinterpret_cast<const double*>(w), N, ws.key, ws.rec, ws.cursor, ws.pay, ws.sidx, ws.st);
     count_launches(1);
   }
+}
+
+void launch_gather(const Geometry& g, const void* w, int w_f32, int64_t N, const Workspace& ws, cudaStream_t s) {
+  if (N <= 0) return;
+  int64_t blocks = (N + kPointThreads - 1) / kPointThreads;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  const uint32_t* total = ws.offset + g.nkeys;
+  if (w_f32)
+    gather_kernel<float><<<(unsigned)blocks, kPointThreads, 0, s>>>(N, total, ws.sidx, ws.st,
+                                                                    reinterpret_cast<const float*>(w), ws.pay);
+  else
+    gather_kernel<double><<<(unsigned)blocks, kPointThreads, 0, s>>>(N, total, ws.sidx, ws.st,
+                                                                     reinterpret_cast<const double*>(w), ws.pay);
+  count_launches(1);
 }
 
 }  // namespace dsht

@@ -170,6 +170,49 @@ class DirectSHT:
         L.check(rc)
         return alm
 
+    def call_maps(self, t, p, wts):
+        """alm of several weight maps on one point set: row k is ``self(t, p, wts[k])``.
+
+        The reference has no multi-map call; its users loop ``__call__``
+        (``sht/sht.py:112-150``) over the maps.  ``wts`` has shape (nmaps, N), float64 or
+        float32 (float32 weights are used exactly, without a float64 copy).  The points
+        are classified and sorted once.  Returns complex128 alm of shape (nmaps, Nlm).
+        """
+        on_device = isinstance(t, torch.Tensor) and t.is_cuda
+        n = len(t)
+        if isinstance(wts, torch.Tensor):
+            wd = wts.to(device=self.device)
+        else:
+            wd = torch.from_numpy(np.ascontiguousarray(np.asarray(wts)))
+        if wd.dim() == 1:
+            wd = wd[None, :]
+        if wd.dtype not in (torch.float32, torch.float64):
+            wd = wd.to(torch.float64)
+        if not (len(t) == len(p) and wd.shape[1] == len(p)):
+            raise AssertionError("theta,phi,wt must be the same length.")
+        nmaps = int(wd.shape[0])
+        dtype = L.DSHT_W_F32 if wd.dtype == torch.float32 else L.DSHT_W_F64
+        with torch.cuda.device(self.device):
+            td = _as_device_f64(t, self.device)
+            pd = _as_device_f64(p, self.device)
+            wd = wd.to(device=self.device).contiguous()
+            alm = torch.empty((nmaps, self.Nlm), dtype=torch.complex128, device=self.device)
+            nbytes = ct.c_size_t()
+            L.check(self._lib.dsht_workspace_size_maps(self._plan, n, nmaps, ct.byref(nbytes)))
+            ws = torch.empty(max(int(nbytes.value), 1), dtype=torch.uint8, device=self.device)
+            stream = torch.cuda.current_stream(self.device).cuda_stream
+            rc = self._lib.dsht_execute_maps(self._plan, L.ptr(td), L.ptr(pd), L.ptr(wd), dtype, n, nmaps,
+                                             wd.stride(0), L.DSHT_MODE_CALL, L.ptr(alm), L.ptr(ws), ws.numel(),
+                                             ct.c_void_p(stream))
+        if rc == L.DSHT_ERR_POLAR_RANGE:
+            print(f"AssertionError in basic_sht: theta must be in [ACos[xmax],ACos[-xmax]).")
+            alm.zero_()
+        elif rc == L.DSHT_ERR_THETA_RANGE:
+            raise AssertionError("theta must be in [ACos[xmax],ACos[-xmax]).")
+        else:
+            L.check(rc)
+        return alm if on_device else alm.cpu().numpy()
+
     def basic_sht(self, theta, phi, wt, reg_factor=1.0, verbose=True):
         """alm of points with |cos theta| < xmax, no rotation (``sht/sht.py:153-283``).
 

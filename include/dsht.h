@@ -11,6 +11,7 @@
  * Reference interfaces replaced (martinjameswhite/directsht):
  *   dsht_plan_create      DirectSHT.__init__            sht/sht.py:32-56
  *   dsht_execute          DirectSHT.__call__ / basic_sht sht/sht.py:112-150, :153-283
+ *   dsht_execute_maps     __call__ / basic_sht looped over weight maps of one point set
  *   dsht_get_row          DirectSHT.get_Ylm / get_dYlm  sht/sht.py:69-93
  *   dsht_alm2cl           DirectSHT.alm2cl              sht/sht.py:95-109
  *   dsht_index            DirectSHT.indx                sht/sht.py:58-67
@@ -109,6 +110,23 @@ int dsht_execute(dsht_plan_t plan, const double* theta, const double* phi, const
                  int64_t N, int mode, double* alm, void* workspace, size_t workspace_bytes,
                  void* stream);
 
+/* Weight dtypes of dsht_execute_maps. */
+enum { DSHT_W_F64 = 0, DSHT_W_F32 = 1 };
+
+/* Bytes of device workspace dsht_execute_maps needs for N points and nmaps maps. */
+int dsht_workspace_size_maps(dsht_plan_t plan, int64_t N, int nmaps, size_t* bytes);
+
+/* nmaps weight maps on one point set: alm of map k = DirectSHT(theta, phi, w_k)
+ * with w_k = the N weights at w + k * w_stride ELEMENTS, float64 or float32 (w_dtype);
+ * float32 weights are widened to float64 exactly.  theta, phi, w: DEVICE pointers.
+ * alm: DEVICE pointer to nmaps * 2 * Nlm doubles, map k at alm + k * 2 * Nlm.  The
+ * reference has no multi-map call: a user loops DirectSHT.__call__ (sht/sht.py:112-150)
+ * or basic_sht over the maps with the same theta, phi, and gets the same alm.  Here the
+ * points are classified and sorted once.  Other arguments as dsht_execute. */
+int dsht_execute_maps(dsht_plan_t plan, const double* theta, const double* phi, const void* w,
+                      int w_dtype, int64_t N, int nmaps, int64_t w_stride, int mode, double* alm,
+                      void* workspace, size_t workspace_bytes, void* stream);
+
 /* alm_out = alm_add + R(alm_rot): alm of points rotated by +90 deg about y rotated back to
  * the original frame with Wigner d(pi/2) (DEVICE pointers, 2*Nlm doubles each; alm_add may be
  * NULL for zeros, alm_out may alias alm_add).  Replaces healpy's
@@ -159,7 +177,9 @@ int dsht_do_transform(int Nl, int Nx, double xmax, double* Yv, double* Yd, int N
                       double* cost, double* phi, double* wt, double* carr, double* sarr);
 
 /* Stage timers (CUDA events recorded on the execute stream around every stage).
- * Stages: 0 points+sort, 1 bin sums, 2 fold, 3 contraction, 4 rotation. */
+ * Stages: 0 points+sort, 1 bin sums, 2 fold, 3 contraction, 4 rotation.  For
+ * dsht_execute_maps, stage 0 is the one sort and stages 1-4 are those of the last map
+ * (stage 1 including its payload gather). */
 enum { DSHT_STAGE_POINTS = 0, DSHT_STAGE_BIN_SUMS = 1, DSHT_STAGE_FOLD = 2, DSHT_STAGE_CONTRACT = 3,
        DSHT_STAGE_ROTATE = 4, DSHT_STAGE_COUNT = 5 };
 int dsht_profile_enable(dsht_plan_t plan, int enable);

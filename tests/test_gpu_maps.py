@@ -1,0 +1,97 @@
+"""Multi-map transforms (one point set, many weight maps) through dsht_execute_maps.
+
+Every map must give the alm of a single-map call with the same points (the reference's
+users loop DirectSHT.__call__ over maps, sht/sht.py:112-150).  FP64: within 1e-12 x
+max|alm| of the oracle; mixed levels: within 1e-7 x max|alm| of the oracle."""
+import numpy as np
+import pytest
+import torch
+
+from directsht_b200 import DirectSHT
+from oracle import dsht_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(np.asarray(b)).max(), 1e-300)
+
+
+def _points(N, seed):
+    rng = np.random.default_rng(seed)
+    th = np.arccos(rng.uniform(-1, 1, N))
+    ph = rng.uniform(0, 2 * np.pi, N)
+    return rng, th, ph
+
+
+@pytest.mark.parametrize("Nl,Nx,N,nmaps", [(64, 128, 20000, 5), (37, 50, 700, 3), (96, 192, 50000, 2)])
+def test_maps_fp64_vs_oracle(Nl, Nx, N, nmaps):
+    rng, th, ph = _points(N, 11 + Nl)
+    W = rng.normal(1.0, 0.3, (nmaps, N))
+    d = DirectSHT(Nl, Nx)
+    A = d.call_maps(th, ph, W)
+    assert A.shape == (nmaps, d.Nlm) and A.dtype == np.complex128
+    tab = O.build_tables(Nl, Nx)
+    for k in range(nmaps):
+        ref = O.direct_sht(tab, th, ph, W[k])
+        assert _rel(A[k], ref) <= 1e-12, k
+
+
+def test_maps_f32_weights_are_exact():
+    """float32 maps give the alm of their exact float64 widening."""
+    Nl, Nx, N = 64, 128, 30000
+    rng, th, ph = _points(N, 3)
+    W = rng.normal(1.0, 0.3, (4, N)).astype(np.float32)
+    d = DirectSHT(Nl, Nx)
+    A = d.call_maps(th, ph, W)
+    tab = O.build_tables(Nl, Nx)
+    for k in range(4):
+        assert _rel(A[k], O.direct_sht(tab, th, ph, W[k].astype(np.float64))) <= 1e-12
+
+
+def test_maps_strided_torch_input_stays_on_device():
+    Nl, Nx, N = 48, 96, 10000
+    rng, th, ph = _points(N, 5)
+    big = torch.tensor(rng.normal(1.0, 0.3, (3, N + 17)), device="cuda")
+    W = big[:, :N]  # row stride N + 17
+    d = DirectSHT(Nl, Nx)
+    A = d.call_maps(torch.tensor(th, device="cuda"), torch.tensor(ph, device="cuda"), W)
+    assert A.is_cuda and A.shape == (3, d.Nlm)
+    for k in range(3):
+        single = d(th, ph, W[k].cpu().numpy())
+        assert _rel(A[k].cpu().numpy(), single) <= 1e-13
+
+
+@pytest.mark.parametrize("precision", ["mixed", "mixed_f64_tables"])
+def test_maps_mixed_vs_oracle(precision):
+    Nl, Nx, N, nmaps = 128, 256, 200000, 3
+    rng, th, ph = _points(N, 21)
+    W = rng.normal(1.0, 0.3, (nmaps, N)).astype(np.float32)
+    d = DirectSHT(Nl, Nx, precision=precision)
+    A = d.call_maps(th, ph, W)
+    tab = O.build_tables(Nl, Nx)
+    for k in range(nmaps):
+        ref = O.direct_sht(tab, th, ph, W[k].astype(np.float64))
+        assert _rel(A[k], ref) <= 1e-7, (k, _rel(A[k], ref))
+
+
+def test_single_map_f32_and_one_row():
+    Nl, Nx, N = 32, 64, 5000
+    rng, th, ph = _points(N, 8)
+    w = rng.uniform(0.5, 1.5, N)
+    d = DirectSHT(Nl, Nx)
+    A = d.call_maps(th, ph, w)  # 1-D weights: one map
+    assert A.shape == (1, d.Nlm)
+    assert _rel(A[0], d(th, ph, w)) <= 1e-13
+
+
+def test_maps_empty_and_polar_failure():
+    d = DirectSHT(16, 32)
+    A = d.call_maps(np.zeros(0), np.zeros(0), np.zeros((2, 0)))
+    assert A.shape == (2, d.Nlm) and not np.any(A)
+    # xmax below sin(pi/4): cos(theta) = 0.7 at phi = 0 maps to cos(theta') = -sin(theta) = -0.714 after the rotation.
+    d2 = DirectSHT(16, 32, xmax=0.6)
+    th = np.array([np.arccos(0.7), 1.5])
+    ph = np.array([0.0, 0.2])
+    A2 = d2.call_maps(th, ph, np.ones((2, 2)))
+    assert not np.any(A2)
