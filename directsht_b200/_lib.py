@@ -26,6 +26,12 @@ DSHT_MODE_BASIC = 1
 DSHT_W_F64 = 0
 DSHT_W_F32 = 1
 
+DSHT_PLAN_DEFAULT = 0
+DSHT_PLAN_F32_TABLES = 1
+
+DSHT_TUNE_PIECE_MAX = 1
+DSHT_TUNE_MAPS_PER_PASS = 2
+
 DSHT_PREC_FP64 = 0
 DSHT_PREC_MIXED = 1
 DSHT_PREC_MIXED_F64_TABLES = 2
@@ -43,9 +49,18 @@ SIGNATURES = {
     "dsht_index": (ct.c_int64, [ct.c_int, ct.c_int, ct.c_int]),
     "dsht_workspace_size": (ct.c_int, [_vp, ct.c_int64, ct.POINTER(ct.c_size_t)]),
     "dsht_execute": (ct.c_int, [_vp, _vp, _vp, _vp, ct.c_int64, ct.c_int, _vp, _vp, ct.c_size_t, _vp]),
+    "dsht_plan_tune": (ct.c_int, [_vp, ct.c_int, ct.c_int]),
+    "dsht_plan_get_tune": (ct.c_int, [_vp, ct.c_int, ct.POINTER(ct.c_int)]),
     "dsht_workspace_size_maps": (ct.c_int, [_vp, ct.c_int64, ct.c_int, ct.POINTER(ct.c_size_t)]),
     "dsht_execute_maps": (ct.c_int, [_vp, _vp, _vp, _vp, ct.c_int, ct.c_int64, ct.c_int, ct.c_int64, ct.c_int, _vp,
                                      _vp, ct.c_size_t, _vp]),
+    "dsht_enqueue_maps": (ct.c_int, [_vp, _vp, _vp, _vp, ct.c_int, ct.c_int64, ct.c_int, ct.c_int64, ct.c_int, _vp,
+                                     _vp, _vp, ct.c_size_t, _vp]),
+    "dsht_status": (ct.c_int, [ct.c_uint, ct.c_int]),
+    "dsht_workspace_size_batch": (ct.c_int, [_vp, ct.c_int64, ct.c_int, ct.POINTER(ct.c_size_t)]),
+    "dsht_execute_batch": (ct.c_int, [_vp, ct.c_int, _vp, _vp, _vp, _vp, ct.c_int, _vp, _vp, ct.c_size_t, _vp]),
+    "dsht_enqueue_batch": (ct.c_int, [_vp, ct.c_int, _vp, _vp, _vp, _vp, ct.c_int, _vp, _vp, _vp, ct.c_size_t,
+                                      _vp]),
     "dsht_execute_noalloc": (ct.c_int, [_vp, _vp, _vp, _vp, ct.c_int64, ct.c_int, _vp, _vp]),
     "dsht_noalloc_scratch_bytes": (ct.c_size_t, []),
     "dsht_execute_host": (ct.c_int, [_vp, _dp, _dp, _dp, ct.c_int64, ct.c_int, _dp]),

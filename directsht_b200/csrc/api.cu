@@ -44,7 +44,8 @@ int default_piece_max(const Geometry& g, int64_t N) {
   return (int)p;
 }
 
-size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* base, Workspace* ws, bool maps) {
+size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* base, Workspace* ws, int fold_slots,
+                        bool multi) {
   size_t off = 0;
   auto take = [&](size_t bytes) -> uint8_t* {
     uint8_t* p = base ? base + off : nullptr;
@@ -59,6 +60,7 @@ size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* ba
   w.key = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * n));
   w.rec = reinterpret_cast<double*>(take(sizeof(double) * 3 * n));
   w.pay = reinterpret_cast<double*>(take(sizeof(double) * 6 * n));
+  const bool maps = multi;
   if (maps) {
     w.sidx = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * n));
     w.st = reinterpret_cast<double*>(take(sizeof(double) * n));
@@ -72,18 +74,43 @@ size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* ba
   w.piece_len = reinterpret_cast<int*>(take(sizeof(int) * pmax));
   w.npieces = reinterpret_cast<int*>(take(sizeof(int)));
   w.flags = reinterpret_cast<unsigned*>(take(sizeof(unsigned)));
+  if (maps) {
+    w.slot_flags = reinterpret_cast<unsigned*>(take(sizeof(unsigned) * kMaxRot));
+    w.all_flags = reinterpret_cast<unsigned*>(take(sizeof(unsigned)));
+  }
   w.partial = reinterpret_cast<double*>(take(sizeof(double) * 8 * (size_t)g.Nl * pmax));
-  w.fold = reinterpret_cast<double*>(take(sizeof(double) * 16 * (size_t)g.Nl * g.Nx));
+  // One fold per map of a contraction pass (multi-map transforms).
+  w.fold_slots = std::max(1, std::min(fold_slots, kMaxPass));
+  w.fold = reinterpret_cast<double*>(take(sizeof(double) * 16 * (size_t)g.Nl * g.Nx * w.fold_slots));
   w.tile_live = reinterpret_cast<uint8_t*>(take(2 * (size_t)ntile));
   w.tile_live2 = reinterpret_cast<uint8_t*>(take(2 * (size_t)((g.Nx + 255) / 256)));
   w.alm_equ = reinterpret_cast<double*>(take(sizeof(double) * 2 * (size_t)g.Nlm));
-  w.alm_pol = reinterpret_cast<double*>(take(sizeof(double) * 2 * (size_t)g.Nlm));
+  w.alm_pol = reinterpret_cast<double*>(take(sizeof(double) * 2 * (size_t)g.Nlm * (maps ? kMaxRot : 1)));
   w.npts = n;
   w.pmax = pmax;
   w.piece_max = piece_max;
   w.bytes = off;
   if (ws) *ws = w;
   return off;
+}
+
+int plan_piece_max(const dsht_plan_s* p, int64_t N) {
+  return p->tune_piece_max > 0 ? p->tune_piece_max : default_piece_max(p->g, N);
+}
+
+int plan_maps_per_pass(const dsht_plan_s* p) {
+  const int mx = contract_stream_max_maps(true);
+  return p->tune_maps_per_pass > 0 ? std::min(p->tune_maps_per_pass, mx) : mx;
+}
+
+Route plan_route(const dsht_plan_s* p, int64_t N) {
+  Route r{};
+  r.tc = p->precision != DSHT_PREC_FP64 && N >= DSHT_MIXED_MIN_POINTS;
+  // FP32 tables for tensor-core transforms at the MIXED level, and for every transform of a
+  // plan that holds no FP64 tables.
+  r.f32_tables = p->tm32 && ((r.tc && p->precision == DSHT_PREC_MIXED) || !p->Yv);
+  r.streamed = r.f32_tables || p->tm64;
+  return r;
 }
 
 Geometry make_geometry(int Nl, int Nx, double xmax) {
@@ -110,9 +137,9 @@ int run_after_sort(dsht_plan_s* p, int64_t N, int mode, double* alm, const Works
   };
   Workspace w2 = ws;
   // Small transforms run the FP64 stages even on a mixed-precision plan.
-  const bool mixed = p->precision != DSHT_PREC_FP64 && N >= DSHT_MIXED_MIN_POINTS;
-  const bool f32_tables = mixed && p->precision == DSHT_PREC_MIXED && p->tm32;
-  if (mixed) {
+  const Route rt = plan_route(p, N);
+  const bool f32_tables = rt.f32_tables;
+  if (rt.tc) {
     int rc = launch_bin_sums_tc(g, ws, s);
     if (rc) return rc;
     w2.partial_f32 = 1;
@@ -151,24 +178,143 @@ int run_pipeline(dsht_plan_s* p, const double* theta, const double* phi, const d
   return run_after_sort(p, N, mode, alm, ws, s, true);
 }
 
-// Several weight maps on one point set: one classification and sort (which also records the
-// input index and t of every sorted slot), then for every further map a gather rebuilds the
-// weighted payload and the later stages run again.  Stage events cover the last map.
-int run_maps(dsht_plan_s* p, const double* theta, const double* phi, const void* w, int w_f32, int64_t N,
-             int nmaps, int64_t w_stride, int mode, double* alm, const Workspace& ws, cudaStream_t s) {
-  const size_t esz = w_f32 ? sizeof(float) : sizeof(double);
-  const size_t nlm2 = 2 * (size_t)p->g.Nlm;
+// Several transforms in one call: multi-map transforms (one point set, the later maps marked
+// same_points) and batches of independent transforms on one plan.  Each point set is
+// classified and sorted once; a same_points item only gathers its weights into the sorted
+// payload.  Bin sums and the fold run per item; the contraction runs in passes of up to
+// contract_stream_max_maps items whose folds share one read of the tables; equatorial alm
+// go straight to item.alm, polar alm to a rotation slot, and every kMaxRot slots one
+// batched rotation adds them back.  Items with N < DSHT_MIXED_MIN_POINTS on a mixed plan
+// run the FP64 stages, in their own passes.
+int run_items(dsht_plan_s* p, const Item* items, int n, int mode, const Workspace& ws, cudaStream_t s) {
+  const Geometry& g = p->g;
+  const int64_t nlm2 = 2 * g.Nlm;
+  const int64_t fold_stride = 4 * (int64_t)g.Nl * g.Nx;  // F4 elements per fold
+  const int ntile2 = (g.Nx + 255) / 256;
+  auto ev = [&](int i) {
+    if (p->prof) cudaEventRecord(p->ev[i], s);
+  };
   p->prof_maps = true;
-  if (p->prof) cudaEventRecord(p->ev[0], s);
-  launch_points(p->g, theta, phi, w, w_f32, N, mode, ws, s);
-  if (p->prof) cudaEventRecord(p->ev[1], s);
-  for (int k = 0; k < nmaps; ++k) {
-    const bool last = k == nmaps - 1;
-    if (last && p->prof) cudaEventRecord(p->ev[DSHT_STAGE_COUNT + 1], s);
-    if (k > 0) launch_gather(p->g, static_cast<const uint8_t*>(w) + esz * (size_t)w_stride * k, w_f32, N, ws, s);
-    int rc = run_after_sort(p, N, mode, alm + nlm2 * k, ws, s, last);
+  DSHT_CUDA_OK(cudaMemsetAsync(ws.all_flags, 0, sizeof(unsigned), s));
+  // Items in two classes by the precision their size selects; same_points chains stay whole
+  // (they share N, hence the class).
+  std::vector<int> order[2];
+  for (int i = 0; i < n; ++i) order[plan_route(p, items[i].N).tc ? 1 : 0].push_back(i);
+  int sorted_item = -1;  // item whose sort the workspace holds
+  bool first_ev = true;
+  for (int cls = 0; cls < 2; ++cls) {
+    const std::vector<int>& list = order[cls];
+    if (list.empty()) continue;
+    const Route rt = plan_route(p, items[list[0]].N);
+    const bool mixed = rt.tc;
+    const bool f32_tables = rt.f32_tables;
+    const bool streamed = rt.streamed;
+    const int G = f32_tables ? ws.fold_slots : 1;
+    const size_t f4 = f32_tables ? sizeof(float4) : sizeof(double4);
+    std::vector<int> pass, pend;          // item indices; slot of pass[k] = pend.size() + k
+    auto flush_rotation = [&]() -> int {  // rotate and publish every pending item
+      if (pend.empty()) return DSHT_OK;
+      RotMaps rm{};
+      StatusOut so{};
+      for (size_t k = 0; k < pend.size(); ++k) {
+        rm.rot[k] = ws.alm_pol + nlm2 * k;
+        rm.io[k] = items[pend[k]].alm;
+        rm.flags[k] = ws.slot_flags + k;
+        so.slot[k] = ws.slot_flags + k;
+        so.status[k] = items[pend[k]].status;
+      }
+      if (mode == DSHT_MODE_CALL) launch_rotate_back_maps(g, rm, (int)pend.size(), s);
+      launch_publish_flags(so, (int)pend.size(), ws.all_flags, s);
+      pend.clear();
+      return DSHT_OK;
+    };
+    auto run_pass = [&]() -> int {
+      if (pass.empty()) return DSHT_OK;
+      const int base = (int)pend.size();
+      if (streamed) {
+        MapOut out{};
+        for (size_t k = 0; k < pass.size(); ++k) {
+          out.equ[k] = items[pass[k]].alm;
+          out.pol[k] = ws.alm_pol + nlm2 * (base + k);
+        }
+        launch_contract_pass(g, f32_tables, f32_tables ? p->tmYv32 : p->tmYv, f32_tables ? p->tmYd32 : p->tmYd,
+                             ws.fold, fold_stride, (int)pass.size(), ws.tile_live2, out, ws.slot_flags + base, s);
+      }
+      for (int it : pass) pend.push_back(it);
+      pass.clear();
+      if (pend.size() + G > (size_t)kMaxRot) return flush_rotation();
+      return DSHT_OK;
+    };
+    for (size_t li = 0; li < list.size(); ++li) {
+      const int i = list[li];
+      const Item& item = items[i];
+      const bool last = li + 1 == list.size() && cls == 1 - (order[1].empty() ? 1 : 0);
+      const int slot = (int)(pend.size() + pass.size());
+      Workspace w2 = ws;
+      w2.flags = ws.slot_flags + slot;
+      if (p->prof && first_ev) {
+        ev(0);
+      }
+      if (item.same_points && sorted_item >= 0) {
+        launch_gather(g, item.w, item.w_f32, item.N, ws, s);
+      } else {
+        // The sort keeps the input index and t of every slot when later items share it.
+        Workspace wp = ws;
+        const bool shared = li + 1 < list.size() && items[list[li + 1]].same_points;
+        if (!shared) {
+          wp.sidx = nullptr;
+          wp.st = nullptr;
+        }
+        launch_points(g, item.theta, item.phi, item.w, item.w_f32, item.N, mode, wp, s);
+        sorted_item = i;
+      }
+      if (p->prof && first_ev) {
+        ev(1);
+        first_ev = false;
+      }
+      if (last) ev(DSHT_STAGE_COUNT + 1);
+      DSHT_CUDA_OK(cudaMemcpyAsync(w2.flags, ws.flags, sizeof(unsigned), cudaMemcpyDeviceToDevice, s));
+      if (mixed) {
+        int rc = launch_bin_sums_tc(g, w2, s);
+        if (rc) return rc;
+        w2.partial_f32 = 1;
+      } else {
+        launch_bin_sums_fp64(g, w2, s);
+        w2.partial_f32 = 0;
+      }
+      if (last) ev(2);
+      if (streamed) {
+        if (pass.empty()) DSHT_CUDA_OK(cudaMemsetAsync(ws.tile_live2, 0, 2 * (size_t)ntile2, s));
+        w2.fold_f32 = f32_tables ? 1 : 0;
+        w2.fold = reinterpret_cast<double*>(reinterpret_cast<uint8_t*>(ws.fold) + f4 * fold_stride * pass.size());
+        w2.live_or = 1;
+        launch_fold(g, w2, s);
+        if (last) ev(3);
+        pass.push_back(i);
+        if ((int)pass.size() == G || li + 1 == list.size()) {
+          int rc = run_pass();
+          if (rc) return rc;
+        }
+      } else {  // tables without the streaming layout: the single-transform stages
+        w2.fold_f32 = 0;
+        w2.alm_pol = ws.alm_pol + nlm2 * slot;
+        w2.alm_equ = item.alm;
+        launch_fold(g, w2, s);
+        if (last) ev(3);
+        launch_contract_fp64(g, p->Yv, p->Yd, w2, s);
+        pend.push_back(i);
+        if (pend.size() + 1 > (size_t)kMaxRot) {
+          int rc = flush_rotation();
+          if (rc) return rc;
+        }
+      }
+      if (last) ev(4);
+    }
+    int rc = flush_rotation();
     if (rc) return rc;
   }
+  ev(5);
+  DSHT_CUDA_OK(cudaGetLastError());
   return DSHT_OK;
 }
 
@@ -209,7 +355,9 @@ static int ensure_plan_workspace(dsht_plan_s* p, size_t bytes) {
 
 using namespace dsht;
 
+
 extern "C" {
+static size_t call_layout(dsht_plan_s* p, int64_t N, int ntrans, bool multi, uint8_t* base, Workspace* ws);
 
 const char* dsht_last_error(void) { return g_last_error.c_str(); }
 
@@ -218,38 +366,58 @@ const char* dsht_version(void) { return "directsht_b200 0.1 (sm_100a)"; }
 int64_t dsht_index(int Nl, int ell, int m) { return hp_index(ell, m, Nl); }
 
 int dsht_plan_create(int Nl, int Nx, double xmax, int flags, dsht_plan_t* plan) {
-  (void)flags;
   if (!plan) return set_error(DSHT_ERR_INVALID, "plan pointer is NULL");
   *plan = nullptr;
   if (Nl < 1 || Nx < 2 || !(xmax > 0.0 && xmax < 1.0) || Nl > 16384 || Nx > 65536)
     return set_error(DSHT_ERR_INVALID, "invalid sizes Nl=%d Nx=%d xmax=%g", Nl, Nx, xmax);
+  if (flags & ~DSHT_PLAN_F32_TABLES) return set_error(DSHT_ERR_INVALID, "unknown plan flags %d", flags);
+  const bool f32_only = (flags & DSHT_PLAN_F32_TABLES) != 0;
+  if (f32_only && (Nx % 4 != 0 || Nl > 2048))
+    return set_error(DSHT_ERR_INVALID, "FP32-table plans need Nx %% 4 == 0 and Nl <= 2048 (Nl=%d Nx=%d)", Nl, Nx);
   dsht_plan_s* p = new dsht_plan_s();
   p->g = make_geometry(Nl, Nx, xmax);
   cudaGetDevice(&p->device);
-  const size_t tb = sizeof(double) * (size_t)p->g.Nlm * Nx;
-  cudaError_t e = cudaMalloc(&p->Yv, tb);
-  if (e == cudaSuccess) e = cudaMalloc(&p->Yd, tb);
-  if (e == cudaSuccess) e = cudaMallocHost(&p->h_flags, sizeof(unsigned));
-  if (e != cudaSuccess) {
+  auto fail = [&](cudaError_t e, const char* what) {
     cudaFree(p->Yv);
     cudaFree(p->Yd);
-    delete p;
-    return set_cuda_error(e, "plan allocation", __FILE__, __LINE__);
-  }
-  launch_tables(p->g, p->Yv, p->Yd, 0);
-  e = cudaDeviceSynchronize();
-  if (e == cudaSuccess) e = cudaGetLastError();
-  if (e != cudaSuccess) {
-    cudaFree(p->Yv);
-    cudaFree(p->Yd);
+    cudaFree(p->Yv32);
+    cudaFree(p->Yd32);
     cudaFreeHost(p->h_flags);
     delete p;
-    return set_cuda_error(e, "table build", __FILE__, __LINE__);
+    cudaGetLastError();
+    return set_cuda_error(e, what, __FILE__, __LINE__);
+  };
+  cudaError_t e = cudaMallocHost(&p->h_flags, sizeof(unsigned));
+  if (f32_only) {
+    const size_t tb = sizeof(float) * (size_t)p->g.Nlm * Nx;
+    if (e == cudaSuccess) e = cudaMalloc(&p->Yv32, tb);
+    if (e == cudaSuccess) e = cudaMalloc(&p->Yd32, tb);
+    if (e != cudaSuccess) return fail(e, "plan allocation");
+    launch_tables_f32(p->g, p->Yv32, p->Yd32, 0);
+  } else {
+    const size_t tb = sizeof(double) * (size_t)p->g.Nlm * Nx;
+    if (e == cudaSuccess) e = cudaMalloc(&p->Yv, tb);
+    if (e == cudaSuccess) e = cudaMalloc(&p->Yd, tb);
+    if (e != cudaSuccess) return fail(e, "plan allocation");
+    launch_tables(p->g, p->Yv, p->Yd, 0);
   }
-  if (contract_stream_ok(p->g, sizeof(double)) &&
-      make_table_tmap(&p->tmYv, p->Yv, sizeof(double), Nx, p->g.Nlm) == DSHT_OK &&
-      make_table_tmap(&p->tmYd, p->Yd, sizeof(double), Nx, p->g.Nlm) == DSHT_OK)
+  e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(e, "table build");
+  if (f32_only) {
+    if (!(contract_stream_ok(p->g, sizeof(float)) &&
+          make_table_tmap(&p->tmYv32, p->Yv32, sizeof(float), Nx, p->g.Nlm) == DSHT_OK &&
+          make_table_tmap(&p->tmYd32, p->Yd32, sizeof(float), Nx, p->g.Nlm) == DSHT_OK)) {
+      dsht_plan_destroy(p);
+      return DSHT_ERR_CUDA;
+    }
+    p->tm32 = true;
+    p->precision = DSHT_PREC_MIXED;
+  } else if (contract_stream_ok(p->g, sizeof(double)) &&
+             make_table_tmap(&p->tmYv, p->Yv, sizeof(double), Nx, p->g.Nlm) == DSHT_OK &&
+             make_table_tmap(&p->tmYd, p->Yd, sizeof(double), Nx, p->g.Nlm) == DSHT_OK) {
     p->tm64 = true;
+  }
   *plan = p;
   return DSHT_OK;
 }
@@ -276,6 +444,8 @@ int dsht_set_precision(dsht_plan_t p, int precision) {
     return set_error(DSHT_ERR_INVALID, "unknown precision %d", precision);
   if (precision != DSHT_PREC_FP64 && p->g.Nl > 2048)
     return set_error(DSHT_ERR_INVALID, "mixed precision supports Nl <= 2048 (Nl=%d)", p->g.Nl);
+  if (!p->Yv && precision != DSHT_PREC_MIXED)
+    return set_error(DSHT_ERR_INVALID, "this plan holds FP32 tables only (DSHT_PLAN_F32_TABLES): precision MIXED");
   std::lock_guard<std::mutex> lock(p->mu);
   if (precision == DSHT_PREC_MIXED && !p->Yv32) {
     const size_t tb = sizeof(float) * (size_t)p->g.Nlm * p->g.Nx;
@@ -298,6 +468,32 @@ int dsht_set_precision(dsht_plan_t p, int precision) {
       p->tm32 = true;
   }
   p->precision = precision;
+  return DSHT_OK;
+}
+
+int dsht_plan_tune(dsht_plan_t p, int param, int value) {
+  if (!p) return set_error(DSHT_ERR_INVALID, "plan is NULL");
+  std::lock_guard<std::mutex> lock(p->mu);
+  switch (param) {
+    case DSHT_TUNE_PIECE_MAX:
+      if (value != 0 && (value < 256 || value > 2048 || value % 32))
+        return set_error(DSHT_ERR_INVALID, "piece size %d: 0 or a multiple of 32 in [256, 2048]", value);
+      p->tune_piece_max = value;
+      return DSHT_OK;
+    case DSHT_TUNE_MAPS_PER_PASS:
+      if (value < 0 || value > contract_stream_max_maps(true))
+        return set_error(DSHT_ERR_INVALID, "maps per pass %d: 0 (most) or 1..%d", value, contract_stream_max_maps(true));
+      p->tune_maps_per_pass = value;
+      return DSHT_OK;
+  }
+  return set_error(DSHT_ERR_INVALID, "unknown tuning parameter %d", param);
+}
+
+int dsht_plan_get_tune(dsht_plan_t p, int param, int* value) {
+  if (!p || !value) return set_error(DSHT_ERR_INVALID, "invalid arguments");
+  if (param == DSHT_TUNE_PIECE_MAX) *value = p->tune_piece_max;
+  else if (param == DSHT_TUNE_MAPS_PER_PASS) *value = p->tune_maps_per_pass;
+  else return set_error(DSHT_ERR_INVALID, "unknown tuning parameter %d", param);
   return DSHT_OK;
 }
 
@@ -344,13 +540,37 @@ int dsht_plan_info(dsht_plan_t p, int* Nl, int* Nx, double* xmax, int64_t* Nlm) 
 
 int dsht_workspace_size(dsht_plan_t p, int64_t N, size_t* bytes) {
   if (!p || !bytes || N < 0) return set_error(DSHT_ERR_INVALID, "invalid arguments");
-  *bytes = workspace_layout(p->g, N, default_piece_max(p->g, N), nullptr, nullptr);
+  *bytes = call_layout(p, N, 1, false, nullptr, nullptr);
   return DSHT_OK;
 }
 
-static int execute_device(dsht_plan_t p, const double* theta, const double* phi, const void* w, int w_dtype,
-                          int64_t N, int nmaps, int64_t w_stride, int mode, double* alm, void* workspace,
-                          size_t workspace_bytes, void* stream) {
+// Workspace of a call: single transforms use the lean layout; multi-transform calls add
+// the gather records, fold slots, rotation slots and flag slots.
+static size_t call_layout(dsht_plan_s* p, int64_t N, int ntrans, bool multi, uint8_t* base, Workspace* ws) {
+  const int slots = multi ? std::min(std::max(ntrans, 1), plan_maps_per_pass(p)) : 1;
+  return workspace_layout(p->g, N, plan_piece_max(p, N), base, ws, slots, multi);
+}
+
+// Resolves the workspace (caller's or the plan's, grown on demand) for a call.
+static int call_workspace(dsht_plan_s* p, size_t need, void* workspace, size_t workspace_bytes,
+                          std::unique_lock<std::mutex>& lock, uint8_t** base) {
+  *base = reinterpret_cast<uint8_t*>(workspace);
+  if (*base) {
+    if (workspace_bytes < need)
+      return set_error(DSHT_ERR_NOMEM, "workspace of %zu bytes is smaller than the %zu needed", workspace_bytes, need);
+    return DSHT_OK;
+  }
+  lock.lock();
+  int rc = ensure_plan_workspace(p, need);
+  if (rc) return rc;
+  *base = reinterpret_cast<uint8_t*>(p->ws);
+  return DSHT_OK;
+}
+
+// Enqueues nmaps maps of one point set; sync = false leaves the flags in *status (device).
+static int maps_device(dsht_plan_t p, const double* theta, const double* phi, const void* w, int w_dtype,
+                       int64_t N, int nmaps, int64_t w_stride, int mode, double* alm, void* workspace,
+                       size_t workspace_bytes, void* stream, bool sync, unsigned* status) {
   if (!p || !alm || N < 0 || (N > 0 && (!theta || !phi || !w)))
     return set_error(DSHT_ERR_INVALID, "invalid arguments");
   if (mode != DSHT_MODE_CALL && mode != DSHT_MODE_BASIC) return set_error(DSHT_ERR_INVALID, "bad mode %d", mode);
@@ -360,33 +580,96 @@ static int execute_device(dsht_plan_t p, const double* theta, const double* phi,
   if (N > (int64_t)0xfffffff0LL) return set_error(DSHT_ERR_INVALID, "too many points (%lld)", (long long)N);
   if (N == 0 && mode == DSHT_MODE_BASIC)
     return set_error(DSHT_ERR_EMPTY, "The theta array seems to be empty!");
-  const bool maps = nmaps > 1;
+  if (!sync && !workspace) return set_error(DSHT_ERR_INVALID, "an enqueued call needs a caller workspace");
+  const bool multi = nmaps > 1 || w_dtype == DSHT_W_F32;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   std::unique_lock<std::mutex> lock(p->mu, std::defer_lock);
-  const int piece_max = default_piece_max(p->g, N);
-  const size_t need = workspace_layout(p->g, N, piece_max, nullptr, nullptr, maps);
-  uint8_t* base = reinterpret_cast<uint8_t*>(workspace);
-  if (base) {
-    if (workspace_bytes < need)
-      return set_error(DSHT_ERR_NOMEM, "workspace of %zu bytes is smaller than the %zu needed", workspace_bytes, need);
-  } else {
-    lock.lock();
-    int rc = ensure_plan_workspace(p, need);
-    if (rc) return rc;
-    base = reinterpret_cast<uint8_t*>(p->ws);
-  }
+  const size_t need = call_layout(p, N, nmaps, multi, nullptr, nullptr);
+  uint8_t* base = nullptr;
+  int rc = call_workspace(p, need, workspace, workspace_bytes, lock, &base);
+  if (rc) return rc;
   if (N == 0) {  // __call__ on no points returns zeros (sht/sht.py:127,150)
     DSHT_CUDA_OK(cudaMemsetAsync(alm, 0, sizeof(double) * 2 * p->g.Nlm * nmaps, s));
+    if (status) DSHT_CUDA_OK(cudaMemsetAsync(status, 0, sizeof(unsigned), s));
     return DSHT_OK;
   }
   Workspace ws;
-  workspace_layout(p->g, N, piece_max, base, &ws, maps);
-  int rc = maps || w_dtype == DSHT_W_F32
-               ? run_maps(p, theta, phi, w, w_dtype == DSHT_W_F32, N, nmaps, w_stride, mode, alm, ws, s)
-               : run_pipeline(p, theta, phi, static_cast<const double*>(w), N, mode, alm, ws, s);
+  call_layout(p, N, nmaps, multi, base, &ws);
+  const unsigned* flags = ws.flags;
+  if (multi) {
+    std::vector<Item> items(nmaps);
+    const size_t esz = w_dtype == DSHT_W_F32 ? sizeof(float) : sizeof(double);
+    for (int k = 0; k < nmaps; ++k)
+      items[k] = Item{theta, phi, static_cast<const uint8_t*>(w) + esz * (size_t)w_stride * k,
+                      w_dtype == DSHT_W_F32, N, alm + 2 * p->g.Nlm * k, k > 0, nullptr};
+    rc = run_items(p, items.data(), nmaps, mode, ws, s);
+    flags = ws.all_flags;
+  } else {
+    rc = run_pipeline(p, theta, phi, static_cast<const double*>(w), N, mode, alm, ws, s);
+  }
   if (rc) return rc;
+  if (!sync) {
+    if (status) DSHT_CUDA_OK(cudaMemcpyAsync(status, flags, sizeof(unsigned), cudaMemcpyDeviceToDevice, s));
+    return DSHT_OK;
+  }
   unsigned hf = 0;
-  DSHT_CUDA_OK(cudaMemcpyAsync(&hf, ws.flags, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  DSHT_CUDA_OK(cudaMemcpyAsync(&hf, flags, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  DSHT_CUDA_OK(cudaStreamSynchronize(s));
+  collect_profile(p);
+  return flags_to_status(hf, mode);
+}
+
+static int execute_device(dsht_plan_t p, const double* theta, const double* phi, const void* w, int w_dtype,
+                          int64_t N, int nmaps, int64_t w_stride, int mode, double* alm, void* workspace,
+                          size_t workspace_bytes, void* stream) {
+  return maps_device(p, theta, phi, w, w_dtype, N, nmaps, w_stride, mode, alm, workspace, workspace_bytes, stream,
+                     true, nullptr);
+}
+
+// Enqueues a batch of independent transforms on one plan.
+static int batch_device(dsht_plan_t p, int ntrans, const double* const* theta, const double* const* phi,
+                        const double* const* w, const int64_t* N, int mode, double* const* alm, unsigned* status,
+                        void* workspace, size_t workspace_bytes, void* stream, bool sync) {
+  if (!p || ntrans < 0 || (ntrans > 0 && (!theta || !phi || !w || !N || !alm)))
+    return set_error(DSHT_ERR_INVALID, "invalid arguments");
+  if (mode != DSHT_MODE_CALL && mode != DSHT_MODE_BASIC) return set_error(DSHT_ERR_INVALID, "bad mode %d", mode);
+  if (!sync && !workspace) return set_error(DSHT_ERR_INVALID, "an enqueued call needs a caller workspace");
+  int64_t nmax = 0;
+  for (int i = 0; i < ntrans; ++i) {
+    if (N[i] < 0 || N[i] > (int64_t)0xfffffff0LL || !alm[i] || (N[i] > 0 && (!theta[i] || !phi[i] || !w[i])))
+      return set_error(DSHT_ERR_INVALID, "invalid transform %d of the batch", i);
+    if (N[i] == 0 && mode == DSHT_MODE_BASIC)
+      return set_error(DSHT_ERR_EMPTY, "The theta array seems to be empty! (transform %d of the batch)", i);
+    nmax = std::max(nmax, N[i]);
+  }
+  if (ntrans == 0) return DSHT_OK;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  std::unique_lock<std::mutex> lock(p->mu, std::defer_lock);
+  const size_t need = call_layout(p, nmax, ntrans, true, nullptr, nullptr);
+  uint8_t* base = nullptr;
+  int rc = call_workspace(p, need, workspace, workspace_bytes, lock, &base);
+  if (rc) return rc;
+  // The piece layout follows the largest N: every transform uses the same workspace carve.
+  Workspace ws;
+  call_layout(p, nmax, ntrans, true, base, &ws);
+  std::vector<Item> items;
+  for (int i = 0; i < ntrans; ++i) {
+    if (N[i] == 0) {
+      DSHT_CUDA_OK(cudaMemsetAsync(alm[i], 0, sizeof(double) * 2 * p->g.Nlm, s));
+      if (status) DSHT_CUDA_OK(cudaMemsetAsync(status + i, 0, sizeof(unsigned), s));
+      continue;
+    }
+    items.push_back(Item{theta[i], phi[i], w[i], 0, N[i], alm[i], false, status ? status + i : nullptr});
+  }
+  if (!items.empty()) {
+    rc = run_items(p, items.data(), (int)items.size(), mode, ws, s);
+    if (rc) return rc;
+  } else {
+    DSHT_CUDA_OK(cudaMemsetAsync(ws.all_flags, 0, sizeof(unsigned), s));
+  }
+  if (!sync) return DSHT_OK;
+  unsigned hf = 0;
+  DSHT_CUDA_OK(cudaMemcpyAsync(&hf, ws.all_flags, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
   DSHT_CUDA_OK(cudaStreamSynchronize(s));
   collect_profile(p);
   return flags_to_status(hf, mode);
@@ -399,7 +682,8 @@ int dsht_execute(dsht_plan_t p, const double* theta, const double* phi, const do
 
 int dsht_workspace_size_maps(dsht_plan_t p, int64_t N, int nmaps, size_t* bytes) {
   if (!p || !bytes || N < 0 || nmaps < 1) return set_error(DSHT_ERR_INVALID, "invalid arguments");
-  *bytes = workspace_layout(p->g, N, default_piece_max(p->g, N), nullptr, nullptr, nmaps > 1);
+  // float32 single maps take the multi-transform layout too; size for it.
+  *bytes = call_layout(p, N, nmaps, true, nullptr, nullptr);
   return DSHT_OK;
 }
 
@@ -410,13 +694,43 @@ int dsht_execute_maps(dsht_plan_t p, const double* theta, const double* phi, con
                         stream);
 }
 
+int dsht_enqueue_maps(dsht_plan_t p, const double* theta, const double* phi, const void* w, int w_dtype, int64_t N,
+                      int nmaps, int64_t w_stride, int mode, double* alm, unsigned* status, void* workspace,
+                      size_t workspace_bytes, void* stream) {
+  return maps_device(p, theta, phi, w, w_dtype, N, nmaps, w_stride, mode, alm, workspace, workspace_bytes, stream,
+                     false, status);
+}
+
+int dsht_workspace_size_batch(dsht_plan_t p, int64_t max_N, int ntrans, size_t* bytes) {
+  if (!p || !bytes || max_N < 0 || ntrans < 1) return set_error(DSHT_ERR_INVALID, "invalid arguments");
+  *bytes = call_layout(p, max_N, ntrans, true, nullptr, nullptr);
+  return DSHT_OK;
+}
+
+int dsht_execute_batch(dsht_plan_t p, int ntrans, const double* const* theta, const double* const* phi,
+                       const double* const* w, const int64_t* N, int mode, double* const* alm, void* workspace,
+                       size_t workspace_bytes, void* stream) {
+  return batch_device(p, ntrans, theta, phi, w, N, mode, alm, nullptr, workspace, workspace_bytes, stream, true);
+}
+
+int dsht_enqueue_batch(dsht_plan_t p, int ntrans, const double* const* theta, const double* const* phi,
+                       const double* const* w, const int64_t* N, int mode, double* const* alm, unsigned* status,
+                       void* workspace, size_t workspace_bytes, void* stream) {
+  return batch_device(p, ntrans, theta, phi, w, N, mode, alm, status, workspace, workspace_bytes, stream, false);
+}
+
+int dsht_status(unsigned flags, int mode) {
+  if (mode != DSHT_MODE_CALL && mode != DSHT_MODE_BASIC) return set_error(DSHT_ERR_INVALID, "bad mode %d", mode);
+  return flags_to_status(flags, mode);
+}
+
 int dsht_execute_host(dsht_plan_t p, const double* theta, const double* phi, const double* w, int64_t N, int mode,
                       double* alm_host) {
   if (!p || !alm_host || N < 0 || (N > 0 && (!theta || !phi || !w)))
     return set_error(DSHT_ERR_INVALID, "invalid arguments");
   if (N == 0 && mode == DSHT_MODE_BASIC) return set_error(DSHT_ERR_EMPTY, "The theta array seems to be empty!");
   std::lock_guard<std::mutex> lock(p->mu);
-  const int piece_max = default_piece_max(p->g, N);
+  const int piece_max = plan_piece_max(p, N);
   const size_t need = workspace_layout(p->g, N, piece_max, nullptr, nullptr);
   int rc = ensure_plan_workspace(p, need);
   if (rc) return rc;
@@ -469,16 +783,35 @@ int dsht_rotate_back(dsht_plan_t p, const double* alm_rot, const double* alm_add
 int dsht_get_row(dsht_plan_t p, int which, int ell, int m, double* out) {
   if (!p || !out || which < 0 || which > 1 || m < 0 || ell < m || ell >= p->g.Nl)
     return set_error(DSHT_ERR_INVALID, "invalid row (which=%d, l=%d, m=%d)", which, ell, m);
-  const double* t = which == 0 ? p->Yv : p->Yd;
-  DSHT_CUDA_OK(cudaMemcpy(out, t + hp_index(ell, m, p->g.Nl) * p->g.Nx, sizeof(double) * p->g.Nx,
-                          cudaMemcpyDeviceToHost));
+  const int64_t off = hp_index(ell, m, p->g.Nl) * p->g.Nx;
+  if (p->Yv) {
+    const double* t = which == 0 ? p->Yv : p->Yd;
+    DSHT_CUDA_OK(cudaMemcpy(out, t + off, sizeof(double) * p->g.Nx, cudaMemcpyDeviceToHost));
+  } else {  // FP32-table plan: the stored values, widened
+    std::vector<float> tmp(p->g.Nx);
+    const float* t = which == 0 ? p->Yv32 : p->Yd32;
+    DSHT_CUDA_OK(cudaMemcpy(tmp.data(), t + off, sizeof(float) * p->g.Nx, cudaMemcpyDeviceToHost));
+    for (int j = 0; j < p->g.Nx; ++j) out[j] = tmp[j];
+  }
   return DSHT_OK;
 }
 
 int dsht_get_table(dsht_plan_t p, int which, double* out) {
   if (!p || !out || which < 0 || which > 1) return set_error(DSHT_ERR_INVALID, "invalid arguments");
-  const double* t = which == 0 ? p->Yv : p->Yd;
-  DSHT_CUDA_OK(cudaMemcpy(out, t, sizeof(double) * p->g.Nlm * p->g.Nx, cudaMemcpyDeviceToHost));
+  const size_t n = (size_t)p->g.Nlm * p->g.Nx;
+  if (p->Yv) {
+    const double* t = which == 0 ? p->Yv : p->Yd;
+    DSHT_CUDA_OK(cudaMemcpy(out, t, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  } else {
+    const float* t = which == 0 ? p->Yv32 : p->Yd32;
+    const size_t chunk = (size_t)1 << 24;
+    std::vector<float> tmp(std::min(n, chunk));
+    for (size_t i = 0; i < n; i += chunk) {
+      const size_t c = std::min(chunk, n - i);
+      DSHT_CUDA_OK(cudaMemcpy(tmp.data(), t + i, sizeof(float) * c, cudaMemcpyDeviceToHost));
+      for (size_t k = 0; k < c; ++k) out[i + k] = tmp[k];
+    }
+  }
   return DSHT_OK;
 }
 

@@ -70,12 +70,6 @@ __device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
   return __byte_perm(lo, hi, 0x5410);
 }
 
-// 16-byte chunk `h` (points 16h..16h+15) of row `r` in a 64-byte swizzled K-major tile
-// (8-row atoms of 512 B; address bits [4,6) are XORed with bits [7,9)).
-__device__ __forceinline__ uint4* tile_chunk(uint8_t* tile, int r, int h) {
-  return reinterpret_cast<uint4*>(tile + r * 64 + ((h ^ ((r >> 1) & 3)) << 4));
-}
-
 __device__ __forceinline__ void bar_producers() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
 __device__ __forceinline__ void bar_epilogue() { asm volatile("bar.sync 2, 128;" ::: "memory"); }
 

@@ -14,6 +14,7 @@
 // HBM bound: 2 sizeof(T) bytes of table per (l, m, node).
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <type_traits>
 
 #include "dsht_internal.cuh"
@@ -76,25 +77,28 @@ __device__ __forceinline__ void item_of(int64_t item, int Nl, int* m_out, int* g
 // FP64 tables: double tables and fold, 16 rows per item, FP64 FMAs.  FP32 tables (the
 // DSHT_PREC_MIXED level): float tables and fold, 32 rows per item, FP32 FMAs within a
 // tile and FP64 sums across tiles -- half the HBM traffic.
-template <bool kMixed>
+template <bool kMixed, int kG = 1>
 struct StageLayout {
   using T = typename std::conditional<kMixed, float, double>::type;
   using F4 = typename std::conditional<kMixed, float4, double4>::type;
   static constexpr int kRows = kMixed ? 32 : 16;
   static constexpr int kRowsPerWarp = kRows / 8;               // same parity, stride 2
   static constexpr int kTab = kRows * kTJ * sizeof(T);         // one of Yv, Yd
-  static constexpr int kFold = 4 * kTJ * sizeof(F4);           // 4 q x kTJ
-  static constexpr int kStage = 2 * kTab + kFold;
+  static constexpr int kFold = 4 * kTJ * sizeof(F4);           // 4 q x kTJ, one map
+  static constexpr int kStage = 2 * kTab + kG * kFold;
   static constexpr int kBytes = kStagesC * kStage + 128 + 128;
 };
 
-template <bool kMixed>
+// kG maps per pass (multi-map transforms): map g's fold at fold_v + g * fold_stride (F4
+// elements) and its alm at out.equ[g], out.pol[g] (2 Nlm doubles each).  The
+// table tile in shared memory serves all kG maps, so a pass reads the tables once.
+template <bool kMixed, int kG>
 __global__ void __launch_bounds__(kThreads, 1)
 contract_stream_kernel(int Nl, int Nx, int64_t nitems, const __grid_constant__ CUtensorMap tmv,
                        const __grid_constant__ CUtensorMap tmd, const void* __restrict__ fold_v,
-                       const uint8_t* __restrict__ live, int ntile, double* __restrict__ alm_equ,
-                       double* __restrict__ alm_pol, unsigned* __restrict__ err) {
-  using L = StageLayout<kMixed>;
+                       int64_t fold_stride, const uint8_t* __restrict__ live, int ntile,
+                       const MapOut out, unsigned* __restrict__ err) {
+  using L = StageLayout<kMixed, kG>;
   using T = typename L::T;
   using F4 = typename L::F4;
   constexpr int kRows = L::kRows;
@@ -139,12 +143,14 @@ contract_stream_kernel(int Nl, int Nx, int64_t nitems, const __grid_constant__ C
           uint8_t* st = smem + s * L::kStage;
           const uint32_t fold_bytes = nj * sizeof(F4);
           // The table boxes always transfer kRows x kTJ elements (zero fill out of range).
-          mbar_arrive_tx(&full[s], 2u * L::kTab + 4u * fold_bytes);
+          mbar_arrive_tx(&full[s], 2u * L::kTab + 4u * kG * fold_bytes);
           tma_load_2d(st, &tmv, j0, (int)row0, &full[s]);
           tma_load_2d(st + L::kTab, &tmd, j0, (int)row0, &full[s]);
-          for (int q = 0; q < 4; ++q)
-            bulk_g2s(st + 2 * L::kTab + q * kTJ * sizeof(F4), fold + ((size_t)m * 4 + q) * Nx + j0, fold_bytes,
-                     &full[s]);
+#pragma unroll
+          for (int gm = 0; gm < kG; ++gm)
+            for (int q = 0; q < 4; ++q)
+              bulk_g2s(st + 2 * L::kTab + gm * L::kFold + q * kTJ * sizeof(F4),
+                       fold + gm * fold_stride + ((size_t)m * 4 + q) * Nx + j0, fold_bytes, &full[s]);
           ++n;
         }
       }
@@ -160,11 +166,13 @@ contract_stream_kernel(int Nl, int Nx, int64_t nitems, const __grid_constant__ C
       int m, g;
       item_of<kRows>(item, Nl, &m, &g);
       const int l0 = m + g * kRows;
-      double acc[RW][4];
+      double acc[kG][RW][4];
 #pragma unroll
-      for (int i = 0; i < RW; ++i)
+      for (int gm = 0; gm < kG; ++gm)
 #pragma unroll
-        for (int c = 0; c < 4; ++c) acc[i][c] = 0.0;
+        for (int i = 0; i < RW; ++i)
+#pragma unroll
+          for (int c = 0; c < 4; ++c) acc[gm][i][c] = 0.0;
       for (int t = 0; t < ntile; ++t) {
         if (!live[t] && !live[ntile + t]) continue;
         const int s = n % kStagesC;
@@ -179,54 +187,71 @@ contract_stream_kernel(int Nl, int Nx, int64_t nitems, const __grid_constant__ C
           const uint8_t* st = smem + s * L::kStage;
           const T* Tv = reinterpret_cast<const T*>(st);
           const T* Td = reinterpret_cast<const T*>(st + L::kTab);
-          const F4* Fe = reinterpret_cast<const F4*>(st + 2 * L::kTab) + par * kTJ;
-          const F4* Fp = Fe + 2 * kTJ;
           const int nj = min(kTJ, Nx - t * kTJ);
-          T part[RW][4];
+          T part[kG][RW][4];
 #pragma unroll
-          for (int i = 0; i < RW; ++i)
+          for (int gm = 0; gm < kG; ++gm)
 #pragma unroll
-            for (int c = 0; c < 4; ++c) part[i][c] = (T)0;
-#pragma unroll 4
+            for (int i = 0; i < RW; ++i)
+#pragma unroll
+              for (int c = 0; c < 4; ++c) part[gm][i][c] = (T)0;
+#pragma unroll(kG == 1 ? 4 : 2)
           for (int jj = lane; jj < nj; jj += 32) {
-            const F4 fe = Fe[jj], fp = Fp[jj];
+            T v[RW], d[RW];
 #pragma unroll
             for (int i = 0; i < RW; ++i) {
               const int r = rbase + 2 * i;
-              const T v = Tv[r * kTJ + jj], d = Td[r * kTJ + jj];
-              part[i][0] = fma(v, fe.x, fma(d, fe.z, part[i][0]));
-              part[i][1] = fma(v, fe.y, fma(d, fe.w, part[i][1]));
-              part[i][2] = fma(v, fp.x, fma(d, fp.z, part[i][2]));
-              part[i][3] = fma(v, fp.y, fma(d, fp.w, part[i][3]));
+              v[i] = Tv[r * kTJ + jj];
+              d[i] = Td[r * kTJ + jj];
+            }
+#pragma unroll
+            for (int gm = 0; gm < kG; ++gm) {
+              const F4* Fe = reinterpret_cast<const F4*>(st + 2 * L::kTab + gm * L::kFold) + par * kTJ;
+              const F4 fe = Fe[jj], fp = Fe[2 * kTJ + jj];
+#pragma unroll
+              for (int i = 0; i < RW; ++i) {
+                part[gm][i][0] = fma(v[i], fe.x, fma(d[i], fe.z, part[gm][i][0]));
+                part[gm][i][1] = fma(v[i], fe.y, fma(d[i], fe.w, part[gm][i][1]));
+                part[gm][i][2] = fma(v[i], fp.x, fma(d[i], fp.z, part[gm][i][2]));
+                part[gm][i][3] = fma(v[i], fp.y, fma(d[i], fp.w, part[gm][i][3]));
+              }
             }
           }
 #pragma unroll
-          for (int i = 0; i < RW; ++i)
+          for (int gm = 0; gm < kG; ++gm)
 #pragma unroll
-            for (int c = 0; c < 4; ++c) acc[i][c] += (double)part[i][c];
+            for (int i = 0; i < RW; ++i)
+#pragma unroll
+              for (int c = 0; c < 4; ++c) acc[gm][i][c] += (double)part[gm][i][c];
         }
         __syncwarp();
         if (lane == 0) tc::mbar_arrive(&empty[s]);
         ++n;
       }
 #pragma unroll
-      for (int i = 0; i < RW; ++i)
+      for (int gm = 0; gm < kG; ++gm)
 #pragma unroll
-        for (int c = 0; c < 4; ++c)
+        for (int i = 0; i < RW; ++i)
 #pragma unroll
-          for (int o = 16; o > 0; o >>= 1) acc[i][c] += __shfl_xor_sync(0xffffffffu, acc[i][c], o);
+          for (int c = 0; c < 4; ++c)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc[gm][i][c] += __shfl_xor_sync(0xffffffffu, acc[gm][i][c], o);
       if (lane == 0) {
 #pragma unroll
-        for (int i = 0; i < RW; ++i) {
-          const int l = l0 + rbase + 2 * i;
-          if (l < Nl) {
-            const int64_t idx = hp_index(l, m, Nl);
-            alm_equ[2 * idx] = acc[i][0];
-            alm_equ[2 * idx + 1] = acc[i][1];
-            alm_pol[2 * idx] = acc[i][2];
-            alm_pol[2 * idx + 1] = acc[i][3];
+        for (int gm = 0; gm < kG; ++gm)
+#pragma unroll
+          for (int i = 0; i < RW; ++i) {
+            const int l = l0 + rbase + 2 * i;
+            if (l < Nl) {
+              const int64_t idx = hp_index(l, m, Nl);
+              double* ae = out.equ[gm];
+              double* ap = out.pol[gm];
+              ae[2 * idx] = acc[gm][i][0];
+              ae[2 * idx + 1] = acc[gm][i][1];
+              ap[2 * idx] = acc[gm][i][2];
+              ap[2 * idx + 1] = acc[gm][i][3];
+            }
           }
-        }
       }
     }
   }
@@ -242,7 +267,7 @@ bool contract_stream_ok(const Geometry& g, size_t elem_bytes) {
 }
 
 int make_table_tmap(CUtensorMap* tm, const void* base, size_t elem_bytes, int Nx, int64_t Nlm) {
-  const int kRows = elem_bytes == 8 ? StageLayout<false>::kRows : StageLayout<true>::kRows;
+  const int kRows = elem_bytes == 8 ? StageLayout<false, 1>::kRows : StageLayout<true, 1>::kRows;
   static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
   if (!encode) {
     void* fn = nullptr;
@@ -264,28 +289,54 @@ int make_table_tmap(CUtensorMap* tm, const void* base, size_t elem_bytes, int Nx
   return DSHT_OK;
 }
 
-void launch_contract_stream(const Geometry& g, bool mixed, const CUtensorMap& tmv, const CUtensorMap& tmd,
-                            const Workspace& ws, cudaStream_t s) {
+template <bool kMixed, int kG>
+static void stream_launch(const Geometry& g, const CUtensorMap& tmv, const CUtensorMap& tmd, const void* fold,
+                          int64_t fold_stride, const uint8_t* live, const MapOut& out, unsigned* flags,
+                          cudaStream_t s) {
+  using L = StageLayout<kMixed, kG>;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int ntile = (g.Nx + kTJ - 1) / kTJ;
-  const int rows = mixed ? StageLayout<true>::kRows : StageLayout<false>::kRows;
   int64_t nitems = 0;
-  for (int m = 0; m < g.Nl; ++m) nitems += (g.Nl - m + rows - 1) / rows;
+  for (int m = 0; m < g.Nl; ++m) nitems += (g.Nl - m + L::kRows - 1) / L::kRows;
   const int64_t grid = nitems < sms ? nitems : sms;
-  if (mixed) {
-    using L = StageLayout<true>;
-    cudaFuncSetAttribute(contract_stream_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kBytes);
-    contract_stream_kernel<true><<<(unsigned)grid, kThreads, L::kBytes, s>>>(
-        g.Nl, g.Nx, nitems, tmv, tmd, ws.fold, ws.tile_live2, ntile, ws.alm_equ, ws.alm_pol, ws.flags);
-  } else {
-    using L = StageLayout<false>;
-    cudaFuncSetAttribute(contract_stream_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kBytes);
-    contract_stream_kernel<false><<<(unsigned)grid, kThreads, L::kBytes, s>>>(
-        g.Nl, g.Nx, nitems, tmv, tmd, ws.fold, ws.tile_live2, ntile, ws.alm_equ, ws.alm_pol, ws.flags);
-  }
+  cudaFuncSetAttribute(contract_stream_kernel<kMixed, kG>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kBytes);
+  contract_stream_kernel<kMixed, kG><<<(unsigned)grid, kThreads, L::kBytes, s>>>(
+      g.Nl, g.Nx, nitems, tmv, tmd, fold, fold_stride, live, ntile, out, flags);
   count_launches(1);
+}
+
+void launch_contract_stream(const Geometry& g, bool mixed, const CUtensorMap& tmv, const CUtensorMap& tmd,
+                            const Workspace& ws, cudaStream_t s) {
+  MapOut out{};
+  out.equ[0] = ws.alm_equ;
+  out.pol[0] = ws.alm_pol;
+  if (mixed)
+    stream_launch<true, 1>(g, tmv, tmd, ws.fold, 0, ws.tile_live2, out, ws.flags, s);
+  else
+    stream_launch<false, 1>(g, tmv, tmd, ws.fold, 0, ws.tile_live2, out, ws.flags, s);
+}
+
+int contract_stream_max_maps(bool mixed) { return mixed ? kMaxPass : 1; }
+
+void launch_contract_pass(const Geometry& g, bool mixed, const CUtensorMap& tmv, const CUtensorMap& tmd,
+                          const void* fold, int64_t fold_stride, int nmaps, const uint8_t* live, const MapOut& out,
+                          unsigned* flags, cudaStream_t s) {
+  if (mixed && nmaps == 3)
+    stream_launch<true, 3>(g, tmv, tmd, fold, fold_stride, live, out, flags, s);
+  else if (mixed && nmaps == 2)
+    stream_launch<true, 2>(g, tmv, tmd, fold, fold_stride, live, out, flags, s);
+  else if (mixed)
+    stream_launch<true, 1>(g, tmv, tmd, fold, fold_stride, live, out, flags, s);
+  else  // FP64 tables: one map per pass (two stages of two maps' FP64 folds do not fit)
+    for (int k = 0; k < nmaps; ++k) {
+      MapOut o1{};
+      o1.equ[0] = out.equ[k];
+      o1.pol[0] = out.pol[k];
+      stream_launch<false, 1>(g, tmv, tmd, static_cast<const double4*>(fold) + fold_stride * k, 0, live, o1, flags,
+                              s);
+    }
 }
 
 }  // namespace dsht

@@ -42,6 +42,27 @@ struct Geometry {
   int nkeys;          // kSets * nbins
 };
 
+// Output pointers of one contraction pass (kernel parameter, passed by value).
+constexpr int kMaxPass = 3;
+struct MapOut {
+  double* equ[kMaxPass];
+  double* pol[kMaxPass];
+};
+
+// Maps of one batched rotation: io[k] += R(rot[k]) when *flags[k] has polar points.
+constexpr int kMaxRot = 8;
+struct RotMaps {
+  const double* rot[kMaxRot];
+  double* io[kMaxRot];
+  const unsigned* flags[kMaxRot];
+};
+
+// Flag words of finished transforms: *all |= *slot[k]; status[k] (if set) = *slot[k].
+struct StatusOut {
+  const unsigned* slot[kMaxRot];
+  unsigned* status[kMaxRot];
+};
+
 // Workspace carve-up for one execute call.
 struct Workspace {
   uint32_t* key;        // [N]
@@ -59,28 +80,44 @@ struct Workspace {
   int* npieces;         // [1]
   unsigned* flags;      // [1]
   double* partial;      // [pmax][8][Nl]
-  double* fold;         // [Nl][4][Nx][4]
+  double* fold;         // [fold_slots][Nl][4][Nx][4]
   uint8_t* tile_live;   // [2][ceil(Nx/128)] tiles of the fallback contraction
   uint8_t* tile_live2;  // [2][ceil(Nx/256)] tiles of the streaming contraction
   double* alm_equ;      // [Nlm][2]
-  double* alm_pol;      // [Nlm][2]
+  double* alm_pol;      // [Nlm][2] (x nmaps for multi-map transforms)
   int64_t npts;         // N, the stride of pay
   int partial_f32;      // partial sums stored as float (tensor-core path) instead of double
   int fold_f32;         // fold written as float4 (mixed contraction) instead of double4
   int64_t pmax;
   int piece_max;
+  int fold_slots;       // folds held at once (maps of one contraction pass)
+  int live_or;          // tile_live2 accumulates (OR) over the folds of a pass
+  unsigned* slot_flags; // [kMaxRot] flags of the transforms awaiting rotation (multi-transform calls)
+  unsigned* all_flags;  // [1] OR of every finished transform's flags
   size_t bytes;
 };
 
+// fold_slots: folds held at once (one contraction pass); multi: add the records of
+// multi-transform calls (gather indices, rotation and flag slots).
 size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* base, Workspace* ws,
-                        bool maps = false);
+                        int fold_slots = 1, bool multi = false);
 int default_piece_max(const Geometry& g, int64_t N);
+int plan_piece_max(const dsht_plan_s* p, int64_t N);
+// How a transform of N points runs on a plan: tensor-core bin sums (tc), FP32 tables
+// (f32_tables), streamed contraction (streamed; otherwise the FP64 fallback kernel).
+struct Route {
+  bool tc, f32_tables, streamed;
+};
+Route plan_route(const dsht_plan_s* p, int64_t N);
+int plan_maps_per_pass(const dsht_plan_s* p);
 
 // Kernels launched by api.cu (each file owns its launch helpers).
 void launch_tables(const Geometry& g, double* Yv, double* Yd, cudaStream_t s);
+void launch_tables_f32(const Geometry& g, float* Yv, float* Yd, cudaStream_t s);
 void launch_points(const Geometry& g, const double* theta, const double* phi, const void* w, int w_f32,
                    int64_t N, int mode, const Workspace& ws, cudaStream_t s);
 void launch_gather(const Geometry& g, const void* w, int w_f32, int64_t N, const Workspace& ws, cudaStream_t s);
+void launch_publish_flags(const StatusOut& st, int n, unsigned* all, cudaStream_t s);
 void launch_bin_sums_fp64(const Geometry& g, const Workspace& ws, cudaStream_t s);
 int launch_bin_sums_tc(const Geometry& g, const Workspace& ws, cudaStream_t s);
 int tc_inner_factor(int Nl);
@@ -90,12 +127,21 @@ void launch_contract_fp64(const Geometry& g, const double* Yv, const double* Yd,
 bool contract_stream_ok(const Geometry& g, size_t elem_bytes);
 void launch_contract_stream(const Geometry& g, bool mixed, const CUtensorMap& tmv, const CUtensorMap& tmd,
                             const Workspace& ws, cudaStream_t s);
+// One contraction pass over up to contract_stream_max_maps(mixed) folds (fold k at fold +
+// k * fold_stride F4 elements) that share one read of the tables; alm of fold k to
+// out.equ[k], out.pol[k].  FP64 tables take one fold per launch.
+int contract_stream_max_maps(bool mixed);
+void launch_contract_pass(const Geometry& g, bool mixed, const CUtensorMap& tmv, const CUtensorMap& tmd,
+                          const void* fold, int64_t fold_stride, int nmaps, const uint8_t* live, const MapOut& out,
+                          unsigned* flags, cudaStream_t s);
 // 2D tensor map over a (Nlm x Nx) table for the streaming contraction's TMA loads.
 int make_table_tmap(CUtensorMap* tm, const void* base, size_t elem_bytes, int Nx, int64_t Nlm);
 void launch_tables_to_f32(const Geometry& g, const double* Yv, const double* Yd, float* Yv32, float* Yd32,
                           cudaStream_t s);
 void launch_rotate_back(const Geometry& g, const double* alm_rot, const double* alm_add,
                         double* alm_out, const unsigned* flags, cudaStream_t s);
+// alm io[k] += R(rot[k]) for k < nmaps <= kMaxRot (a map without polar points is left as it is).
+void launch_rotate_back_maps(const Geometry& g, const RotMaps& maps, int nmaps, cudaStream_t s);
 
 // Healpy index of (l, m).
 __host__ __device__ inline int64_t hp_index(int l, int m, int Nl) {
@@ -124,6 +170,8 @@ struct dsht_plan_s {
   double* alm = nullptr;  // [2 Nlm]
   unsigned* h_flags = nullptr;  // pinned
   int precision = DSHT_PREC_FP64;
+  int tune_piece_max = 0;      // points per bin piece (0: chosen from N)
+  int tune_maps_per_pass = 0;  // maps per multi-map contraction pass (0: the most that fit)
   // Stage timers.
   bool prof = false;
   // ev[0..5]: stage boundaries; ev[6]: start of the last map's bin sums (multi-map calls,
@@ -143,9 +191,20 @@ int run_pipeline(dsht_plan_s* p, const double* theta, const double* phi, const d
 // The stages after the sort: bin sums, fold, contraction, rotation.
 int run_after_sort(dsht_plan_s* p, int64_t N, int mode, double* alm, const Workspace& ws, cudaStream_t s,
                    bool marks);
-// Several weight maps (float or double, map k at w + k * w_stride) on one point set.
-int run_maps(dsht_plan_s* p, const double* theta, const double* phi, const void* w, int w_f32, int64_t N,
-             int nmaps, int64_t w_stride, int mode, double* alm, const Workspace& ws, cudaStream_t s);
+// One transform of a multi-transform call.  same_points: the points are those of the
+// previous item (its sort is reused and only the weights are gathered again).
+struct Item {
+  const double* theta;
+  const double* phi;
+  const void* w;
+  int w_f32;
+  int64_t N;
+  double* alm;
+  bool same_points;
+  unsigned* status;  // device word that receives the item's flags, or null
+};
+// Runs the items in order; every finished item's flags are OR-ed into ws.all_flags.
+int run_items(dsht_plan_s* p, const Item* items, int n, int mode, const Workspace& ws, cudaStream_t s);
 // After the stream has been synchronised: fold the stage events into the plan's totals.
 void collect_profile(dsht_plan_s* p);
 // Map device flag bits to a DSHT status code (and set the error message).

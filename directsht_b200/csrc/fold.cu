@@ -64,7 +64,7 @@ fold_kernel(int Nl, int Nx, int nbins, double dx, const int* __restrict__ piece_
 // tile_live[h][t] = 1 when any point of the equatorial (h = 0) or polar (h = 1) sets
 // touches a node of the tile t of kContractTile nodes.
 __global__ void tile_live_kernel(int nbins, int ntile, int tile, const uint32_t* __restrict__ count,
-                                 uint8_t* __restrict__ live) {
+                                 uint8_t* __restrict__ live, int accumulate) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ntile) return;
   for (int h = 0; h < 2; ++h) {
@@ -72,7 +72,8 @@ __global__ void tile_live_kernel(int nbins, int ntile, int tile, const uint32_t*
     const int j0 = t * tile - 1, j1 = t * tile + tile;  // bins feeding nodes [t*tile, t*tile+tile)
     for (int s = 2 * h; s < 2 * h + 2; ++s)
       for (int j = max(j0, 0); j < min(j1, nbins); ++j) any |= (count[s * nbins + j] != 0);
-    live[h * ntile + t] = any;
+    if (!accumulate) live[h * ntile + t] = any;
+    else if (any) live[h * ntile + t] = 1;
   }
 }
 
@@ -87,6 +88,9 @@ void launch_fold(const Geometry& g, const Workspace& ws, cudaStream_t s) {
   double4* f64 = reinterpret_cast<double4*>(ws.fold);
   if (ws.partial_f32 && ws.fold_f32)
     fold_kernel<float, float4><<<grid, kFoldThreads, 0, s>>>(g.Nl, g.Nx, g.nbins, g.dx, ws.piece_first, pf, f32);
+  else if (ws.fold_f32)
+    fold_kernel<double, float4><<<grid, kFoldThreads, 0, s>>>(g.Nl, g.Nx, g.nbins, g.dx, ws.piece_first,
+                                                             ws.partial, f32);
   else if (ws.partial_f32)
     fold_kernel<float, double4><<<grid, kFoldThreads, 0, s>>>(g.Nl, g.Nx, g.nbins, g.dx, ws.piece_first, pf, f64);
   else
@@ -95,10 +99,11 @@ void launch_fold(const Geometry& g, const Workspace& ws, cudaStream_t s) {
   count_launches(1);
   const int tile = contract_tile();
   const int ntile = (g.Nx + tile - 1) / tile;
-  tile_live_kernel<<<(ntile + 127) / 128, 128, 0, s>>>(g.nbins, ntile, tile, ws.count, ws.tile_live);
+  tile_live_kernel<<<(ntile + 127) / 128, 128, 0, s>>>(g.nbins, ntile, tile, ws.count, ws.tile_live, 0);
   count_launches(1);
   const int ntile2 = (g.Nx + 255) / 256;
-  tile_live_kernel<<<(ntile2 + 127) / 128, 128, 0, s>>>(g.nbins, ntile2, 256, ws.count, ws.tile_live2);
+  tile_live_kernel<<<(ntile2 + 127) / 128, 128, 0, s>>>(g.nbins, ntile2, 256, ws.count, ws.tile_live2,
+                                                             ws.live_or);
   count_launches(1);
 }
 

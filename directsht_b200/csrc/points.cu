@@ -265,6 +265,14 @@ gather_kernel(int64_t N, const uint32_t* __restrict__ total, const uint32_t* __r
   }
 }
 
+__global__ void publish_flags_kernel(const StatusOut st, int n, unsigned* all) {
+  const int k = threadIdx.x;
+  if (k >= n) return;
+  const unsigned f = *st.slot[k];
+  atomicOr(all, f);
+  if (st.status[k]) *st.status[k] = f;
+}
+
 }  // namespace
 
 void launch_points(const Geometry& g, const double* theta, const double* phi, const void* w, int w_f32,
@@ -309,6 +317,12 @@ void launch_gather(const Geometry& g, const void* w, int w_f32, int64_t N, const
   else
     gather_kernel<double><<<(unsigned)blocks, kPointThreads, 0, s>>>(N, total, ws.sidx, ws.st,
                                                                      reinterpret_cast<const double*>(w), ws.pay);
+  count_launches(1);
+}
+
+void launch_publish_flags(const StatusOut& st, int n, unsigned* all, cudaStream_t s) {
+  if (n <= 0) return;
+  publish_flags_kernel<<<1, 32, 0, s>>>(st, n, all);
   count_launches(1);
 }
 

@@ -20,8 +20,10 @@ struct Coef {
   double a, b, f2, q, dc, nrm;
 };
 
+// TO = double: the FP64 tables; TO = float: the same FP64 values rounded once to float.
+template <typename TO>
 __global__ void __launch_bounds__(kTableThreads)
-table_kernel(int Nl, int Nx, double step, double* __restrict__ Yv, double* __restrict__ Yd) {
+table_kernel(int Nl, int Nx, double step, TO* __restrict__ Yv, TO* __restrict__ Yd) {
   extern __shared__ double smem_raw[];
   const int m = blockIdx.y;
   Coef* cf = reinterpret_cast<Coef*>(smem_raw);       // [Nl]
@@ -52,8 +54,8 @@ table_kernel(int Nl, int Nx, double step, double* __restrict__ Yv, double* __res
   for (int k = 1; k <= m; ++k) ymm = __dmul_rn(__dmul_rn(-smm[k], sx), ymm);
 
   const int64_t row0 = hp_index(m, m, Nl);
-  double* yv = Yv + row0 * Nx + j;
-  double* yd = Yd + row0 * Nx + j;
+  TO* yv = Yv + row0 * Nx + j;
+  TO* yd = Yd + row0 * Nx + j;
 
   // l = m
   double y2 = 0.0, y1 = ymm;  // y2 = Y_{l-2}, y1 = Y_{l-1}
@@ -65,8 +67,8 @@ table_kernel(int Nl, int Nx, double step, double* __restrict__ Yv, double* __res
       d = __ddiv_rn(__dadd_rn(0.0, -__dmul_rn(__dmul_rn((double)m, x), ymm)), omx2);
     }
     const double n = cf[m].nrm;
-    yv[0] = __dmul_rn(ymm, n);
-    yd[0] = __dmul_rn(d, n);
+    yv[0] = (TO)__dmul_rn(ymm, n);
+    yd[0] = (TO)__dmul_rn(d, n);
   }
   if (m + 1 >= Nl) return;
   // l = m + 1: Y = sqrt(2m+1) x Y_mm (sht/legendre_py.py:32-34); m = 0 row is x itself.
@@ -85,8 +87,8 @@ table_kernel(int Nl, int Nx, double step, double* __restrict__ Yv, double* __res
       d = __ddiv_rn(__dadd_rn(__dmul_rn(cf[l].dc, y1), -__dmul_rn(__dmul_rn((double)l, x), y)), omx2);
     }
     const double n = cf[l].nrm;
-    yv[(size_t)Nx] = __dmul_rn(y, n);
-    yd[(size_t)Nx] = __dmul_rn(d, n);
+    yv[(size_t)Nx] = (TO)__dmul_rn(y, n);
+    yd[(size_t)Nx] = (TO)__dmul_rn(d, n);
   }
   y2 = y1;
   y1 = y;
@@ -102,8 +104,8 @@ table_kernel(int Nl, int Nx, double step, double* __restrict__ Yv, double* __res
       d = __ddiv_rn(__dadd_rn(__dmul_rn(c.dc, y1), -__dmul_rn(__dmul_rn((double)l, x), y)), omx2);
     }
     const size_t off = (size_t)(l - m) * Nx;
-    yv[off] = __dmul_rn(y, c.nrm);
-    yd[off] = __dmul_rn(d, c.nrm);
+    yv[off] = (TO)__dmul_rn(y, c.nrm);
+    yd[off] = (TO)__dmul_rn(d, c.nrm);
     y2 = y1;
     y1 = y;
   }
@@ -126,12 +128,17 @@ void launch_tables_to_f32(const Geometry& g, const double* Yv, const double* Yd,
   count_launches(1);
 }
 
-void launch_tables(const Geometry& g, double* Yv, double* Yd, cudaStream_t s) {
+template <typename TO>
+static void tables_launch(const Geometry& g, TO* Yv, TO* Yd, cudaStream_t s) {
   const size_t smem = (size_t)g.Nl * sizeof(Coef) + (size_t)(g.Nl + 1) * sizeof(double);
-  cudaFuncSetAttribute(table_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute(table_kernel<TO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   dim3 grid((g.Nx + kTableThreads - 1) / kTableThreads, g.Nl);
-  table_kernel<<<grid, kTableThreads, smem, s>>>(g.Nl, g.Nx, g.dx, Yv, Yd);
+  table_kernel<TO><<<grid, kTableThreads, smem, s>>>(g.Nl, g.Nx, g.dx, Yv, Yd);
   count_launches(1);
 }
+
+void launch_tables(const Geometry& g, double* Yv, double* Yd, cudaStream_t s) { tables_launch(g, Yv, Yd, s); }
+
+void launch_tables_f32(const Geometry& g, float* Yv, float* Yd, cudaStream_t s) { tables_launch(g, Yv, Yd, s); }
 
 }  // namespace dsht

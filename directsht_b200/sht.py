@@ -29,7 +29,7 @@ class DirectSHT:
     """Brute-force spherical harmonic transforms on a B200 (``sht/sht.py:30``)."""
 
     def __init__(self, Nell, Nx, xmax=0.75, dflt_type="float64", null_unphysical=True, device=None,
-                 precision="fp64"):
+                 precision="fp64", f32_tables=False):
         """Build the FP64 Ylm/dYlm tables on the GPU (``sht/sht.py:32-56``).
 
         :param Nell: number of ells (and m's).
@@ -42,6 +42,8 @@ class DirectSHT:
             per-bin sums and FP32 tables: fastest, <= 1e-7 x max|alm| for point sets spread over
             many x bins) or "mixed_f64_tables" (tensor-core sums, FP64 tables: <= 1e-7 also when
             the weight concentrates in one bin).
+        :param f32_tables: keep only FP32 copies of the tables (half the memory; the plan then
+            runs at precision "mixed" only).
         """
         self._lib = L.load()
         if not torch.cuda.is_available():
@@ -55,9 +57,10 @@ class DirectSHT:
         self.x = xx
         self._plan = ct.c_void_p()
         with torch.cuda.device(self.device):
-            L.check(self._lib.dsht_plan_create(self.Nell, self.Nx, self.xmax, 0, ct.byref(self._plan)))
+            flags = L.DSHT_PLAN_F32_TABLES if f32_tables else L.DSHT_PLAN_DEFAULT
+            L.check(self._lib.dsht_plan_create(self.Nell, self.Nx, self.xmax, flags, ct.byref(self._plan)))
         self.precision = None
-        self.set_precision(precision)
+        self.set_precision("mixed" if f32_tables else precision)
         self._Yv = None
         self._Yd = None
         self.verbose_timing = None
@@ -82,6 +85,20 @@ class DirectSHT:
         self.precision = precision
 
     # -- tables ---------------------------------------------------------------------
+    def tune(self, piece_max=None, maps_per_pass=None):
+        """Set launch-shape parameters (``dsht_plan_tune``); None leaves one unchanged, 0
+        restores the automatic choice.  Returns the current values as a dict."""
+        if piece_max is not None:
+            L.check(self._lib.dsht_plan_tune(self._plan, L.DSHT_TUNE_PIECE_MAX, int(piece_max)))
+        if maps_per_pass is not None:
+            L.check(self._lib.dsht_plan_tune(self._plan, L.DSHT_TUNE_MAPS_PER_PASS, int(maps_per_pass)))
+        out = {}
+        for name, code in (("piece_max", L.DSHT_TUNE_PIECE_MAX), ("maps_per_pass", L.DSHT_TUNE_MAPS_PER_PASS)):
+            v = ct.c_int()
+            L.check(self._lib.dsht_plan_get_tune(self._plan, code, ct.byref(v)))
+            out[name] = v.value
+        return out
+
     def indx(self, ell, m):
         """Healpy index (``sht/sht.py:58-67``)."""
         return (m * (2 * self.Nell - 1 - m)) // 2 + ell
@@ -212,6 +229,53 @@ class DirectSHT:
         else:
             L.check(rc)
         return alm if on_device else alm.cpu().numpy()
+
+    def call_batch(self, point_sets, mode="call"):
+        """alm of several independent point sets, each ``(theta, phi, w)``: item i is
+        ``self(*point_sets[i])`` (or ``basic_sht`` with mode="basic").
+
+        The reference has no batch call; its users loop ``__call__`` (``sht/sht.py:112-150``).
+        Here the contraction of up to three point sets shares one read of the tables and the
+        rotation of up to eight shares one Wigner-d recursion.  Returns a list of complex128
+        alm (numpy, or CUDA tensors when the inputs are CUDA tensors).  A transform whose polar
+        points cannot be rotated into range gives zeros, as ``__call__`` does.
+        """
+        code = L.DSHT_MODE_CALL if mode == "call" else L.DSHT_MODE_BASIC
+        n = len(point_sets)
+        if n == 0:
+            return []
+        on_device = isinstance(point_sets[0][0], torch.Tensor) and point_sets[0][0].is_cuda
+        with torch.cuda.device(self.device):
+            dev = []
+            for t, p, w in point_sets:
+                if not (len(t) == len(p) and len(p) == len(w)):
+                    raise AssertionError("theta,phi,wt must be the same length.")
+                dev.append(tuple(_as_device_f64(a, self.device) for a in (t, p, w)))
+            alms = [torch.empty(self.Nlm, dtype=torch.complex128, device=self.device) for _ in range(n)]
+            Ns = (ct.c_int64 * n)(*[len(d[0]) for d in dev])
+            arr = lambda xs: (ct.c_void_p * n)(*[x.data_ptr() for x in xs])
+            status = torch.zeros(n, dtype=torch.int32, device=self.device)
+            nbytes = ct.c_size_t()
+            L.check(self._lib.dsht_workspace_size_batch(self._plan, max(Ns), n, ct.byref(nbytes)))
+            ws = torch.empty(max(int(nbytes.value), 1), dtype=torch.uint8, device=self.device)
+            stream = torch.cuda.current_stream(self.device).cuda_stream
+            rc = self._lib.dsht_enqueue_batch(self._plan, n, arr([d[0] for d in dev]), arr([d[1] for d in dev]),
+                                              arr([d[2] for d in dev]), Ns, code, arr(alms), L.ptr(status),
+                                              L.ptr(ws), ws.numel(), ct.c_void_p(stream))
+            if rc == L.DSHT_ERR_EMPTY:
+                raise ValueError("The theta array seems to be empty!")
+            L.check(rc)
+            flags = status.cpu().numpy().astype(np.uint32)
+        for i, f in enumerate(flags):
+            rc = self._lib.dsht_status(int(f), code)
+            if rc == L.DSHT_ERR_POLAR_RANGE and code == L.DSHT_MODE_CALL:
+                print(f"AssertionError in basic_sht: theta must be in [ACos[xmax],ACos[-xmax]).")
+                alms[i].zero_()
+            elif rc == L.DSHT_ERR_THETA_RANGE:
+                raise AssertionError("theta must be in [ACos[xmax],ACos[-xmax]).")
+            else:
+                L.check(rc)
+        return alms if on_device else [a.cpu().numpy() for a in alms]
 
     def basic_sht(self, theta, phi, wt, reg_factor=1.0, verbose=True):
         """alm of points with |cos theta| < xmax, no rotation (``sht/sht.py:153-283``).

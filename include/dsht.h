@@ -12,6 +12,7 @@
  *   dsht_plan_create      DirectSHT.__init__            sht/sht.py:32-56
  *   dsht_execute          DirectSHT.__call__ / basic_sht sht/sht.py:112-150, :153-283
  *   dsht_execute_maps     __call__ / basic_sht looped over weight maps of one point set
+ *   dsht_execute_batch    __call__ / basic_sht looped over point sets of one (Nl, Nx)
  *   dsht_get_row          DirectSHT.get_Ylm / get_dYlm  sht/sht.py:69-93
  *   dsht_alm2cl           DirectSHT.alm2cl              sht/sht.py:95-109
  *   dsht_index            DirectSHT.indx                sht/sht.py:58-67
@@ -53,9 +54,14 @@ enum {
   DSHT_MODE_BASIC = 1   /* DirectSHT.basic_sht: every point must be equatorial     */
 };
 
-/* Plan flags. */
+/* Plan flags.  DSHT_PLAN_F32_TABLES: keep only FP32 copies of the tables (the FP64 values
+ * rounded once; half the memory: 68.7 GB instead of 137 GB at Nl=2048, Nx=4096).  Such a
+ * plan runs at DSHT_PREC_MIXED only; transforms below DSHT_MIXED_MIN_POINTS points use FP64
+ * bin sums with the FP32 tables; dsht_get_row / dsht_get_table return the FP32 values
+ * widened to double.  Needs Nx % 4 == 0 and Nl <= 2048. */
 enum {
-  DSHT_PLAN_DEFAULT = 0
+  DSHT_PLAN_DEFAULT = 0,
+  DSHT_PLAN_F32_TABLES = 1
 };
 
 /* Arithmetic of a plan's transforms.
@@ -84,6 +90,15 @@ enum {
 int64_t dsht_mixed_min_points(void);
 int dsht_set_precision(dsht_plan_t plan, int precision);
 int dsht_get_precision(dsht_plan_t plan, int* precision);
+
+/* Launch-shape tuning of a plan (no counterpart in the reference; results do not depend on
+ * it beyond rounding).  DSHT_TUNE_PIECE_MAX: points per bin piece of the per-bin sums, a
+ * multiple of 32 in [256, 2048], 0 = chosen from N.  DSHT_TUNE_MAPS_PER_PASS: maps that
+ * share one read of the tables in the multi-map contraction, 1..3, 0 = 3.  Workspace sizes
+ * depend on both: query them after tuning. */
+enum { DSHT_TUNE_PIECE_MAX = 1, DSHT_TUNE_MAPS_PER_PASS = 2 };
+int dsht_plan_tune(dsht_plan_t plan, int param, int value);
+int dsht_plan_get_tune(dsht_plan_t plan, int param, int* value);
 
 /* Build the x grid and the FP64 Ylm/dYlm tables on the current CUDA device.
  * Replaces DirectSHT.__init__ (sht/sht.py:32-56). Nl >= 1, Nx >= 2, 0 < xmax < 1. */
@@ -126,6 +141,36 @@ int dsht_workspace_size_maps(dsht_plan_t plan, int64_t N, int nmaps, size_t* byt
 int dsht_execute_maps(dsht_plan_t plan, const double* theta, const double* phi, const void* w,
                       int w_dtype, int64_t N, int nmaps, int64_t w_stride, int mode, double* alm,
                       void* workspace, size_t workspace_bytes, void* stream);
+
+/* dsht_execute_maps without synchronisation, for CUDA-graph capture and overlapped
+ * streams: needs a caller workspace, allocates nothing, waits for nothing.  The device
+ * word *status (may be NULL) receives the transform's flags when the work has run;
+ * dsht_status(flags, mode) turns them into the DSHT_* code dsht_execute_maps would return. */
+int dsht_enqueue_maps(dsht_plan_t plan, const double* theta, const double* phi, const void* w,
+                      int w_dtype, int64_t N, int nmaps, int64_t w_stride, int mode, double* alm,
+                      unsigned* status, void* workspace, size_t workspace_bytes, void* stream);
+int dsht_status(unsigned flags, int mode);
+
+/* Batches of independent transforms on one plan (no counterpart in the reference, whose
+ * users call DirectSHT.__call__ once per point set).  Transform i: N[i] points at the
+ * DEVICE pointers theta[i], phi[i], w[i] (float64), alm to the DEVICE pointer alm[i]
+ * (2*Nlm doubles); the pointer arrays themselves are HOST arrays read during the call.
+ * Each point set is sorted on its own; the contraction serves up to 3 transforms per read
+ * of the tables (DSHT_TUNE_MAPS_PER_PASS) and the rotation up to 8.  Results equal those of
+ * one dsht_execute per transform.  The workspace (dsht_workspace_size_batch with the
+ * largest N of the batch) is used in turn by every transform.  dsht_execute_batch
+ * synchronises and returns the first error of any transform; dsht_enqueue_batch does not
+ * synchronise, allocates nothing, and writes the flags of transform i to the DEVICE word
+ * status[i] (status may be NULL). */
+int dsht_workspace_size_batch(dsht_plan_t plan, int64_t max_N, int ntrans, size_t* bytes);
+int dsht_execute_batch(dsht_plan_t plan, int ntrans, const double* const* theta,
+                       const double* const* phi, const double* const* w, const int64_t* N,
+                       int mode, double* const* alm, void* workspace, size_t workspace_bytes,
+                       void* stream);
+int dsht_enqueue_batch(dsht_plan_t plan, int ntrans, const double* const* theta,
+                       const double* const* phi, const double* const* w, const int64_t* N,
+                       int mode, double* const* alm, unsigned* status, void* workspace,
+                       size_t workspace_bytes, void* stream);
 
 /* alm_out = alm_add + R(alm_rot): alm of points rotated by +90 deg about y rotated back to
  * the original frame with Wigner d(pi/2) (DEVICE pointers, 2*Nlm doubles each; alm_add may be
@@ -178,8 +223,9 @@ int dsht_do_transform(int Nl, int Nx, double xmax, double* Yv, double* Yd, int N
 
 /* Stage timers (CUDA events recorded on the execute stream around every stage).
  * Stages: 0 points+sort, 1 bin sums, 2 fold, 3 contraction, 4 rotation.  For
- * dsht_execute_maps, stage 0 is the one sort and stages 1-4 are those of the last map
- * (stage 1 including its payload gather). */
+ * dsht_execute_maps: stage 0 is the one sort, stages 1-2 are those of the last map
+ * (stage 1 including its payload gather), stage 3 is the last contraction pass (it serves
+ * up to 3 maps) and stage 4 the rotation of all maps. */
 enum { DSHT_STAGE_POINTS = 0, DSHT_STAGE_BIN_SUMS = 1, DSHT_STAGE_FOLD = 2, DSHT_STAGE_CONTRACT = 3,
        DSHT_STAGE_ROTATE = 4, DSHT_STAGE_COUNT = 5 };
 int dsht_profile_enable(dsht_plan_t plan, int enable);

@@ -95,3 +95,41 @@ def test_maps_empty_and_polar_failure():
     ph = np.array([0.0, 0.2])
     A2 = d2.call_maps(th, ph, np.ones((2, 2)))
     assert not np.any(A2)
+
+
+def test_maps_per_pass_does_not_change_results():
+    """The mixed path's integer bin sums are exact (every bin here fits one piece), so the
+    grouping of maps into contraction passes leaves every map's alm bit for bit the same."""
+    Nl, Nx, N = 96, 192, 60000
+    rng, th, ph = _points(N, 31)
+    W = rng.normal(1.0, 0.3, (5, N)).astype(np.float32)
+    d = DirectSHT(Nl, Nx, precision="mixed")
+    out = []
+    for per_pass in (1, 2, 3):
+        assert d.tune(maps_per_pass=per_pass)["maps_per_pass"] == per_pass
+        out.append(d.call_maps(th, ph, W))
+    assert np.array_equal(out[0], out[1]) and np.array_equal(out[0], out[2])
+    ref = O.direct_sht(O.build_tables(Nl, Nx), th, ph, W[4].astype(np.float64))
+    assert _rel(out[0][4], ref) <= 1e-7
+
+
+@pytest.mark.parametrize("piece", [256, 512, 2048])
+def test_piece_size_tuning(piece):
+    Nl, Nx, N = 64, 64, 40000  # few bins: many points per bin, split into pieces
+    rng, th, ph = _points(N, 41)
+    w = rng.uniform(0.5, 1.5, N)
+    ref = O.direct_sht(O.build_tables(Nl, Nx), th, ph, w)
+    d = DirectSHT(Nl, Nx)
+    d.tune(piece_max=piece)
+    assert _rel(d(th, ph, w), ref) <= 1e-12
+    d.set_precision("mixed_f64_tables")
+    assert _rel(d(th, ph, w), ref) <= 1e-7
+
+
+def test_tune_rejects_bad_values():
+    from directsht_b200 import _lib as L
+    d = DirectSHT(16, 32)
+    for param, value in ((L.DSHT_TUNE_PIECE_MAX, 100), (L.DSHT_TUNE_PIECE_MAX, 4096),
+                         (L.DSHT_TUNE_MAPS_PER_PASS, 9), (77, 1)):
+        assert d._lib.dsht_plan_tune(d._plan, param, value) == L.DSHT_ERR_INVALID
+    assert d.tune() == {"piece_max": 0, "maps_per_pass": 0}
