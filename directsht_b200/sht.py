@@ -60,6 +60,7 @@ class DirectSHT:
             flags = L.DSHT_PLAN_F32_TABLES if f32_tables else L.DSHT_PLAN_DEFAULT
             L.check(self._lib.dsht_plan_create(self.Nell, self.Nx, self.xmax, flags, ct.byref(self._plan)))
         self.precision = None
+        self._f32_only = bool(f32_tables)
         self.set_precision("mixed" if f32_tables else precision)
         self._Yv = None
         self._Yd = None

@@ -125,9 +125,10 @@ def test_enqueue_batch_in_cuda_graph():
             a.zero_()
         g.replay()
         torch.cuda.synchronize()
-        for i in range(n):
-            assert np.array_equal(alms[i].cpu().numpy(), eager[i])
-    assert not status.any()
+        for i in range(n):  # N < 1024 runs the FP64 bin sums, whose order inside a bin varies
+            got = alms[i].cpu().numpy()
+            assert np.array_equal(got, eager[i]) if len(sets[i][0]) >= 1024 else _rel(got, eager[i]) <= 1e-13
+    assert all(d._lib.dsht_status(int(f), L.DSHT_MODE_CALL) == L.DSHT_OK for f in status.cpu().numpy())
 
 
 def test_f32_table_plan():
