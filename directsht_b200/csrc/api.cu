@@ -64,8 +64,10 @@ size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* ba
   if (maps) {
     w.sidx = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * n));
     w.st = reinterpret_cast<double*>(take(sizeof(double) * n));
+    w.skey = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * n));
   }
   w.count = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * (g.nkeys + 1)));
+  w.keymax = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * g.nkeys));
   w.offset = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * (g.nkeys + 1)));
   w.cursor = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * (g.nkeys + 1)));
   w.piece_first = reinterpret_cast<int*>(take(sizeof(int) * (g.nkeys + 1)));
@@ -264,6 +266,7 @@ int run_items(dsht_plan_s* p, const Item* items, int n, int mode, const Workspac
         if (!shared) {
           wp.sidx = nullptr;
           wp.st = nullptr;
+          wp.skey = nullptr;
         }
         launch_points(g, item.theta, item.phi, item.w, item.w_f32, item.N, mode, wp, s);
         sorted_item = i;

@@ -126,6 +126,7 @@ template <int CH>
 __global__ void __launch_bounds__(kThreads, 1)
 bin_sums_tc_kernel(int Nl, int Cf, int64_t Npay, const double* __restrict__ pay, const int* __restrict__ npieces_p,
                    int64_t pmax, const int64_t* __restrict__ piece_start, const int* __restrict__ piece_len,
+                   const int* __restrict__ piece_key, const uint32_t* __restrict__ keymax,
                    float* __restrict__ partial, unsigned* __restrict__ err_flags) {
   using Lay = Layout<CH>;
   constexpr int N = Lay::N;
@@ -149,7 +150,6 @@ bin_sums_tc_kernel(int Nl, int Cf, int64_t Npay, const double* __restrict__ pay,
   uint64_t* done = full + 2 * S;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(misc + 128);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(misc + 132);
-  unsigned* smax = reinterpret_cast<unsigned*>(misc + 136);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int cbase = blockIdx.y * CH;
@@ -178,19 +178,9 @@ bin_sums_tc_kernel(int Nl, int Cf, int64_t Npay, const double* __restrict__ pay,
     const int nblk = (len + kBK - 1) / kBK;
 
     if (warp < 8) {
-      // ---- scale: largest |g_k| of the piece ----------------------------------------
-      if (tid == 0) *smax = 0u;
-      bar_producers();
-      float mx = 0.f;
-      for (int i = tid; i < len; i += kProducers)
-#pragma unroll
-        for (int k = 0; k < 4; ++k) mx = fmaxf(mx, (float)fabs(pay[6 * (start + i) + 2 + k]));
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-      if (lane == 0) atomicMax(smax, __float_as_uint(mx));
-      bar_producers();
+      // ---- scale: largest |g_k| of the piece's key (gathered by the sort) -------------
       // Round the scale up so that |g_k| / scale <= 1 holds after rounding too.
-      double scale = (double)__uint_as_float(*smax) * (1.0 + 1.0 / 1048576.0);
+      double scale = (double)__uint_as_float(keymax[piece_key[piece]]) * (1.0 + 1.0 / 1048576.0);
       if (!(scale > 0.0) || !isfinite(scale)) scale = 1.0;
       const double inv_scale = 1.0 / scale;
 
@@ -510,8 +500,9 @@ void launch_ch(const Geometry& g, const Workspace& ws, int Cf, cudaStream_t s) {
   if (grid < 1) grid = 1;
   dim3 gd((unsigned)grid, groups);
   bin_sums_tc_kernel<CH><<<gd, kThreads, Lay::kBytes, s>>>(g.Nl, Cf, ws.npts, ws.pay, ws.npieces, ws.pmax,
-                                                           ws.piece_start, ws.piece_len,
-                                                           reinterpret_cast<float*>(ws.partial), ws.flags);
+                                                           ws.piece_start, ws.piece_len, ws.piece_key,
+                                                           ws.keymax, reinterpret_cast<float*>(ws.partial),
+                                                           ws.flags);
   count_launches(1);
 }
 

@@ -70,6 +70,8 @@ struct Workspace {
   double* pay;          // [N][6]
   uint32_t* sidx;       // [N] input index of each sorted slot (multi-map transforms)
   double* st;           // [N] t of each sorted slot
+  uint32_t* skey;       // [N] key of each sorted slot
+  uint32_t* keymax;     // [nkeys] largest |w h_k| of the key's points (float bits)
   uint32_t* count;      // [nkeys + 1]
   uint32_t* offset;     // [nkeys + 1]
   uint32_t* cursor;     // [nkeys]

@@ -210,15 +210,27 @@ __device__ __forceinline__ void hermite(double t, double wi, double* out4) {
   out4[3] = __dmul_rn(wi, __dmul_rn(t2, __dadd_rn(t, -1.0)));
 }
 
-template <typename WT>
+// Largest |w h_k| of a point as float bits (non-negative floats order like their bits).
+__device__ __forceinline__ uint32_t gmax_bits(const double* h) {
+  return __float_as_uint((float)fmax(fmax(fabs(h[0]), fabs(h[1])), fmax(fabs(h[2]), fabs(h[3]))));
+}
+
+// kSmemMax: the per-key maxima of the block are gathered in shared memory first (when
+// 2 * nkeys words fit), else every point updates keymax in global memory.
+template <typename WT, bool kSmemMax>
 __global__ void __launch_bounds__(kPointThreads)
 scatter_kernel(Geometry g, const WT* __restrict__ w, int64_t N, const uint32_t* __restrict__ keys,
                const double* __restrict__ rec, uint32_t* __restrict__ cursor, double* __restrict__ pay,
-               uint32_t* __restrict__ sidx, double* __restrict__ st) {
-  extern __shared__ uint32_t loc[];  // [nkeys] local counts, then local bases
+               uint32_t* __restrict__ keymax, uint32_t* __restrict__ sidx, double* __restrict__ st,
+               uint32_t* __restrict__ skey) {
+  extern __shared__ uint32_t loc[];  // [nkeys] local counts, then local bases; [nkeys] maxima
+  uint32_t* kmx = loc + g.nkeys;
   const int64_t lo = (int64_t)blockIdx.x * kScatterTile;
   const int64_t hi = min(lo + (int64_t)kScatterTile, N);
-  for (int k = threadIdx.x; k < g.nkeys; k += blockDim.x) loc[k] = 0;
+  for (int k = threadIdx.x; k < g.nkeys; k += blockDim.x) {
+    loc[k] = 0;
+    if (kSmemMax) kmx[k] = 0;
+  }
   __syncthreads();
   for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
     const uint32_t k = keys[i];
@@ -241,10 +253,18 @@ scatter_kernel(Geometry g, const WT* __restrict__ w, int64_t N, const uint32_t* 
     out[0] = make_double2(rec[3 * i], rec[3 * i + 1]);
     out[1] = make_double2(h[0], h[1]);
     out[2] = make_double2(h[2], h[3]);
+    if (kSmemMax) atomicMax(&kmx[k], gmax_bits(h));
+    else atomicMax(&keymax[k], gmax_bits(h));
     if (sidx) {
       sidx[pos] = (uint32_t)i;
       st[pos] = t;
+      skey[pos] = k;
     }
+  }
+  if (kSmemMax) {
+    __syncthreads();
+    for (int k = threadIdx.x; k < g.nkeys; k += blockDim.x)
+      if (kmx[k]) atomicMax(&keymax[k], kmx[k]);
   }
 }
 
@@ -253,7 +273,8 @@ scatter_kernel(Geometry g, const WT* __restrict__ w, int64_t N, const uint32_t* 
 template <typename WT>
 __global__ void __launch_bounds__(kPointThreads)
 gather_kernel(int64_t N, const uint32_t* __restrict__ total, const uint32_t* __restrict__ sidx,
-              const double* __restrict__ st, const WT* __restrict__ w, double* __restrict__ pay) {
+              const double* __restrict__ st, const uint32_t* __restrict__ skey, const WT* __restrict__ w,
+              double* __restrict__ pay, uint32_t* __restrict__ keymax) {
   const int64_t n = (int64_t)*total;
   for (int64_t pos = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; pos < n && pos < N;
        pos += (int64_t)gridDim.x * blockDim.x) {
@@ -262,6 +283,7 @@ gather_kernel(int64_t N, const uint32_t* __restrict__ total, const uint32_t* __r
     double2* out = reinterpret_cast<double2*>(pay + (size_t)6 * pos);
     out[1] = make_double2(h[0], h[1]);
     out[2] = make_double2(h[2], h[3]);
+    atomicMax(&keymax[skey[pos]], gmax_bits(h));
   }
 }
 
@@ -278,11 +300,12 @@ __global__ void publish_flags_kernel(const StatusOut st, int n, unsigned* all) {
 void launch_points(const Geometry& g, const double* theta, const double* phi, const void* w, int w_f32,
                    int64_t N, int mode, const Workspace& ws, cudaStream_t s) {
   cudaMemsetAsync(ws.count, 0, sizeof(uint32_t) * (g.nkeys + 1), s);
+  cudaMemsetAsync(ws.keymax, 0, sizeof(uint32_t) * g.nkeys, s);
   cudaMemsetAsync(ws.flags, 0, sizeof(unsigned), s);
   const size_t hsmem = sizeof(uint32_t) * g.nkeys;
+  const bool smax = 2 * hsmem <= 200 * 1024;
+  const size_t ssmem = smax ? 2 * hsmem : hsmem;
   cudaFuncSetAttribute(count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem);
-  cudaFuncSetAttribute(scatter_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem);
-  cudaFuncSetAttribute(scatter_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem);
   if (N > 0) {
     int64_t blocks = (N + kPointThreads * 8 - 1) / (kPointThreads * 8);
     if (blocks > 148 * 8) blocks = 148 * 8;
@@ -296,12 +319,15 @@ void launch_points(const Geometry& g, const double* theta, const double* phi, co
   count_launches(1);
   if (N > 0) {
     const int64_t blocks = (N + kScatterTile - 1) / kScatterTile;
-    if (w_f32)
-      scatter_kernel<float><<<(unsigned)blocks, kPointThreads, hsmem, s>>>(
-          g, reinterpret_cast<const float*>(w), N, ws.key, ws.rec, ws.cursor, ws.pay, ws.sidx, ws.st);
-    else
-      scatter_kernel<double><<<(unsigned)blocks, kPointThreads, hsmem, s>>>(
-          g, reinterpret_cast<const double*>(w), N, ws.key, ws.rec, ws.cursor, ws.pay, ws.sidx, ws.st);
+    auto go = [&](auto kern, const auto* wp) {
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssmem);
+      kern<<<(unsigned)blocks, kPointThreads, ssmem, s>>>(g, wp, N, ws.key, ws.rec, ws.cursor, ws.pay, ws.keymax,
+                                                          ws.sidx, ws.st, ws.skey);
+    };
+    if (w_f32 && smax) go(scatter_kernel<float, true>, reinterpret_cast<const float*>(w));
+    else if (w_f32) go(scatter_kernel<float, false>, reinterpret_cast<const float*>(w));
+    else if (smax) go(scatter_kernel<double, true>, reinterpret_cast<const double*>(w));
+    else go(scatter_kernel<double, false>, reinterpret_cast<const double*>(w));
     count_launches(1);
   }
 }
@@ -311,12 +337,13 @@ void launch_gather(const Geometry& g, const void* w, int w_f32, int64_t N, const
   int64_t blocks = (N + kPointThreads - 1) / kPointThreads;
   if (blocks > 148 * 16) blocks = 148 * 16;
   const uint32_t* total = ws.offset + g.nkeys;
+  cudaMemsetAsync(ws.keymax, 0, sizeof(uint32_t) * g.nkeys, s);
   if (w_f32)
-    gather_kernel<float><<<(unsigned)blocks, kPointThreads, 0, s>>>(N, total, ws.sidx, ws.st,
-                                                                    reinterpret_cast<const float*>(w), ws.pay);
+    gather_kernel<float><<<(unsigned)blocks, kPointThreads, 0, s>>>(
+        N, total, ws.sidx, ws.st, ws.skey, reinterpret_cast<const float*>(w), ws.pay, ws.keymax);
   else
-    gather_kernel<double><<<(unsigned)blocks, kPointThreads, 0, s>>>(N, total, ws.sidx, ws.st,
-                                                                     reinterpret_cast<const double*>(w), ws.pay);
+    gather_kernel<double><<<(unsigned)blocks, kPointThreads, 0, s>>>(
+        N, total, ws.sidx, ws.st, ws.skey, reinterpret_cast<const double*>(w), ws.pay, ws.keymax);
   count_launches(1);
 }
 

@@ -225,8 +225,8 @@ class Server:
         t0 = time.perf_counter()
         if drain:
             while True:
-                with self._lock:
-                    if not self.adm.queue and not self.running:
+                with self._lock:  # adm.running counts admitted requests until their release
+                    if not self.adm.queue and self.adm.running == 0:
                         break
                 if timeout is not None and time.perf_counter() - t0 > timeout:
                     break
@@ -241,7 +241,7 @@ class Server:
             with self._cv:
                 if self._stop:
                     return
-                if not self.adm.queue and not self.running:
+                if not self.adm.queue and self.adm.running == 0:
                     self._cv.wait(timeout=0.05)
                     continue
                 start, rejected = self.adm.pop_admissible()
