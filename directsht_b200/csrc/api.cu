@@ -59,21 +59,20 @@ size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* ba
   Workspace w{};
   w.key = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * n));
   w.rec = reinterpret_cast<double*>(take(sizeof(double) * 3 * n));
-  w.pay = reinterpret_cast<double*>(take(sizeof(double) * 6 * n));
+  w.pay = reinterpret_cast<double*>(take(sizeof(double) * kRec * n));
   const bool maps = multi;
   if (maps) {
     w.sidx = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * n));
-    w.st = reinterpret_cast<double*>(take(sizeof(double) * n));
     w.skey = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * n));
   }
   w.count = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * (g.nkeys + 1)));
-  w.keymax = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * g.nkeys));
   w.offset = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * (g.nkeys + 1)));
   w.cursor = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * (g.nkeys + 1)));
   w.piece_first = reinterpret_cast<int*>(take(sizeof(int) * (g.nkeys + 1)));
   w.piece_key = reinterpret_cast<int*>(take(sizeof(int) * pmax));
   w.piece_start = reinterpret_cast<int64_t*>(take(sizeof(int64_t) * pmax));
   w.piece_len = reinterpret_cast<int*>(take(sizeof(int) * pmax));
+  w.piecemax = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * pmax));
   w.npieces = reinterpret_cast<int*>(take(sizeof(int)));
   w.flags = reinterpret_cast<unsigned*>(take(sizeof(unsigned)));
   if (maps) {
@@ -265,7 +264,6 @@ int run_items(dsht_plan_s* p, const Item* items, int n, int mode, const Workspac
         const bool shared = li + 1 < list.size() && items[list[li + 1]].same_points;
         if (!shared) {
           wp.sidx = nullptr;
-          wp.st = nullptr;
           wp.skey = nullptr;
         }
         launch_points(g, item.theta, item.phi, item.w, item.w_f32, item.N, mode, wp, s);

@@ -59,7 +59,7 @@ bin_sums_fp64_kernel(int Nl, int64_t N, const double* __restrict__ pay, const in
         const int p = tid >> 1, half = tid & 1;
         if (p < np) {
           const int64_t i = start + base + p;
-          const double* rp = pay + 6 * i;
+          const double* rp = pay + kRec * i;
           const cplx e1 = {rp[0], rp[1]};
           cplx e8 = cmul(e1, e1);
           e8 = cmul(e8, e8);
@@ -85,10 +85,12 @@ bin_sums_fp64_kernel(int Nl, int64_t N, const double* __restrict__ pay, const in
               sT2[p][b] = z;
             }
             sE1[p] = e1;
-            sG[p][0] = rp[2];
-            sG[p][1] = rp[3];
-            sG[p][2] = rp[4];
-            sG[p][3] = rp[5];
+            double h[4];
+            hermite(rp[3], rp[2], h);
+            sG[p][0] = h[0];
+            sG[p][1] = h[1];
+            sG[p][2] = h[2];
+            sG[p][3] = h[3];
           }
         }
       }

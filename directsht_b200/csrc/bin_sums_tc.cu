@@ -6,9 +6,10 @@
 // (sht/shared_interp_funcs.py:88-105) are one real GEMM once m is factored as
 // m = Cf a + c (a < 16):  e^{i m phi} = e^{i Cf a phi} e^{i c phi}, so
 //   D[row, col] = sum_p L[row, p] R[col, p]
-// with rows = (re|im, k, a) of L = g_k e^{i Cf a phi} / scale   (M = 128)
-// and  cols = (re|im, c)    of R = e^{i c phi}                   (N = 2 CH),
-// and Vr = D[re,Rr] - D[im,Ri], Vi = D[re,Ri] + D[im,Rr].  The points of the piece are
+// with rows = 2 (16 k + a) + (re|im) of L = g_k e^{i Cf a phi} / scale   (M = 128)
+// and  cols = (re|im, c)    of R = e^{i c phi}                           (N = 2 CH),
+// and Vr = D[re,Rr] - D[im,Ri], Vi = D[re,Ri] + D[im,Rr] (neighbouring TMEM lanes, one
+// warp shuffle).  The points of the piece are
 // the K dimension, 64 per pipeline stage.  When Cf > CH the c range is covered by
 // Cf/CH column groups (grid.y).
 //
@@ -41,6 +42,11 @@ constexpr int kStages = 3;
 constexpr float kQf = 4193280.0f;       // 2^22 - 2^10: |X| < 2^22, so X >> 16 fits int8
 constexpr double kQ = 4193280.0;
 constexpr float kMagic = 12582912.0f;   // 1.5 * 2^23 (bit pattern 0x4B400000)
+// Per-k scale factors: |h_1|, |h_3| <= 4/27 while max(h_0, h_2) >= 1/2, so
+// |w h_1|, |w h_3| <= (8/27) max_k |w h_k| over a piece; their rows use 0.3 of the
+// piece's scale (1.75 more bits).
+__device__ constexpr double kKScale[4] = {1.0, 0.3, 1.0, 0.3};
+__device__ constexpr double kInvKScale[4] = {1.0, 1.0 / 0.3, 1.0, 1.0 / 0.3};
 
 struct cplx {
   double re, im;
@@ -48,16 +54,6 @@ struct cplx {
 __device__ __forceinline__ cplx cmul(cplx a, cplx b) {
   return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
 }
-__device__ __forceinline__ cplx cpow(cplx z, int n) {  // z^n by squaring, n >= 0
-  cplx r = {1.0, 0.0};
-  while (n > 0) {
-    if (n & 1) r = cmul(r, z);
-    z = cmul(z, z);
-    n >>= 1;
-  }
-  return r;
-}
-
 // rint(x q) for |x| <= 1: one FMA puts x q into the binade of 1.5*2^23, where the
 // float's bit pattern minus that of 1.5*2^23 is the rounded integer.
 __device__ __forceinline__ int quant(float x) { return __float_as_int(fmaf(x, kQf, kMagic)) - 0x4B400000; }
@@ -71,7 +67,6 @@ __device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
 }
 
 __device__ __forceinline__ void bar_producers() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
-__device__ __forceinline__ void bar_epilogue() { asm volatile("bar.sync 2, 128;" ::: "memory"); }
 
 // Shared-memory descriptor: K-major operand in the 64-byte swizzle layout (rows of 64 B,
 // 8-row atoms of 512 B packed: stride byte offset 512).
@@ -107,10 +102,8 @@ struct Layout {
   static constexpr int kTileA = kM * 64;                      // bytes of one A slice tile
   static constexpr int kTileB = N * 64;
   static constexpr int kStage = 3 * kTileA + 3 * kTileB;      // A0..A2, B0..B2
-  static constexpr int kXchStride = 65;                       // floats per exchange row
   static constexpr int kAnchorBytes = kBK * (8 + (CH / 2 + 1) * 8 + 17 * 8 + 4 * 4);
-  static constexpr int kXchBytes = kM * kXchStride * 4;
-  static constexpr int kUnion = 2 * kAnchorBytes > kXchBytes ? 2 * kAnchorBytes : kXchBytes;
+  static constexpr int kUnion = 2 * kAnchorBytes;
   static constexpr int kUnionOff = kStages * kStage;
   static constexpr int kMiscOff = kUnionOff + ((kUnion + 1023) / 1024) * 1024;
   static constexpr int kBytes = kMiscOff + 256 + 1024;        // + alignment slack
@@ -126,7 +119,7 @@ template <int CH>
 __global__ void __launch_bounds__(kThreads, 1)
 bin_sums_tc_kernel(int Nl, int Cf, int64_t Npay, const double* __restrict__ pay, const int* __restrict__ npieces_p,
                    int64_t pmax, const int64_t* __restrict__ piece_start, const int* __restrict__ piece_len,
-                   const int* __restrict__ piece_key, const uint32_t* __restrict__ keymax,
+                   const uint32_t* __restrict__ piecemax,
                    float* __restrict__ partial, unsigned* __restrict__ err_flags) {
   using Lay = Layout<CH>;
   constexpr int N = Lay::N;
@@ -143,7 +136,6 @@ bin_sums_tc_kernel(int Nl, int Cf, int64_t Npay, const double* __restrict__ pay,
   auto ec_of = [&](int buf) { return e1_of(buf) + kBK; };
   auto ea_of = [&](int buf) { return ec_of(buf) + kBK * kEcStride; };
   auto gk_of = [&](int buf) { return reinterpret_cast<float*>(ea_of(buf) + kBK * kEaStride); };
-  float* xch = reinterpret_cast<float*>(uni);                    // [128][65]   epilogue exchange
   uint8_t* misc = smem + Lay::kMiscOff;
   uint64_t* full = reinterpret_cast<uint64_t*>(misc);            // [S]
   uint64_t* empty = full + S;                                    // [S]
@@ -178,9 +170,9 @@ bin_sums_tc_kernel(int Nl, int Cf, int64_t Npay, const double* __restrict__ pay,
     const int nblk = (len + kBK - 1) / kBK;
 
     if (warp < 8) {
-      // ---- scale: largest |g_k| of the piece's key (gathered by the sort) -------------
+      // ---- scale: largest |g_k| of the piece (gathered by the sort) -------------------
       // Round the scale up so that |g_k| / scale <= 1 holds after rounding too.
-      double scale = (double)__uint_as_float(keymax[piece_key[piece]]) * (1.0 + 1.0 / 1048576.0);
+      double scale = (double)__uint_as_float(piecemax[piece]) * (1.0 + 1.0 / 1048576.0);
       if (!(scale > 0.0) || !isfinite(scale)) scale = 1.0;
       const double inv_scale = 1.0 / scale;
 
@@ -188,7 +180,25 @@ bin_sums_tc_kernel(int Nl, int Cf, int64_t Npay, const double* __restrict__ pay,
       // Threads 0-127: ec of point t%64, entries [h CH/4, (h+1) CH/4), h = t/64.
       // Threads 128-255: ea of point t%64, entries [8h, 8h+8), and e1, g for h = 1.
       // Lanes of a warp hold consecutive points (warp-uniform branches); every thread runs
-      // two interleaved recurrences so that FP64 latency overlaps.
+      // two interleaved recurrences so that FP64 latency overlaps.  All starting powers are
+      // powers of two of e^{i phi} (CH, Cf are), so they come from straight-line squaring.
+      // The record of block b+1 is loaded into registers while block b is processed.
+      const int p_me = tid & 63, hq = (tid >> 6) & 1;
+      const bool is_ec = tid < 128;
+      const bool need_wt = !is_ec && hq == 1;
+      double r_c = 0.0, r_s = 0.0, r_w = 0.0, r_t = 0.0;  // record of the next block's point
+      auto load_rec = [&](int b) {
+        if (b * kBK + p_me < len) {
+          const double* r = pay + (size_t)kRec * (start + (int64_t)b * kBK + p_me);
+          r_c = r[0];
+          r_s = r[1];
+          if (need_wt) {
+            r_w = r[2];
+            r_t = r[3];
+          }
+        }
+      };
+      load_rec(0);
       auto phase1 = [&](int b) {
         if (*abort_flag) return;
         const int buf = b & 1;
@@ -197,17 +207,25 @@ bin_sums_tc_kernel(int Nl, int Cf, int64_t Npay, const double* __restrict__ pay,
         float2* ea = ea_of(buf);
         float* gk = gk_of(buf);
         const int np = min(kBK, len - b * kBK);
-        const int p = tid & 63, hq = (tid >> 6) & 1;
-        const bool is_ec = tid < 128;
+        const int p = p_me;
+        const cplx z1 = {r_c, r_s};
+        const double wv = r_w, tv = r_t;
+        if (b + 1 < nblk) load_rec(b + 1);
         if (p < np) {
-          const int64_t i = start + (int64_t)b * kBK + p;
-          const cplx z1 = {pay[6 * i], pay[6 * i + 1]};
+          // z^(2^j) for 2^j = CH/4, CH/2, CH
+          cplx zq = z1;
+#pragma unroll
+          for (int q = 1; q < CH / 4; q <<= 1) zq = cmul(zq, zq);
+          const cplx zh = cmul(zq, zq);      // z^(CH/2)
+          const cplx zf = cmul(zh, zh);      // z^CH
           if (is_ec) {
             constexpr int H = CH / 8;  // entries per chain
             const int u0 = hq * (CH / 4);
             const cplx st = cmul(z1, z1);
-            cplx za = cpow(z1, cbase + 2 * u0);
-            cplx zb = cmul(za, cpow(st, H));
+            // za = z^(cbase + 2 u0): cbase in {0, CH}, 2 u0 in {0, CH/2}
+            cplx za = hq ? zh : cplx{1.0, 0.0};
+            if (cbase) za = cmul(za, zf);
+            cplx zb = cmul(za, zq);            // z^(cbase + 2 u0 + CH/4) = za st^H
             for (int u = 0; u < H; ++u) {
               ec[p * kEcStride + u0 + u] = make_float2((float)za.re, (float)za.im);
               ec[p * kEcStride + u0 + H + u] = make_float2((float)zb.re, (float)zb.im);
@@ -216,9 +234,10 @@ bin_sums_tc_kernel(int Nl, int Cf, int64_t Npay, const double* __restrict__ pay,
             }
           } else {
             const int a0 = 8 * hq;
-            const cplx st = cpow(z1, Cf);
-            cplx za = cpow(st, a0);
-            cplx zb = cmul(za, cpow(st, 4));
+            const cplx st = (Cf == CH) ? zf : cmul(zf, zf);  // z^Cf, Cf in {CH, 2 CH}
+            const cplx s2 = cmul(st, st), s4 = cmul(s2, s2);
+            cplx za = hq ? cmul(s4, s4) : cplx{1.0, 0.0};     // st^a0
+            cplx zb = cmul(za, s4);
 #pragma unroll
             for (int a = 0; a < 4; ++a) {
               ea[p * kEaStride + a0 + a] = make_float2((float)za.re, (float)za.im);
@@ -228,8 +247,10 @@ bin_sums_tc_kernel(int Nl, int Cf, int64_t Npay, const double* __restrict__ pay,
             }
             if (hq == 1) {
               e1[p] = make_float2((float)z1.re, (float)z1.im);
+              double h[4];
+              hermite(tv, wv, h);
 #pragma unroll
-              for (int k = 0; k < 4; ++k) gk[p * 4 + k] = (float)(pay[6 * i + 2 + k] * inv_scale);
+              for (int k = 0; k < 4; ++k) gk[p * 4 + k] = (float)(h[k] * inv_scale * kInvKScale[k]);
             }
           }
         } else {  // padding points contribute zero
@@ -287,26 +308,39 @@ bin_sums_tc_kernel(int Nl, int Cf, int64_t Npay, const double* __restrict__ pay,
               base = st_base + 3 * Lay::kTileA;
               tile_bytes = Lay::kTileB;
             } else {
+              // A rows 2 (16 k + a) + (re|im): the two halves of a complex row sit in
+              // neighbouring TMEM lanes, so the epilogue combines them with one shuffle.
               const int v = u - nB;
               h = v >> 5;
               k = (v & 31) >> 3;
               ap = v & 7;
-              rows[0] = 16 * k + 2 * ap;
-              rows[1] = 64 + 16 * k + 2 * ap;
-              rows[2] = 16 * k + 2 * ap + 1;
-              rows[3] = 64 + 16 * k + 2 * ap + 1;
+              const int j0 = 16 * k + 2 * ap;
+              rows[0] = 2 * j0;          // re, a = 2ap
+              rows[1] = 2 * j0 + 1;      // im
+              rows[2] = 2 * j0 + 2;      // re, a = 2ap + 1
+              rows[3] = 2 * j0 + 3;      // im
               base = st_base;
               tile_bytes = Lay::kTileA;
             }
-            // Lanes with bit 2 set write the odd row of each pair first, so that one
-            // store instruction covers all eight 16-byte bank groups.
+            // The first row each lane writes is chosen so that the eight lanes of a quarter
+            // warp cover all eight 16-byte bank groups: B units swap the pair members on
+            // lane bit 2; A units swap the a pair on lane bit 1 and re/im on lane bit 2.
             const bool odd = ((lane >> 2) & 1) != 0;
-            if (odd) {
+            const bool swap_a = !isB && ((lane >> 1) & 1) != 0;
+            if (isB ? odd : swap_a) {
               const int r0 = rows[0], r1 = rows[1];
               rows[0] = rows[2];
               rows[1] = rows[3];
               rows[2] = r0;
               rows[3] = r1;
+            }
+            if (!isB && odd) {
+              int r = rows[0];
+              rows[0] = rows[1];
+              rows[1] = r;
+              r = rows[2];
+              rows[2] = rows[3];
+              rows[3] = r;
             }
 #pragma unroll
             for (int t = 0; t < 4; ++t) {
@@ -324,14 +358,14 @@ bin_sums_tc_kernel(int Nl, int Cf, int64_t Npay, const double* __restrict__ pay,
                   v3 = fmaf(z.x, s.y, z.y * s.x);
                 } else {
                   const float gg = gk[p * 4 + k];
-                  const float2 z0 = ea[p * kEaStride + 2 * ap];
-                  const float2 z1 = ea[p * kEaStride + 2 * ap + 1];
-                  v0 = gg * z0.x;
-                  v1 = gg * z0.y;
-                  v2 = gg * z1.x;
-                  v3 = gg * z1.y;
+                  const float2 z0 = ea[p * kEaStride + 2 * ap + (swap_a ? 1 : 0)];
+                  const float2 z1 = ea[p * kEaStride + 2 * ap + (swap_a ? 0 : 1)];
+                  v0 = gg * (odd ? z0.y : z0.x);
+                  v1 = gg * (odd ? z0.x : z0.y);
+                  v2 = gg * (odd ? z1.y : z1.x);
+                  v3 = gg * (odd ? z1.x : z1.y);
                 }
-                if (odd) {
+                if (isB && odd) {
                   const float t0 = v0, t1 = v1;
                   v0 = v2;
                   v1 = v3;
@@ -372,6 +406,10 @@ bin_sums_tc_kernel(int Nl, int Cf, int64_t Npay, const double* __restrict__ pay,
       }
 
       // ---- epilogue: warps 0-3 own TMEM lanes 0-127 -----------------------------------
+      // Lane r holds row r = 2 (16 k + a) + ri of D.  For every c:
+      //   Vr = D[re, Rr] - D[im, Ri],  Vi = D[re, Ri] + D[im, Rr],
+      // so each lane sends its D[., Ri] to its neighbour (lane r ^ 1) and keeps D[., Rr]:
+      // the re lane writes Vr, the im lane Vi, for m = Cf a + cbase + c.
       if (warp < 4) {
         bool ok = !*abort_flag;
         if (ok && !tc::mbar_wait(done, piece_iter & 1, abort_flag)) {
@@ -381,51 +419,37 @@ bin_sums_tc_kernel(int Nl, int Cf, int64_t Npay, const double* __restrict__ pay,
         }
         tc::tc_fence_after();
         const int r = tid;  // TMEM lane == GEMM row
-        const bool is_re = r < 64;
-        const int k = (r & 63) >> 4, a = r & 15;
-        const double f = scale / (kQ * kQ);
-        for (int cb = 0; cb < CH; cb += 32) {
-          const int cw = min(32, CH - cb);
-          float vr[32], vi[32];
-          if (ok) {
-            const uint32_t lane_off = (uint32_t)(warp * 32) << 16;
+        const int ri = r & 1, j = r >> 1;
+        const int k = j >> 4, a = j & 15;
+        const double f = scale * kKScale[k] / (kQ * kQ);
+        const uint32_t lane_off = (uint32_t)(warp * 32) << 16;
+        float* out = partial + ((size_t)piece * 8 + 2 * k + ri) * Nl;
+        const int m0 = Cf * a + cbase;
+        for (int cb = 0; cb < CH; cb += 8) {
+          double drr[8], dri[8];
 #pragma unroll
-            for (int half = 0; half < 2; ++half) {
-              const uint32_t col = (half ? CH : 0) + cb;
-              float w0[32], w1[32], w2[32], w3[32];
-              tc::tmem_ld32(tmem + lane_off + col, w0);
-              tc::tmem_ld32(tmem + lane_off + N + col, w1);
-              tc::tmem_ld32(tmem + lane_off + 2 * N + col, w2);
-              tc::tmem_ld32(tmem + lane_off + 3 * N + col, w3);
-              float* dst = half ? vi : vr;
-#pragma unroll
-              for (int i = 0; i < 32; ++i) {
-                const double d = 4294967296.0 * (double)__float_as_int(w0[i]) +
-                                 16777216.0 * (double)__float_as_int(w1[i]) +
-                                 65536.0 * (double)__float_as_int(w2[i]) + 256.0 * (double)__float_as_int(w3[i]);
-                dst[i] = (float)(d * f);
-              }
+          for (int half = 0; half < 2; ++half) {
+            const uint32_t col = (half ? CH : 0) + cb;
+            uint32_t w0[8], w1[8], w2[8], w3[8];
+            if (ok) {
+              tc::tmem_ld8(tmem + lane_off + col, w0);
+              tc::tmem_ld8(tmem + lane_off + N + col, w1);
+              tc::tmem_ld8(tmem + lane_off + 2 * N + col, w2);
+              tc::tmem_ld8(tmem + lane_off + 3 * N + col, w3);
             }
-          } else {
+            double* dst = half ? dri : drr;
 #pragma unroll
-            for (int i = 0; i < 32; ++i) vr[i] = vi[i] = 0.f;
+            for (int i = 0; i < 8; ++i)
+              dst[i] = ok ? (4294967296.0 * (double)(int)w0[i] + 16777216.0 * (double)(int)w1[i] +
+                             65536.0 * (double)(int)w2[i] + 256.0 * (double)(int)w3[i]) * f
+                          : 0.0;
           }
 #pragma unroll
-          for (int i = 0; i < 32; ++i) {
-            xch[r * Lay::kXchStride + i] = vr[i];
-            xch[r * Lay::kXchStride + 32 + i] = vi[i];
+          for (int i = 0; i < 8; ++i) {
+            const double x = __shfl_xor_sync(0xffffffffu, dri[i], 1);
+            const double v = ri ? x + drr[i] : drr[i] - x;
+            if (m0 + cb + i < Nl) out[m0 + cb + i] = (float)v;
           }
-          bar_epilogue();
-          // re rows write Vr = D[re,Rr] - D[im,Ri]; im rows write Vi = D[re,Ri] + D[im,Rr].
-          const int rre = r & 63, rim = 64 + (r & 63);
-          float* out = partial + ((size_t)piece * 8 + 2 * k + (is_re ? 0 : 1)) * Nl;
-          const int m0 = Cf * a + cbase + cb;
-          for (int i = 0; i < cw; ++i) {
-            const float v = is_re ? xch[rre * Lay::kXchStride + i] - xch[rim * Lay::kXchStride + 32 + i]
-                                  : xch[rre * Lay::kXchStride + 32 + i] + xch[rim * Lay::kXchStride + i];
-            if (m0 + i < Nl) out[m0 + i] = v;
-          }
-          bar_epilogue();
         }
         tc::tc_fence_before();
       }
@@ -500,8 +524,8 @@ void launch_ch(const Geometry& g, const Workspace& ws, int Cf, cudaStream_t s) {
   if (grid < 1) grid = 1;
   dim3 gd((unsigned)grid, groups);
   bin_sums_tc_kernel<CH><<<gd, kThreads, Lay::kBytes, s>>>(g.Nl, Cf, ws.npts, ws.pay, ws.npieces, ws.pmax,
-                                                           ws.piece_start, ws.piece_len, ws.piece_key,
-                                                           ws.keymax, reinterpret_cast<float*>(ws.partial),
+                                                           ws.piece_start, ws.piece_len, ws.piecemax,
+                                                           reinterpret_cast<float*>(ws.partial),
                                                            ws.flags);
   count_launches(1);
 }

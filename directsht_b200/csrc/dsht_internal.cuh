@@ -4,7 +4,7 @@
 //   tables   Yv, Yd      double [Nlm][Nx]          (sht/sht.py:50-56 layout, numpy path)
 //   points   key         uint32 [N]                set*(Nx-1) + bin, or DSHT_KEY_DROP
 //            record      double [N][3]             (cos phi, sin phi, t) in input order
-//            sorted      double [N][6]             (cos phi, sin phi, w h0..w h3) by key
+//            sorted      double [N][4]             (cos phi, sin phi, w, t) by key
 //   pieces   <= 1 bin each, <= piece_max points    (key, start, len)
 //   partial  double [piece][8][Nl]                 (k, re/im) bin sums for every m
 //   fold     double [Nl][4 q][Nx][4]               q = {equ even, equ odd, pol even, pol odd}
@@ -67,11 +67,10 @@ struct StatusOut {
 struct Workspace {
   uint32_t* key;        // [N]
   double* rec;          // [N][3]
-  double* pay;          // [N][6]
+  double* pay;          // [N][4] sorted records (cos phi, sin phi, w, t)
   uint32_t* sidx;       // [N] input index of each sorted slot (multi-map transforms)
-  double* st;           // [N] t of each sorted slot
   uint32_t* skey;       // [N] key of each sorted slot
-  uint32_t* keymax;     // [nkeys] largest |w h_k| of the key's points (float bits)
+  uint32_t* piecemax;   // [pmax] largest |w h_k| of the piece's points (float bits)
   uint32_t* count;      // [nkeys + 1]
   uint32_t* offset;     // [nkeys + 1]
   uint32_t* cursor;     // [nkeys]
@@ -144,6 +143,21 @@ void launch_rotate_back(const Geometry& g, const double* alm_rot, const double* 
                         double* alm_out, const unsigned* flags, cudaStream_t s);
 // alm io[k] += R(rot[k]) for k < nmaps <= kMaxRot (a map without polar points is left as it is).
 void launch_rotate_back_maps(const Geometry& g, const RotMaps& maps, int nmaps, cudaStream_t s);
+
+// Hermite weights w * {(2t+1)(1-t)^2, t(1-t)^2, t^2(3-2t), t^2(t-1)} of one point, in the
+// rounding order of sht/sht.py:239-240.
+__device__ __forceinline__ void hermite(double t, double wi, double* out4) {
+  const double omt = __dadd_rn(1.0, -t);
+  const double omt2 = __dmul_rn(omt, omt);
+  const double t2 = __dmul_rn(t, t);
+  out4[0] = __dmul_rn(wi, __dmul_rn(__dadd_rn(__dmul_rn(2.0, t), 1.0), omt2));
+  out4[1] = __dmul_rn(wi, __dmul_rn(t, omt2));
+  out4[2] = __dmul_rn(wi, __dmul_rn(t2, __dadd_rn(3.0, -__dmul_rn(2.0, t))));
+  out4[3] = __dmul_rn(wi, __dmul_rn(t2, __dadd_rn(t, -1.0)));
+}
+
+// The sorted record of a point: (cos phi, sin phi, w, t), 32 bytes.
+constexpr int kRec = 4;
 
 // Healpy index of (l, m).
 __host__ __device__ inline int64_t hp_index(int l, int m, int Nl) {

@@ -10,9 +10,9 @@
 // sin phi, t in input order) and histograms the keys in shared memory (one global add per
 // live key and block); a one-block exclusive scan cuts every key into pieces of at most
 // piece_max points; the scatter pass reserves a contiguous range per key and block with
-// one global add and writes each point's 48-byte record (cos phi, sin phi, w h0..w h3) to
-// its sorted slot.  HBM bound: about 16 B read + 28 B written (count), 36 B read + 48 B
-// written (scatter) per point.
+// one global add and writes each point's 32-byte record (cos phi, sin phi, w, t) -- one
+// DRAM sector -- to its sorted slot; the bin-sum kernels form w h_k(t) themselves.  HBM
+// bound: about 16 B read + 28 B written (count), 36 B read + 32 B written (scatter) per point.
 #include "dsht_internal.cuh"
 
 namespace dsht {
@@ -199,38 +199,23 @@ scan_kernel(int nkeys, int nbins, int piece_max, int64_t pmax, const uint32_t* _
   }
 }
 
-// Hermite weights of one point, in the rounding order of sht/sht.py:239-240.
-__device__ __forceinline__ void hermite(double t, double wi, double* out4) {
-  const double omt = __dadd_rn(1.0, -t);
-  const double omt2 = __dmul_rn(omt, omt);
-  const double t2 = __dmul_rn(t, t);
-  out4[0] = __dmul_rn(wi, __dmul_rn(__dadd_rn(__dmul_rn(2.0, t), 1.0), omt2));
-  out4[1] = __dmul_rn(wi, __dmul_rn(t, omt2));
-  out4[2] = __dmul_rn(wi, __dmul_rn(t2, __dadd_rn(3.0, -__dmul_rn(2.0, t))));
-  out4[3] = __dmul_rn(wi, __dmul_rn(t2, __dadd_rn(t, -1.0)));
-}
-
 // Largest |w h_k| of a point as float bits (non-negative floats order like their bits).
 __device__ __forceinline__ uint32_t gmax_bits(const double* h) {
   return __float_as_uint((float)fmax(fmax(fabs(h[0]), fabs(h[1])), fmax(fabs(h[2]), fabs(h[3]))));
 }
 
-// kSmemMax: the per-key maxima of the block are gathered in shared memory first (when
-// 2 * nkeys words fit), else every point updates keymax in global memory.
-template <typename WT, bool kSmemMax>
+// The piece of a sorted slot is piece_first[k] + (pos - offset[k]) / piece_max; every
+// point raises its piece's maximum |w h_k| (the fixed-point scale of the tensor-core sums).
+template <typename WT>
 __global__ void __launch_bounds__(kPointThreads)
 scatter_kernel(Geometry g, const WT* __restrict__ w, int64_t N, const uint32_t* __restrict__ keys,
                const double* __restrict__ rec, uint32_t* __restrict__ cursor, double* __restrict__ pay,
-               uint32_t* __restrict__ keymax, uint32_t* __restrict__ sidx, double* __restrict__ st,
-               uint32_t* __restrict__ skey) {
-  extern __shared__ uint32_t loc[];  // [nkeys] local counts, then local bases; [nkeys] maxima
-  uint32_t* kmx = loc + g.nkeys;
+               const uint32_t* __restrict__ offset, const int* __restrict__ piece_first, int piece_max,
+               uint32_t* __restrict__ piecemax, uint32_t* __restrict__ sidx, uint32_t* __restrict__ skey) {
+  extern __shared__ uint32_t loc[];  // [nkeys] local counts, then local bases
   const int64_t lo = (int64_t)blockIdx.x * kScatterTile;
   const int64_t hi = min(lo + (int64_t)kScatterTile, N);
-  for (int k = threadIdx.x; k < g.nkeys; k += blockDim.x) {
-    loc[k] = 0;
-    if (kSmemMax) kmx[k] = 0;
-  }
+  for (int k = threadIdx.x; k < g.nkeys; k += blockDim.x) loc[k] = 0;
   __syncthreads();
   for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
     const uint32_t k = keys[i];
@@ -247,43 +232,38 @@ scatter_kernel(Geometry g, const WT* __restrict__ w, int64_t N, const uint32_t* 
     if (k == DSHT_KEY_DROP) continue;
     const uint32_t pos = atomicAdd(&loc[k], 1u);
     const double t = rec[3 * i + 2];
-    double h[4];
-    hermite(t, (double)w[i], h);
-    double2* out = reinterpret_cast<double2*>(pay + (size_t)6 * pos);
+    const double wi = (double)w[i];
+    double2* out = reinterpret_cast<double2*>(pay + (size_t)kRec * pos);  // one 32-byte sector
     out[0] = make_double2(rec[3 * i], rec[3 * i + 1]);
-    out[1] = make_double2(h[0], h[1]);
-    out[2] = make_double2(h[2], h[3]);
-    if (kSmemMax) atomicMax(&kmx[k], gmax_bits(h));
-    else atomicMax(&keymax[k], gmax_bits(h));
+    out[1] = make_double2(wi, t);
+    double h[4];
+    hermite(t, wi, h);
+    atomicMax(&piecemax[piece_first[k] + (pos - offset[k]) / (uint32_t)piece_max], gmax_bits(h));
     if (sidx) {
       sidx[pos] = (uint32_t)i;
-      st[pos] = t;
       skey[pos] = k;
     }
   }
-  if (kSmemMax) {
-    __syncthreads();
-    for (int k = threadIdx.x; k < g.nkeys; k += blockDim.x)
-      if (kmx[k]) atomicMax(&keymax[k], kmx[k]);
-  }
 }
 
-// Rebuild the weighted part of the sorted payload for another weight map (multi-map
-// transforms share the sort): g_k(pos) = w[sidx[pos]] h_k(t[pos]).
+// Another weight map on the same sorted points (multi-map transforms share the sort): the
+// record's w becomes w[sidx[pos]], and the piece maxima are rebuilt.
 template <typename WT>
 __global__ void __launch_bounds__(kPointThreads)
 gather_kernel(int64_t N, const uint32_t* __restrict__ total, const uint32_t* __restrict__ sidx,
-              const double* __restrict__ st, const uint32_t* __restrict__ skey, const WT* __restrict__ w,
-              double* __restrict__ pay, uint32_t* __restrict__ keymax) {
+              const uint32_t* __restrict__ skey, const WT* __restrict__ w, double* __restrict__ pay,
+              const uint32_t* __restrict__ offset, const int* __restrict__ piece_first, int piece_max,
+              uint32_t* __restrict__ piecemax) {
   const int64_t n = (int64_t)*total;
   for (int64_t pos = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; pos < n && pos < N;
        pos += (int64_t)gridDim.x * blockDim.x) {
+    double* r = pay + (size_t)kRec * pos;
+    const double wi = (double)w[sidx[pos]];
+    r[2] = wi;
     double h[4];
-    hermite(st[pos], (double)w[sidx[pos]], h);
-    double2* out = reinterpret_cast<double2*>(pay + (size_t)6 * pos);
-    out[1] = make_double2(h[0], h[1]);
-    out[2] = make_double2(h[2], h[3]);
-    atomicMax(&keymax[skey[pos]], gmax_bits(h));
+    hermite(r[3], wi, h);
+    const uint32_t k = skey[pos];
+    atomicMax(&piecemax[piece_first[k] + ((uint32_t)pos - offset[k]) / (uint32_t)piece_max], gmax_bits(h));
   }
 }
 
@@ -300,11 +280,9 @@ __global__ void publish_flags_kernel(const StatusOut st, int n, unsigned* all) {
 void launch_points(const Geometry& g, const double* theta, const double* phi, const void* w, int w_f32,
                    int64_t N, int mode, const Workspace& ws, cudaStream_t s) {
   cudaMemsetAsync(ws.count, 0, sizeof(uint32_t) * (g.nkeys + 1), s);
-  cudaMemsetAsync(ws.keymax, 0, sizeof(uint32_t) * g.nkeys, s);
+  cudaMemsetAsync(ws.piecemax, 0, sizeof(uint32_t) * ws.pmax, s);
   cudaMemsetAsync(ws.flags, 0, sizeof(unsigned), s);
   const size_t hsmem = sizeof(uint32_t) * g.nkeys;
-  const bool smax = 2 * hsmem <= 200 * 1024;
-  const size_t ssmem = smax ? 2 * hsmem : hsmem;
   cudaFuncSetAttribute(count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem);
   if (N > 0) {
     int64_t blocks = (N + kPointThreads * 8 - 1) / (kPointThreads * 8);
@@ -320,14 +298,13 @@ void launch_points(const Geometry& g, const double* theta, const double* phi, co
   if (N > 0) {
     const int64_t blocks = (N + kScatterTile - 1) / kScatterTile;
     auto go = [&](auto kern, const auto* wp) {
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssmem);
-      kern<<<(unsigned)blocks, kPointThreads, ssmem, s>>>(g, wp, N, ws.key, ws.rec, ws.cursor, ws.pay, ws.keymax,
-                                                          ws.sidx, ws.st, ws.skey);
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem);
+      kern<<<(unsigned)blocks, kPointThreads, hsmem, s>>>(g, wp, N, ws.key, ws.rec, ws.cursor, ws.pay, ws.offset,
+                                                          ws.piece_first, ws.piece_max, ws.piecemax, ws.sidx,
+                                                          ws.skey);
     };
-    if (w_f32 && smax) go(scatter_kernel<float, true>, reinterpret_cast<const float*>(w));
-    else if (w_f32) go(scatter_kernel<float, false>, reinterpret_cast<const float*>(w));
-    else if (smax) go(scatter_kernel<double, true>, reinterpret_cast<const double*>(w));
-    else go(scatter_kernel<double, false>, reinterpret_cast<const double*>(w));
+    if (w_f32) go(scatter_kernel<float>, reinterpret_cast<const float*>(w));
+    else go(scatter_kernel<double>, reinterpret_cast<const double*>(w));
     count_launches(1);
   }
 }
@@ -337,13 +314,15 @@ void launch_gather(const Geometry& g, const void* w, int w_f32, int64_t N, const
   int64_t blocks = (N + kPointThreads - 1) / kPointThreads;
   if (blocks > 148 * 16) blocks = 148 * 16;
   const uint32_t* total = ws.offset + g.nkeys;
-  cudaMemsetAsync(ws.keymax, 0, sizeof(uint32_t) * g.nkeys, s);
+  cudaMemsetAsync(ws.piecemax, 0, sizeof(uint32_t) * ws.pmax, s);
   if (w_f32)
     gather_kernel<float><<<(unsigned)blocks, kPointThreads, 0, s>>>(
-        N, total, ws.sidx, ws.st, ws.skey, reinterpret_cast<const float*>(w), ws.pay, ws.keymax);
+        N, total, ws.sidx, ws.skey, reinterpret_cast<const float*>(w), ws.pay, ws.offset, ws.piece_first,
+        ws.piece_max, ws.piecemax);
   else
     gather_kernel<double><<<(unsigned)blocks, kPointThreads, 0, s>>>(
-        N, total, ws.sidx, ws.st, ws.skey, reinterpret_cast<const double*>(w), ws.pay, ws.keymax);
+        N, total, ws.sidx, ws.skey, reinterpret_cast<const double*>(w), ws.pay, ws.offset, ws.piece_first,
+        ws.piece_max, ws.piecemax);
   count_launches(1);
 }
 
