@@ -18,7 +18,22 @@ namespace dsht {
 static thread_local std::string g_last_error;
 static std::atomic<int64_t> g_launches{0};
 
-void count_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+static thread_local cudaError_t g_launch_error = cudaSuccess;
+
+// Every launch helper calls this right after its launches: it counts them and keeps the
+// first launch error of the thread (launch_error() reports and clears it).
+void count_launches(int n) {
+  g_launches.fetch_add(n, std::memory_order_relaxed);
+  const cudaError_t e = cudaPeekAtLastError();
+  if (e != cudaSuccess && g_launch_error == cudaSuccess) g_launch_error = e;
+}
+
+int launch_error(const char* where) {
+  const cudaError_t e = g_launch_error;
+  g_launch_error = cudaSuccess;
+  cudaGetLastError();
+  return e == cudaSuccess ? 0 : set_cuda_error(e, where, __FILE__, __LINE__);
+}
 
 int set_error(int code, const char* fmt, ...) {
   char buf[512];
@@ -165,6 +180,7 @@ int run_after_sort(dsht_plan_s* p, int64_t N, int mode, double* alm, const Works
     DSHT_CUDA_OK(cudaMemcpyAsync(alm, ws.alm_equ, sizeof(double) * 2 * g.Nlm, cudaMemcpyDeviceToDevice, s));
   }
   mark(5);
+  if (int rc = launch_error("kernel launch")) return rc;
   DSHT_CUDA_OK(cudaGetLastError());
   return DSHT_OK;
 }
@@ -315,6 +331,7 @@ int run_items(dsht_plan_s* p, const Item* items, int n, int mode, const Workspac
     if (rc) return rc;
   }
   ev(5);
+  if (int rc = launch_error("kernel launch")) return rc;
   DSHT_CUDA_OK(cudaGetLastError());
   return DSHT_OK;
 }

@@ -24,10 +24,13 @@
 // to the piece's largest |L|, mean below 1e-9.  Pieces of up to 2048 points keep every
 // S32 sum below 2^31.
 //
-// Warp roles: warps 0-7 generate operands into a 3-stage shared-memory ring (64-byte
-// swizzled K-major int8 tiles) and run the epilogue (warps 0-3 own TMEM lanes 0-127);
-// warp 8 issues the MMAs from one thread.  Stages are handed over with mbarriers (full:
-// producers -> MMA, empty: tcgen05.commit -> producers).  Every wait is bounded.
+// Warp roles: warps 8-9 compute the FP64 anchors of a block into one of two anchor
+// buffers, one block ahead; warps 0-7 quantise and slice them into a 3-stage ring of
+// 64-byte-swizzled K-major int8 tiles; warp 10 issues the MMAs from one thread; warps 0-3
+// run each piece's epilogue (TMEM lanes 0-127) while warps 4-7 and the anchor warps start
+// the next piece.  Hand-overs are mbarriers (afull/aempty: anchors <-> slicers, full/empty:
+// slicers <-> MMA via tcgen05.commit, done: MMA -> epilogue, tfree: epilogue -> MMA).
+// Every wait is bounded.
 #include "dsht_internal.cuh"
 #include "tc_ptx.cuh"
 
@@ -35,8 +38,10 @@ namespace dsht {
 namespace {
 
 constexpr int kBK = 64;                 // points per stage: one 64-byte row of int8
-constexpr int kProducers = 256;         // warps 0-7
-constexpr int kThreads = kProducers + 32;
+constexpr int kSlicerWarps = 8;         // warps 0-7: int8 slice tiles (0-3: epilogue too)
+constexpr int kAnchorWarps = 2;         // warps 8-9: FP64 anchors, one block ahead
+constexpr int kSlicers = 32 * kSlicerWarps;
+constexpr int kThreads = 32 * (kSlicerWarps + kAnchorWarps + 1);  // + warp 10: MMA issuer
 constexpr int kM = 128;
 constexpr int kStages = 3;
 constexpr float kQf = 4193280.0f;       // 2^22 - 2^10: |X| < 2^22, so X >> 16 fits int8
@@ -47,6 +52,13 @@ constexpr float kMagic = 12582912.0f;   // 1.5 * 2^23 (bit pattern 0x4B400000)
 // piece's scale (1.75 more bits).
 __device__ constexpr double kKScale[4] = {1.0, 0.3, 1.0, 0.3};
 __device__ constexpr double kInvKScale[4] = {1.0, 1.0 / 0.3, 1.0, 1.0 / 0.3};
+
+// Fixed-point scale of a piece: its largest |g_k| (float bits from the sort), rounded up
+// so that |g_k| / scale <= 1 holds after rounding too.
+__device__ __forceinline__ double tc_scale(uint32_t bits) {
+  const double s = (double)__uint_as_float(bits) * (1.0 + 1.0 / 1048576.0);
+  return (s > 0.0 && isfinite(s)) ? s : 1.0;
+}
 
 struct cplx {
   double re, im;
@@ -66,7 +78,6 @@ __device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
   return __byte_perm(lo, hi, 0x5410);
 }
 
-__device__ __forceinline__ void bar_producers() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
 
 // Shared-memory descriptor: K-major operand in the 64-byte swizzle layout (rows of 64 B,
 // 8-row atoms of 512 B packed: stride byte offset 512).
@@ -117,10 +128,10 @@ struct Layout {
 
 template <int CH>
 __global__ void __launch_bounds__(kThreads, 1)
-bin_sums_tc_kernel(int Nl, int Cf, int64_t Npay, const double* __restrict__ pay, const int* __restrict__ npieces_p,
-                   int64_t pmax, const int64_t* __restrict__ piece_start, const int* __restrict__ piece_len,
-                   const uint32_t* __restrict__ piecemax,
-                   float* __restrict__ partial, unsigned* __restrict__ err_flags) {
+bin_sums_tc_kernel(int Nl, int Cf, const double* __restrict__ pay, const int* __restrict__ npieces_p, int64_t pmax,
+                   const int64_t* __restrict__ piece_start, const int* __restrict__ piece_len,
+                   const uint32_t* __restrict__ piecemax, float* __restrict__ partial,
+                   unsigned* __restrict__ err_flags) {
   using Lay = Layout<CH>;
   constexpr int N = Lay::N;
   constexpr int S = kStages;
@@ -130,27 +141,35 @@ bin_sums_tc_kernel(int Nl, int Cf, int64_t Npay, const double* __restrict__ pay,
   // Row strides are padded by one entry so that lanes holding consecutive points hit
   // different banks.
   constexpr int kEcStride = CH / 2 + 1, kEaStride = 17;
-  // Two anchor buffers (block b uses buffer b & 1), each laid out as
+  // Two anchor buffers (global block g uses buffer g & 1), each laid out as
   //   e1 [64] e^{i phi} | ec [64][CH/2+1] e^{i (cbase + 2u) phi} | ea [64][17] e^{i Cf a phi} | gk [64][4]
   auto e1_of = [&](int buf) { return reinterpret_cast<float2*>(uni + buf * Lay::kAnchorBytes); };
   auto ec_of = [&](int buf) { return e1_of(buf) + kBK; };
   auto ea_of = [&](int buf) { return ec_of(buf) + kBK * kEcStride; };
   auto gk_of = [&](int buf) { return reinterpret_cast<float*>(ea_of(buf) + kBK * kEaStride); };
   uint8_t* misc = smem + Lay::kMiscOff;
-  uint64_t* full = reinterpret_cast<uint64_t*>(misc);            // [S]
-  uint64_t* empty = full + S;                                    // [S]
-  uint64_t* done = full + 2 * S;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(misc + 128);
-  volatile int* abort_flag = reinterpret_cast<volatile int*>(misc + 132);
+  uint64_t* full = reinterpret_cast<uint64_t*>(misc);            // [S]  slicers -> MMA
+  uint64_t* empty = full + S;                                    // [S]  MMA commit -> slicers
+  uint64_t* done = full + 2 * S;                                 // [1]  MMA commit -> epilogue
+  uint64_t* afull = done + 1;                                    // [2]  anchor warps -> slicers
+  uint64_t* aempty = afull + 2;                                  // [2]  slicers -> anchor warps
+  uint64_t* tfree = aempty + 2;                                  // [1]  epilogue -> MMA
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(misc + 192);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(misc + 196);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int cbase = blockIdx.y * CH;
   if (tid == 0) {
     for (int s = 0; s < S; ++s) {
-      tc::mbar_init(&full[s], kProducers / 32);
+      tc::mbar_init(&full[s], kSlicerWarps);
       tc::mbar_init(&empty[s], 1);
     }
     tc::mbar_init(done, 1);
+    for (int b = 0; b < 2; ++b) {
+      tc::mbar_init(&afull[b], kAnchorWarps);
+      tc::mbar_init(&aempty[b], kSlicerWarps);
+    }
+    tc::mbar_init(tfree, 4);
     *abort_flag = 0;
     tc::mbar_fence_init();
   }
@@ -159,139 +178,123 @@ bin_sums_tc_kernel(int Nl, int Cf, int64_t Npay, const double* __restrict__ pay,
   __syncthreads();
   tc::tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-
   const int npieces = (int)min((int64_t)*npieces_p, pmax);
-  uint32_t blk_count = 0;
-  uint32_t piece_iter = 0;
+  auto fail = [&]() {
+    *abort_flag = 1;
+    atomicOr(err_flags, kFlagTimeout);
+  };
 
-  for (int piece = blockIdx.x; piece < npieces; piece += gridDim.x, ++piece_iter) {
-    const int64_t start = piece_start[piece];
-    const int len = piece_len[piece];
-    const int nblk = (len + kBK - 1) / kBK;
-
-    if (warp < 8) {
-      // ---- scale: largest |g_k| of the piece (gathered by the sort) -------------------
-      // Round the scale up so that |g_k| / scale <= 1 holds after rounding too.
-      double scale = (double)__uint_as_float(piecemax[piece]) * (1.0 + 1.0 / 1048576.0);
-      if (!(scale > 0.0) || !isfinite(scale)) scale = 1.0;
-      const double inv_scale = 1.0 / scale;
-
-      // ---- phase 1: anchors of block b (FP64 math, FP32 storage) into buffer b & 1 ----
-      // Threads 0-127: ec of point t%64, entries [h CH/4, (h+1) CH/4), h = t/64.
-      // Threads 128-255: ea of point t%64, entries [8h, 8h+8), and e1, g for h = 1.
-      // Lanes of a warp hold consecutive points (warp-uniform branches); every thread runs
-      // two interleaved recurrences so that FP64 latency overlaps.  All starting powers are
-      // powers of two of e^{i phi} (CH, Cf are), so they come from straight-line squaring.
-      // The record of block b+1 is loaded into registers while block b is processed.
-      const int p_me = tid & 63, hq = (tid >> 6) & 1;
-      const bool is_ec = tid < 128;
-      const bool need_wt = !is_ec && hq == 1;
-      double r_c = 0.0, r_s = 0.0, r_w = 0.0, r_t = 0.0;  // record of the next block's point
-      auto load_rec = [&](int b) {
-        if (b * kBK + p_me < len) {
-          const double* r = pay + (size_t)kRec * (start + (int64_t)b * kBK + p_me);
-          r_c = r[0];
-          r_s = r[1];
-          if (need_wt) {
-            r_w = r[2];
-            r_t = r[3];
-          }
+  if (warp >= kSlicerWarps && warp < kSlicerWarps + kAnchorWarps) {
+    // ==== anchor warps: FP64 powers of e^{i phi} (FP32 storage) one block ahead ========
+    // Thread p: point p of the block.  It runs four interleaved recurrences (FP64 latency
+    // overlaps): the two halves of ec, e^{i (cbase + 2u) phi}, and of ea, e^{i Cf a phi};
+    // all starting powers are powers of two of e^{i phi}.  Then e1 and the Hermite weights
+    // g_k / scale.  The record of the point in the next block is loaded meanwhile.
+    const int p = tid - kSlicers;
+    uint32_t g = 0;
+    for (int piece = blockIdx.x; piece < npieces && !*abort_flag; piece += gridDim.x) {
+      const int64_t start = piece_start[piece];
+      const int len = piece_len[piece];
+      const int nblk = (len + kBK - 1) / kBK;
+      const double inv_scale = 1.0 / tc_scale(piecemax[piece]);
+      double c0 = 0.0, s0 = 0.0, w0 = 0.0, t0 = 0.0;  // record of the point in the next block
+      auto load = [&](int b) {
+        if (b * kBK + p < len) {
+          const double* rec = pay + (size_t)kRec * (start + (int64_t)b * kBK + p);
+          c0 = rec[0];
+          s0 = rec[1];
+          w0 = rec[2];
+          t0 = rec[3];
         }
       };
-      load_rec(0);
-      auto phase1 = [&](int b) {
-        if (*abort_flag) return;
-        const int buf = b & 1;
+      load(0);
+      for (int b = 0; b < nblk; ++b, ++g) {
+        const cplx z1 = {c0, s0};
+        const double wv = w0, tv = t0;
+        if (b + 1 < nblk) load(b + 1);
+        const int buf = g & 1;
+        if (g >= 2 && !tc::mbar_wait(&aempty[buf], ((g >> 1) - 1) & 1, abort_flag)) {
+          fail();
+          break;
+        }
         float2* e1 = e1_of(buf);
         float2* ec = ec_of(buf);
         float2* ea = ea_of(buf);
         float* gk = gk_of(buf);
-        const int np = min(kBK, len - b * kBK);
-        const int p = p_me;
-        const cplx z1 = {r_c, r_s};
-        const double wv = r_w, tv = r_t;
-        if (b + 1 < nblk) load_rec(b + 1);
-        if (p < np) {
-          // z^(2^j) for 2^j = CH/4, CH/2, CH
+        constexpr int H = CH / 4;  // ec entries per chain
+        constexpr int L = H > 8 ? H : 8;
+        if (b * kBK + p < len) {
           cplx zq = z1;
 #pragma unroll
-          for (int q = 1; q < CH / 4; q <<= 1) zq = cmul(zq, zq);
-          const cplx zh = cmul(zq, zq);      // z^(CH/2)
-          const cplx zf = cmul(zh, zh);      // z^CH
-          if (is_ec) {
-            constexpr int H = CH / 8;  // entries per chain
-            const int u0 = hq * (CH / 4);
-            const cplx st = cmul(z1, z1);
-            // za = z^(cbase + 2 u0): cbase in {0, CH}, 2 u0 in {0, CH/2}
-            cplx za = hq ? zh : cplx{1.0, 0.0};
-            if (cbase) za = cmul(za, zf);
-            cplx zb = cmul(za, zq);            // z^(cbase + 2 u0 + CH/4) = za st^H
-            for (int u = 0; u < H; ++u) {
-              ec[p * kEcStride + u0 + u] = make_float2((float)za.re, (float)za.im);
-              ec[p * kEcStride + u0 + H + u] = make_float2((float)zb.re, (float)zb.im);
-              za = cmul(za, st);
-              zb = cmul(zb, st);
-            }
-          } else {
-            const int a0 = 8 * hq;
-            const cplx st = (Cf == CH) ? zf : cmul(zf, zf);  // z^Cf, Cf in {CH, 2 CH}
-            const cplx s2 = cmul(st, st), s4 = cmul(s2, s2);
-            cplx za = hq ? cmul(s4, s4) : cplx{1.0, 0.0};     // st^a0
-            cplx zb = cmul(za, s4);
+          for (int q = 1; q < CH / 4; q <<= 1) zq = cmul(zq, zq);  // z^(CH/4)
+          const cplx zh = cmul(zq, zq);                              // z^(CH/2)
+          const cplx zf = cmul(zh, zh);                              // z^CH
+          const cplx st = cmul(z1, z1);
+          cplx ea0 = cbase ? zf : cplx{1.0, 0.0};                    // z^cbase
+          cplx eb0 = cmul(ea0, zh);                                  // z^(cbase + CH/2)
+          const cplx sc = (Cf == CH) ? zf : cmul(zf, zf);           // z^Cf, Cf in {CH, 2 CH}
+          const cplx s2 = cmul(sc, sc), s4 = cmul(s2, s2);
+          cplx aa = {1.0, 0.0};
+          cplx ab = cmul(s4, s4);                                    // z^(8 Cf)
 #pragma unroll
-            for (int a = 0; a < 4; ++a) {
-              ea[p * kEaStride + a0 + a] = make_float2((float)za.re, (float)za.im);
-              ea[p * kEaStride + a0 + 4 + a] = make_float2((float)zb.re, (float)zb.im);
-              za = cmul(za, st);
-              zb = cmul(zb, st);
+          for (int u = 0; u < L; ++u) {
+            if (u < H) {
+              ec[p * kEcStride + u] = make_float2((float)ea0.re, (float)ea0.im);
+              ec[p * kEcStride + H + u] = make_float2((float)eb0.re, (float)eb0.im);
+              ea0 = cmul(ea0, st);
+              eb0 = cmul(eb0, st);
             }
-            if (hq == 1) {
-              e1[p] = make_float2((float)z1.re, (float)z1.im);
-              double h[4];
-              hermite(tv, wv, h);
-#pragma unroll
-              for (int k = 0; k < 4; ++k) gk[p * 4 + k] = (float)(h[k] * inv_scale * kInvKScale[k]);
+            if (u < 8) {
+              ea[p * kEaStride + u] = make_float2((float)aa.re, (float)aa.im);
+              ea[p * kEaStride + 8 + u] = make_float2((float)ab.re, (float)ab.im);
+              aa = cmul(aa, sc);
+              ab = cmul(ab, sc);
             }
           }
+          e1[p] = make_float2((float)z1.re, (float)z1.im);
+          double h[4];
+          hermite(tv, wv, h);
+#pragma unroll
+          for (int k = 0; k < 4; ++k) gk[p * 4 + k] = (float)(h[k] * inv_scale * kInvKScale[k]);
         } else {  // padding points contribute zero
-          if (is_ec) {
-            for (int u = hq * (CH / 4); u < (hq + 1) * (CH / 4); ++u) ec[p * kEcStride + u] = make_float2(0.f, 0.f);
-          } else {
-            for (int a = 8 * hq; a < 8 * hq + 8; ++a) ea[p * kEaStride + a] = make_float2(0.f, 0.f);
-            if (hq == 1) {
-              e1[p] = make_float2(0.f, 0.f);
+          for (int u = 0; u < CH / 2; ++u) ec[p * kEcStride + u] = make_float2(0.f, 0.f);
+          for (int u = 0; u < 16; ++u) ea[p * kEaStride + u] = make_float2(0.f, 0.f);
+          e1[p] = make_float2(0.f, 0.f);
 #pragma unroll
-              for (int k = 0; k < 4; ++k) gk[p * 4 + k] = 0.f;
-            }
-          }
+          for (int k = 0; k < 4; ++k) gk[p * 4 + k] = 0.f;
         }
-      };
-
-      phase1(0);
-      bar_producers();
-      for (int b = 0; b < nblk; ++b) {
-        const uint32_t g = blk_count + b;
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&afull[buf]);
+      }
+    }
+  } else if (warp < kSlicerWarps) {
+    // ==== slicer warps: int8 slice tiles; warps 0-3 also run the epilogue ==============
+    uint32_t g = 0, piece_iter = 0;
+    for (int piece = blockIdx.x; piece < npieces; piece += gridDim.x, ++piece_iter) {
+      const int len = piece_len[piece];
+      const int nblk = (len + kBK - 1) / kBK;
+      for (int b = 0; b < nblk; ++b, ++g) {
         const int stage = g % S;
         const uint32_t use = g / S;
-        if (b + 1 < nblk) phase1(b + 1);  // overlaps with the other warps' slicing
-        // ---- wait until the MMAs that last read this stage are done -------------------
-        if (use > 0 && !*abort_flag) {
-          if (!tc::mbar_wait(&empty[stage], (use - 1) & 1, abort_flag)) {
-            *abort_flag = 1;
-            atomicOr(err_flags, kFlagTimeout);
-          }
+        const int buf = g & 1;
+        bool ok = !*abort_flag;
+        if (ok && !tc::mbar_wait(&afull[buf], (g >> 1) & 1, abort_flag)) {
+          fail();
+          ok = false;
         }
-        // ---- phase 2: int8 slice tiles of block b from buffer b & 1 ---------------------
+        if (ok && use > 0 && !tc::mbar_wait(&empty[stage], (use - 1) & 1, abort_flag)) {
+          fail();
+          ok = false;
+        }
         uint8_t* st_base = smem + stage * Lay::kStage;
-        if (!*abort_flag) {
-          const int buf = b & 1;
+        if (ok) {
           const float2* e1 = e1_of(buf);
           const float2* ec = ec_of(buf);
           const float2* ea = ea_of(buf);
           const float* gk = gk_of(buf);
           constexpr int nB = 4 * (CH / 2);  // (16-point chunk h, c pair)
           constexpr int nA = 4 * 32;        // (16-point chunk h, k, a pair)
-          for (int u = tid; u < nB + nA; u += kProducers) {
+          for (int u = tid; u < nB + nA; u += kSlicers) {
             int h, rows[4];
             uint8_t* base;
             int tile_bytes;
@@ -347,30 +350,30 @@ bin_sums_tc_kernel(int Nl, int Cf, int64_t Npay, const double* __restrict__ pay,
               int X[4][4];  // [value][point]
 #pragma unroll
               for (int jj = 0; jj < 4; ++jj) {
-                const int p = 16 * h + 4 * t + jj;
+                const int pp = 16 * h + 4 * t + jj;
                 float v0, v1, v2, v3;
                 if (isB) {
-                  const float2 z = ec[p * kEcStride + cp];
-                  const float2 s = e1[p];
+                  const float2 z = ec[pp * kEcStride + cp];
+                  const float2 sq = e1[pp];
                   v0 = z.x;
                   v1 = z.y;
-                  v2 = fmaf(z.x, s.x, -z.y * s.y);
-                  v3 = fmaf(z.x, s.y, z.y * s.x);
+                  v2 = fmaf(z.x, sq.x, -z.y * sq.y);
+                  v3 = fmaf(z.x, sq.y, z.y * sq.x);
+                  if (odd) {
+                    const float t0 = v0, t1 = v1;
+                    v0 = v2;
+                    v1 = v3;
+                    v2 = t0;
+                    v3 = t1;
+                  }
                 } else {
-                  const float gg = gk[p * 4 + k];
-                  const float2 z0 = ea[p * kEaStride + 2 * ap + (swap_a ? 1 : 0)];
-                  const float2 z1 = ea[p * kEaStride + 2 * ap + (swap_a ? 0 : 1)];
+                  const float gg = gk[pp * 4 + k];
+                  const float2 z0 = ea[pp * kEaStride + 2 * ap + (swap_a ? 1 : 0)];
+                  const float2 z1 = ea[pp * kEaStride + 2 * ap + (swap_a ? 0 : 1)];
                   v0 = gg * (odd ? z0.y : z0.x);
                   v1 = gg * (odd ? z0.x : z0.y);
                   v2 = gg * (odd ? z1.y : z1.x);
                   v3 = gg * (odd ? z1.x : z1.y);
-                }
-                if (isB && odd) {
-                  const float t0 = v0, t1 = v1;
-                  v0 = v2;
-                  v1 = v3;
-                  v2 = t0;
-                  v3 = t1;
                 }
                 X[0][jj] = quant(v0);
                 X[1][jj] = quant(v1);
@@ -401,108 +404,117 @@ bin_sums_tc_kernel(int Nl, int Cf, int64_t Npay, const double* __restrict__ pay,
         }
         tc::fence_async_smem();
         __syncwarp();
-        if (lane == 0) tc::mbar_arrive(&full[stage]);
-        bar_producers();  // anchors of block b consumed, anchors of block b+1 complete
+        if (lane == 0) {
+          tc::mbar_arrive(&full[stage]);
+          tc::mbar_arrive(&aempty[buf]);
+        }
       }
 
       // ---- epilogue: warps 0-3 own TMEM lanes 0-127 -----------------------------------
       // Lane r holds row r = 2 (16 k + a) + ri of D.  For every c:
       //   Vr = D[re, Rr] - D[im, Ri],  Vi = D[re, Ri] + D[im, Rr],
       // so each lane sends its D[., Ri] to its neighbour (lane r ^ 1) and keeps D[., Rr]:
-      // the re lane writes Vr, the im lane Vi, for m = Cf a + cbase + c.
+      // the re lane writes Vr, the im lane Vi, for m = Cf a + cbase + c.  Warps 4-7 go on
+      // with the next piece meanwhile.
       if (warp < 4) {
         bool ok = !*abort_flag;
         if (ok && !tc::mbar_wait(done, piece_iter & 1, abort_flag)) {
-          *abort_flag = 1;
-          atomicOr(err_flags, kFlagTimeout);
+          fail();
           ok = false;
         }
         tc::tc_fence_after();
         const int r = tid;  // TMEM lane == GEMM row
         const int ri = r & 1, j = r >> 1;
         const int k = j >> 4, a = j & 15;
-        const double f = scale * kKScale[k] / (kQ * kQ);
+        const double f = tc_scale(piecemax[piece]) * kKScale[k] / (kQ * kQ);
         const uint32_t lane_off = (uint32_t)(warp * 32) << 16;
         float* out = partial + ((size_t)piece * 8 + 2 * k + ri) * Nl;
         const int m0 = Cf * a + cbase;
         for (int cb = 0; cb < CH; cb += 8) {
-          double drr[8], dri[8];
+          double d[2][8];
 #pragma unroll
           for (int half = 0; half < 2; ++half) {
-            const uint32_t col = (half ? CH : 0) + cb;
-            uint32_t w0[8], w1[8], w2[8], w3[8];
+            uint32_t w[4][8];
             if (ok) {
-              tc::tmem_ld8(tmem + lane_off + col, w0);
-              tc::tmem_ld8(tmem + lane_off + N + col, w1);
-              tc::tmem_ld8(tmem + lane_off + 2 * N + col, w2);
-              tc::tmem_ld8(tmem + lane_off + 3 * N + col, w3);
+#pragma unroll
+              for (int q = 0; q < 4; ++q) tc::tmem_ld8_nowait(tmem + lane_off + q * N + (half ? CH : 0) + cb, w[q]);
+              tc::tmem_wait_ld();
             }
-            double* dst = half ? dri : drr;
 #pragma unroll
             for (int i = 0; i < 8; ++i)
-              dst[i] = ok ? (4294967296.0 * (double)(int)w0[i] + 16777216.0 * (double)(int)w1[i] +
-                             65536.0 * (double)(int)w2[i] + 256.0 * (double)(int)w3[i]) * f
-                          : 0.0;
+              d[half][i] = ok ? (4294967296.0 * (double)(int)w[0][i] + 16777216.0 * (double)(int)w[1][i] +
+                                 65536.0 * (double)(int)w[2][i] + 256.0 * (double)(int)w[3][i]) * f
+                              : 0.0;
           }
 #pragma unroll
           for (int i = 0; i < 8; ++i) {
-            const double x = __shfl_xor_sync(0xffffffffu, dri[i], 1);
-            const double v = ri ? x + drr[i] : drr[i] - x;
+            const double x = __shfl_xor_sync(0xffffffffu, d[1][i], 1);
+            const double v = ri ? x + d[0][i] : d[0][i] - x;
             if (m0 + cb + i < Nl) out[m0 + cb + i] = (float)v;
           }
         }
         tc::tc_fence_before();
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(tfree);
       }
-    } else {
-      // ---- MMA issuer (one thread of warp 8) --------------------------------------------
-      constexpr uint32_t iSS = idesc_i8(kM, N, true, true), iSU = idesc_i8(kM, N, true, false),
-                         iUS = idesc_i8(kM, N, false, true), iUU = idesc_i8(kM, N, false, false);
-      for (int b = 0; b < nblk && lane == 0; ++b) {
-        const uint32_t g = blk_count + b;
-        const int stage = g % S;
-        const uint32_t use = g / S;
+    }
+  } else if (warp == kSlicerWarps + kAnchorWarps) {
+    // ==== MMA issuer (one thread) ======================================================
+    constexpr uint32_t iSS = idesc_i8(kM, N, true, true), iSU = idesc_i8(kM, N, true, false),
+                       iUS = idesc_i8(kM, N, false, true), iUU = idesc_i8(kM, N, false, false);
+    if (lane == 0) {
+      uint32_t g = 0, piece_iter = 0;
+      for (int piece = blockIdx.x; piece < npieces; piece += gridDim.x, ++piece_iter) {
+        const int len = piece_len[piece];
+        const int nblk = (len + kBK - 1) / kBK;
         bool ok = !*abort_flag;
-        if (ok && !tc::mbar_wait(&full[stage], use & 1, abort_flag)) {
-          *abort_flag = 1;
-          atomicOr(err_flags, kFlagTimeout);
+        // the previous piece's epilogue has read TMEM
+        if (ok && piece_iter > 0 && !tc::mbar_wait(tfree, (piece_iter - 1) & 1, abort_flag)) {
+          fail();
           ok = false;
         }
         tc::tc_fence_after();
-        if (ok) {
-          const uint32_t base = tc::smem_addr(smem + stage * Lay::kStage);
-          uint32_t A[3], B[3];
-#pragma unroll
-          for (int t = 0; t < 3; ++t) {
-            A[t] = base + t * Lay::kTileA;
-            B[t] = base + 3 * Lay::kTileA + t * Lay::kTileB;
+        for (int b = 0; b < nblk; ++b, ++g) {
+          const int stage = g % S;
+          const uint32_t use = g / S;
+          if (ok && !tc::mbar_wait(&full[stage], use & 1, abort_flag)) {
+            fail();
+            ok = false;
           }
+          tc::tc_fence_after();
+          if (ok) {
+            const uint32_t base = tc::smem_addr(smem + stage * Lay::kStage);
+            uint32_t A[3], B[3];
 #pragma unroll
-          for (int kk = 0; kk < kBK / 32; ++kk) {
-            const uint32_t off = kk * 32;  // 32 int8 along K
-            const bool acc = (b > 0) || (kk > 0);
-            const uint32_t W0 = tmem, W1 = tmem + N, W2 = tmem + 2 * N, W3 = tmem + 3 * N;
-            const uint64_t a0 = desc_k_sw64(A[0] + off), a1 = desc_k_sw64(A[1] + off),
-                           a2 = desc_k_sw64(A[2] + off);
-            const uint64_t b0 = desc_k_sw64(B[0] + off), b1 = desc_k_sw64(B[1] + off),
-                           b2 = desc_k_sw64(B[2] + off);
-            mma_i8(W0, a0, b0, iSS, acc);
-            mma_i8(W1, a0, b1, iSU, acc);
-            mma_i8(W1, a1, b0, iUS, true);
-            mma_i8(W2, a0, b2, iSU, acc);
-            mma_i8(W2, a1, b1, iUU, true);
-            mma_i8(W2, a2, b0, iUS, true);
-            mma_i8(W3, a1, b2, iUU, acc);
-            mma_i8(W3, a2, b1, iUU, true);
+            for (int t = 0; t < 3; ++t) {
+              A[t] = base + t * Lay::kTileA;
+              B[t] = base + 3 * Lay::kTileA + t * Lay::kTileB;
+            }
+#pragma unroll
+            for (int kk = 0; kk < kBK / 32; ++kk) {
+              const uint32_t off = kk * 32;  // 32 int8 along K
+              const bool acc = (b > 0) || (kk > 0);
+              const uint32_t W0 = tmem, W1 = tmem + N, W2 = tmem + 2 * N, W3 = tmem + 3 * N;
+              const uint64_t a0 = desc_k_sw64(A[0] + off), a1 = desc_k_sw64(A[1] + off),
+                             a2 = desc_k_sw64(A[2] + off);
+              const uint64_t b0 = desc_k_sw64(B[0] + off), b1 = desc_k_sw64(B[1] + off),
+                             b2 = desc_k_sw64(B[2] + off);
+              mma_i8(W0, a0, b0, iSS, acc);
+              mma_i8(W1, a0, b1, iSU, acc);
+              mma_i8(W1, a1, b0, iUS, true);
+              mma_i8(W2, a0, b2, iSU, acc);
+              mma_i8(W2, a1, b1, iUU, true);
+              mma_i8(W2, a2, b0, iUS, true);
+              mma_i8(W3, a1, b2, iUU, acc);
+              mma_i8(W3, a2, b1, iUU, true);
+            }
           }
+          tc::mma_commit(&empty[stage]);
         }
-        tc::mma_commit(&empty[stage]);
+        tc::mma_commit(done);
       }
-      if (lane == 0) tc::mma_commit(done);
-      __syncwarp();
     }
-    blk_count += nblk;
-    __syncthreads();  // the epilogue has read TMEM; the next piece may overwrite it
-    tc::tc_fence_after();
+    __syncwarp();
   }
   __syncthreads();
   if (warp == 0) {
@@ -512,9 +524,11 @@ bin_sums_tc_kernel(int Nl, int Cf, int64_t Npay, const double* __restrict__ pay,
 }
 
 template <int CH>
-void launch_ch(const Geometry& g, const Workspace& ws, int Cf, cudaStream_t s) {
+int launch_ch(const Geometry& g, const Workspace& ws, int Cf, cudaStream_t s) {
   using Lay = Layout<CH>;
-  cudaFuncSetAttribute(bin_sums_tc_kernel<CH>, cudaFuncAttributeMaxDynamicSharedMemorySize, Lay::kBytes);
+  cudaError_t e =
+      cudaFuncSetAttribute(bin_sums_tc_kernel<CH>, cudaFuncAttributeMaxDynamicSharedMemorySize, Lay::kBytes);
+  if (e != cudaSuccess) return set_cuda_error(e, "bin_sums_tc attributes", __FILE__, __LINE__);
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -523,11 +537,14 @@ void launch_ch(const Geometry& g, const Workspace& ws, int Cf, cudaStream_t s) {
   int64_t grid = ws.pmax < per ? ws.pmax : per;
   if (grid < 1) grid = 1;
   dim3 gd((unsigned)grid, groups);
-  bin_sums_tc_kernel<CH><<<gd, kThreads, Lay::kBytes, s>>>(g.Nl, Cf, ws.npts, ws.pay, ws.npieces, ws.pmax,
+  bin_sums_tc_kernel<CH><<<gd, kThreads, Lay::kBytes, s>>>(g.Nl, Cf, ws.pay, ws.npieces, ws.pmax,
                                                            ws.piece_start, ws.piece_len, ws.piecemax,
                                                            reinterpret_cast<float*>(ws.partial),
                                                            ws.flags);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return set_cuda_error(e, "bin_sums_tc launch", __FILE__, __LINE__);
   count_launches(1);
+  return DSHT_OK;
 }
 
 }  // namespace
@@ -542,14 +559,13 @@ int tc_inner_factor(int Nl) {
 int launch_bin_sums_tc(const Geometry& g, const Workspace& ws, cudaStream_t s) {
   const int Cf = tc_inner_factor(g.Nl);
   switch (Cf) {
-    case 8: launch_ch<8>(g, ws, 8, s); break;
-    case 16: launch_ch<16>(g, ws, 16, s); break;
-    case 32: launch_ch<32>(g, ws, 32, s); break;
-    case 64: launch_ch<64>(g, ws, 64, s); break;
-    case 128: launch_ch<64>(g, ws, 128, s); break;  // two column groups
+    case 8: return launch_ch<8>(g, ws, 8, s);
+    case 16: return launch_ch<16>(g, ws, 16, s);
+    case 32: return launch_ch<32>(g, ws, 32, s);
+    case 64: return launch_ch<64>(g, ws, 64, s);
+    case 128: return launch_ch<64>(g, ws, 128, s);  // two column groups
     default: return set_error(DSHT_ERR_INVALID, "mixed precision supports Nl <= 2048 (Nl=%d)", g.Nl);
   }
-  return DSHT_OK;
 }
 
 }  // namespace dsht

@@ -238,4 +238,6 @@ int set_error(int code, const char* fmt, ...);
 // Adds n to the process-wide count of kernels this library launched.
 void count_launches(int n);
 int set_cuda_error(cudaError_t e, const char* what, const char* file, int line);
+// First kernel-launch error since the last call (recorded by count_launches), as a status.
+int launch_error(const char* where);
 }  // namespace dsht
