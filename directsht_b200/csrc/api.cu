@@ -52,9 +52,12 @@ int set_cuda_error(cudaError_t e, const char* what, const char* file, int line) 
 
 static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
+// Points per bin piece: at most 2048 (the S32 sums of the tensor path stay exact), at
+// least 256, and about N/2048 in between.  Smaller pieces keep the fixed-point scale of
+// the tensor path (the piece's largest |w h_k|) closer to its typical weight.
 int default_piece_max(const Geometry& g, int64_t N) {
   int64_t p = (N + 2047) / 2048;
-  if (p < 512) p = 512;
+  if (p < 256) p = 256;
   if (p > 2048) p = 2048;
   return (int)p;
 }

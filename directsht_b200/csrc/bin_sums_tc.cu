@@ -197,21 +197,28 @@ bin_sums_tc_kernel(int Nl, int Cf, const double* __restrict__ pay, const int* __
       const int len = piece_len[piece];
       const int nblk = (len + kBK - 1) / kBK;
       const double inv_scale = 1.0 / tc_scale(piecemax[piece]);
-      double c0 = 0.0, s0 = 0.0, w0 = 0.0, t0 = 0.0;  // record of the point in the next block
-      auto load = [&](int b) {
+      // Records of the point in the next two blocks (loads run two blocks ahead).
+      double c0 = 0.0, s0 = 0.0, w0 = 0.0, t0 = 0.0, c1 = 0.0, s1 = 0.0, w1 = 0.0, t1 = 0.0;
+      auto load = [&](int b, double& c, double& sn, double& w, double& t) {
         if (b * kBK + p < len) {
-          const double* rec = pay + (size_t)kRec * (start + (int64_t)b * kBK + p);
-          c0 = rec[0];
-          s0 = rec[1];
-          w0 = rec[2];
-          t0 = rec[3];
+          const double2* rec = reinterpret_cast<const double2*>(pay + (size_t)kRec * (start + (int64_t)b * kBK + p));
+          const double2 r0 = rec[0], r1 = rec[1];
+          c = r0.x;
+          sn = r0.y;
+          w = r1.x;
+          t = r1.y;
         }
       };
-      load(0);
+      load(0, c0, s0, w0, t0);
+      if (nblk > 1) load(1, c1, s1, w1, t1);
       for (int b = 0; b < nblk; ++b, ++g) {
         const cplx z1 = {c0, s0};
         const double wv = w0, tv = t0;
-        if (b + 1 < nblk) load(b + 1);
+        c0 = c1;
+        s0 = s1;
+        w0 = w1;
+        t0 = t1;
+        if (b + 2 < nblk) load(b + 2, c1, s1, w1, t1);
         const int buf = g & 1;
         if (g >= 2 && !tc::mbar_wait(&aempty[buf], ((g >> 1) - 1) & 1, abort_flag)) {
           fail();
@@ -313,38 +320,22 @@ bin_sums_tc_kernel(int Nl, int Cf, const double* __restrict__ pay, const int* __
             } else {
               // A rows 2 (16 k + a) + (re|im): the two halves of a complex row sit in
               // neighbouring TMEM lanes, so the epilogue combines them with one shuffle.
+              // A unit takes the a pair (ap, ap + 8).
               const int v = u - nB;
               h = v >> 5;
               k = (v & 31) >> 3;
               ap = v & 7;
-              const int j0 = 16 * k + 2 * ap;
-              rows[0] = 2 * j0;          // re, a = 2ap
+              const int j0 = 16 * k + ap;
+              rows[0] = 2 * j0;          // re, a = ap
               rows[1] = 2 * j0 + 1;      // im
-              rows[2] = 2 * j0 + 2;      // re, a = 2ap + 1
-              rows[3] = 2 * j0 + 3;      // im
+              rows[2] = 2 * j0 + 16;     // re, a = ap + 8
+              rows[3] = 2 * j0 + 17;     // im
               base = st_base;
               tile_bytes = Lay::kTileA;
             }
-            // The first row each lane writes is chosen so that the eight lanes of a quarter
-            // warp cover all eight 16-byte bank groups: B units swap the pair members on
-            // lane bit 2; A units swap the a pair on lane bit 1 and re/im on lane bit 2.
-            const bool odd = ((lane >> 2) & 1) != 0;
-            const bool swap_a = !isB && ((lane >> 1) & 1) != 0;
-            if (isB ? odd : swap_a) {
-              const int r0 = rows[0], r1 = rows[1];
-              rows[0] = rows[2];
-              rows[1] = rows[3];
-              rows[2] = r0;
-              rows[3] = r1;
-            }
-            if (!isB && odd) {
-              int r = rows[0];
-              rows[0] = rows[1];
-              rows[1] = r;
-              r = rows[2];
-              rows[2] = rows[3];
-              rows[3] = r;
-            }
+            // A quarter warp's first stores land in four distinct 16-byte bank groups
+            // (two-way conflicts): the swizzle XORs the chunk with (row / 2) & 3, which runs
+            // through 0..3 with cp or ap.
 #pragma unroll
             for (int t = 0; t < 4; ++t) {
               int X[4][4];  // [value][point]
@@ -359,21 +350,14 @@ bin_sums_tc_kernel(int Nl, int Cf, const double* __restrict__ pay, const int* __
                   v1 = z.y;
                   v2 = fmaf(z.x, sq.x, -z.y * sq.y);
                   v3 = fmaf(z.x, sq.y, z.y * sq.x);
-                  if (odd) {
-                    const float t0 = v0, t1 = v1;
-                    v0 = v2;
-                    v1 = v3;
-                    v2 = t0;
-                    v3 = t1;
-                  }
                 } else {
                   const float gg = gk[pp * 4 + k];
-                  const float2 z0 = ea[pp * kEaStride + 2 * ap + (swap_a ? 1 : 0)];
-                  const float2 z1 = ea[pp * kEaStride + 2 * ap + (swap_a ? 0 : 1)];
-                  v0 = gg * (odd ? z0.y : z0.x);
-                  v1 = gg * (odd ? z0.x : z0.y);
-                  v2 = gg * (odd ? z1.y : z1.x);
-                  v3 = gg * (odd ? z1.x : z1.y);
+                  const float2 z0 = ea[pp * kEaStride + ap];
+                  const float2 z1 = ea[pp * kEaStride + ap + 8];
+                  v0 = gg * z0.x;
+                  v1 = gg * z0.y;
+                  v2 = gg * z1.x;
+                  v3 = gg * z1.y;
                 }
                 X[0][jj] = quant(v0);
                 X[1][jj] = quant(v1);

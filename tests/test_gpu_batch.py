@@ -150,3 +150,26 @@ def test_f32_table_plan():
         ref = O.direct_sht(tab, th, ph, w)
         assert _rel(got[i], ref) <= 1e-7, i
         assert _rel(d(th, ph, w), ref) <= 1e-7, i
+
+
+def test_pipeline_overlapped_host_transforms():
+    """Pipeline: host point sets in, host alm out, copies overlapped with the previous
+    transform's kernels; every result equals DirectSHT.__call__ on the same arrays."""
+    from directsht_b200.pipeline import Pipeline
+    Nl, Nx = 64, 128
+    d = DirectSHT(Nl, Nx, precision="mixed")
+    sets = _sets(7, [30000, 12000, 30000, 500, 25000])
+    pipe = Pipeline(d, max_N=30000, depth=2)
+    tickets = [pipe.submit(*s) for s in sets[:2]]
+    outs = [pipe.result(tickets[0])]
+    tickets = tickets[1:] + [pipe.submit(*s) for s in sets[2:]]
+    outs += [pipe.result(t) for t in tickets]
+    for (th, ph, w), got in zip(sets, outs):
+        single = d(th, ph, w)
+        assert _rel(got, single) <= 1e-13 or np.array_equal(got, single)
+    with pytest.raises(ValueError):
+        pipe.submit(*_sets(8, [40000])[0])
+    # pinned CPU tensors go to the device without the staging copy
+    th, ph, w = sets[0]
+    pt = [torch.from_numpy(a).pin_memory() for a in (th, ph, w)]
+    assert _rel(pipe.result(pipe.submit(*pt)), outs[0]) <= 1e-13
