@@ -43,7 +43,6 @@ constexpr int kAnchorWarps = 2;         // warps 8-9: FP64 anchors, one block ah
 constexpr int kSlicers = 32 * kSlicerWarps;
 constexpr int kThreads = 32 * (kSlicerWarps + kAnchorWarps + 1);  // + warp 10: MMA issuer
 constexpr int kM = 128;
-constexpr int kStages = 3;
 constexpr float kQf = 4193280.0f;       // 2^22 - 2^10: |X| < 2^22, so X >> 16 fits int8
 constexpr double kQ = 4193280.0;
 constexpr float kMagic = 12582912.0f;   // 1.5 * 2^23 (bit pattern 0x4B400000)
@@ -66,6 +65,10 @@ struct cplx {
 __device__ __forceinline__ cplx cmul(cplx a, cplx b) {
   return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
 }
+// rint(x q) of an FP64 value: one DFMA puts x q into the binade of 1.5*2^52, whose low
+// word is then the rounded integer (no conversion instruction).
+__device__ __forceinline__ int qfix(double x) { return __double2loint(fma(x, kQ, 6755399441055744.0)); }
+
 // rint(x q) for |x| <= 1: one FMA puts x q into the binade of 1.5*2^23, where the
 // float's bit pattern minus that of 1.5*2^23 is the rounded integer.
 __device__ __forceinline__ int quant(float x) { return __float_as_int(fmaf(x, kQf, kMagic)) - 0x4B400000; }
@@ -107,15 +110,54 @@ __device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t adesc, uint64_t
       : "memory");
 }
 
+// One slicing unit: 16 points (chunk h of the 64-point block) x 4 operand rows.  `values`
+// writes the four fixed-point values of point pp into X[0..3]; they are byte-transposed
+// into the three slice tiles (slice s of four points is byte 2 - s of X) and stored as
+// 16-byte chunks of the 64-byte swizzled K-major rows (chunk h XOR (row / 2) & 3).  A
+// quarter warp's first stores land in four distinct 16-byte bank groups.
+template <typename F>
+__device__ __forceinline__ void slice_unit(uint8_t* base, int tile_bytes, int h, const int* rows, F values) {
+  uint32_t w[4][3][4];  // [value][slice][word of 4 points]
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    int X[4][4];  // [point][value]
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) values(16 * h + 4 * t + jj, X[jj]);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const uint32_t t0 = __byte_perm((uint32_t)X[0][e], (uint32_t)X[1][e], 0x5140);
+      const uint32_t t1 = __byte_perm((uint32_t)X[0][e], (uint32_t)X[1][e], 0x7362);
+      const uint32_t u0 = __byte_perm((uint32_t)X[2][e], (uint32_t)X[3][e], 0x5140);
+      const uint32_t u1 = __byte_perm((uint32_t)X[2][e], (uint32_t)X[3][e], 0x7362);
+      w[e][0][t] = __byte_perm(t1, u1, 0x5410);
+      w[e][1][t] = __byte_perm(t0, u0, 0x7632);
+      w[e][2][t] = __byte_perm(t0, u0, 0x5410);
+    }
+  }
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    uint8_t* rowp = base + rows[e] * 64 + ((h ^ ((rows[e] >> 1) & 3)) << 4);
+#pragma unroll
+    for (int sl = 0; sl < 3; ++sl)
+      *reinterpret_cast<uint4*>(rowp + sl * tile_bytes) = make_uint4(w[e][sl][0], w[e][sl][1], w[e][sl][2], w[e][sl][3]);
+  }
+}
+
 template <int CH>
 struct Layout {
   static constexpr int N = 2 * CH;
   static constexpr int kTileA = kM * 64;                      // bytes of one A slice tile
   static constexpr int kTileB = N * 64;
   static constexpr int kStage = 3 * kTileA + 3 * kTileB;      // A0..A2, B0..B2
-  static constexpr int kAnchorBytes = kBK * (8 + (CH / 2 + 1) * 8 + 17 * 8 + 4 * 4);
+  // Anchor buffer: eb [64][CH + 2] int2 (fixed-point e^{i c phi}; rows padded by 16 bytes
+  // so that a quarter warp's 16-byte stores of different points hit different banks),
+  // ea [64][17] float2, gk [64][4] float.
+  static constexpr int kEbStride = CH + 2;                    // int2 per point
+  static constexpr int kAnchorBytes = kBK * (kEbStride * 8 + 17 * 8 + 4 * 4);
   static constexpr int kUnion = 2 * kAnchorBytes;
-  static constexpr int kUnionOff = kStages * kStage;
+  // As many operand stages (3 or 2) as fit beside the two anchor buffers.
+  static constexpr int kStagesFit = (3 * kStage + ((kUnion + 1023) / 1024) * 1024 + 256 + 1024 <= 227 * 1024) ? 3 : 2;
+  static constexpr int kUnionOff = kStagesFit * kStage;
   static constexpr int kMiscOff = kUnionOff + ((kUnion + 1023) / 1024) * 1024;
   static constexpr int kBytes = kMiscOff + 256 + 1024;        // + alignment slack
   // W0..W3 in columns [jN, (j+1)N); the epilogue reads 32-column windows starting below
@@ -134,18 +176,17 @@ bin_sums_tc_kernel(int Nl, int Cf, const double* __restrict__ pay, const int* __
                    unsigned* __restrict__ err_flags) {
   using Lay = Layout<CH>;
   constexpr int N = Lay::N;
-  constexpr int S = kStages;
+  constexpr int S = Lay::kStagesFit;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint8_t* uni = smem + Lay::kUnionOff;
   // Row strides are padded by one entry so that lanes holding consecutive points hit
   // different banks.
-  constexpr int kEcStride = CH / 2 + 1, kEaStride = 17;
+  constexpr int kEbStride = Lay::kEbStride, kEaStride = 17;
   // Two anchor buffers (global block g uses buffer g & 1), each laid out as
-  //   e1 [64] e^{i phi} | ec [64][CH/2+1] e^{i (cbase + 2u) phi} | ea [64][17] e^{i Cf a phi} | gk [64][4]
-  auto e1_of = [&](int buf) { return reinterpret_cast<float2*>(uni + buf * Lay::kAnchorBytes); };
-  auto ec_of = [&](int buf) { return e1_of(buf) + kBK; };
-  auto ea_of = [&](int buf) { return ec_of(buf) + kBK * kEcStride; };
+  //   eb [64][CH+2] int2 rint(q e^{i (cbase + c) phi}) | ea [64][17] e^{i Cf a phi} | gk [64][4]
+  auto eb_of = [&](int buf) { return reinterpret_cast<int2*>(uni + buf * Lay::kAnchorBytes); };
+  auto ea_of = [&](int buf) { return reinterpret_cast<float2*>(eb_of(buf) + kBK * kEbStride); };
   auto gk_of = [&](int buf) { return reinterpret_cast<float*>(ea_of(buf) + kBK * kEaStride); };
   uint8_t* misc = smem + Lay::kMiscOff;
   uint64_t* full = reinterpret_cast<uint64_t*>(misc);            // [S]  slicers -> MMA
@@ -224,11 +265,10 @@ bin_sums_tc_kernel(int Nl, int Cf, const double* __restrict__ pay, const int* __
           fail();
           break;
         }
-        float2* e1 = e1_of(buf);
-        float2* ec = ec_of(buf);
+        int4* eb = reinterpret_cast<int4*>(eb_of(buf) + p * kEbStride);  // pairs of c
         float2* ea = ea_of(buf);
         float* gk = gk_of(buf);
-        constexpr int H = CH / 4;  // ec entries per chain
+        constexpr int H = CH / 4;  // c pairs per chain
         constexpr int L = H > 8 ? H : 8;
         if (b * kBK + p < len) {
           cplx zq = z1;
@@ -246,8 +286,10 @@ bin_sums_tc_kernel(int Nl, int Cf, const double* __restrict__ pay, const int* __
 #pragma unroll
           for (int u = 0; u < L; ++u) {
             if (u < H) {
-              ec[p * kEcStride + u] = make_float2((float)ea0.re, (float)ea0.im);
-              ec[p * kEcStride + H + u] = make_float2((float)eb0.re, (float)eb0.im);
+              // c = 2u, 2u + 1 and CH/2 + 2u, CH/2 + 2u + 1, straight to fixed point
+              const cplx a1 = cmul(ea0, z1), b1 = cmul(eb0, z1);
+              eb[u] = make_int4(qfix(ea0.re), qfix(ea0.im), qfix(a1.re), qfix(a1.im));
+              eb[H + u] = make_int4(qfix(eb0.re), qfix(eb0.im), qfix(b1.re), qfix(b1.im));
               ea0 = cmul(ea0, st);
               eb0 = cmul(eb0, st);
             }
@@ -258,15 +300,13 @@ bin_sums_tc_kernel(int Nl, int Cf, const double* __restrict__ pay, const int* __
               ab = cmul(ab, sc);
             }
           }
-          e1[p] = make_float2((float)z1.re, (float)z1.im);
           double h[4];
           hermite(tv, wv, h);
 #pragma unroll
           for (int k = 0; k < 4; ++k) gk[p * 4 + k] = (float)(h[k] * inv_scale * kInvKScale[k]);
         } else {  // padding points contribute zero
-          for (int u = 0; u < CH / 2; ++u) ec[p * kEcStride + u] = make_float2(0.f, 0.f);
+          for (int u = 0; u < CH / 2; ++u) eb[u] = make_int4(0, 0, 0, 0);
           for (int u = 0; u < 16; ++u) ea[p * kEaStride + u] = make_float2(0.f, 0.f);
-          e1[p] = make_float2(0.f, 0.f);
 #pragma unroll
           for (int k = 0; k < 4; ++k) gk[p * 4 + k] = 0.f;
         }
@@ -295,95 +335,39 @@ bin_sums_tc_kernel(int Nl, int Cf, const double* __restrict__ pay, const int* __
         }
         uint8_t* st_base = smem + stage * Lay::kStage;
         if (ok) {
-          const float2* e1 = e1_of(buf);
-          const float2* ec = ec_of(buf);
+          const int4* eb = reinterpret_cast<const int4*>(eb_of(buf));
           const float2* ea = ea_of(buf);
           const float* gk = gk_of(buf);
           constexpr int nB = 4 * (CH / 2);  // (16-point chunk h, c pair)
           constexpr int nA = 4 * 32;        // (16-point chunk h, k, a pair)
-          for (int u = tid; u < nB + nA; u += kSlicers) {
-            int h, rows[4];
-            uint8_t* base;
-            int tile_bytes;
-            uint32_t w[4][3][4];  // [value][slice][word of 4 points]
-            const bool isB = u < nB;
-            int cp = 0, k = 0, ap = 0;
-            if (isB) {
-              h = u / (CH / 2);
-              cp = u % (CH / 2);
-              rows[0] = 2 * cp;            // Re e^{i c phi},       c = 2cp
-              rows[1] = CH + 2 * cp;       // Im e^{i c phi}
-              rows[2] = 2 * cp + 1;        // Re e^{i (c+1) phi}
-              rows[3] = CH + 2 * cp + 1;   // Im e^{i (c+1) phi}
-              base = st_base + 3 * Lay::kTileA;
-              tile_bytes = Lay::kTileB;
-            } else {
-              // A rows 2 (16 k + a) + (re|im): the two halves of a complex row sit in
-              // neighbouring TMEM lanes, so the epilogue combines them with one shuffle.
-              // A unit takes the a pair (ap, ap + 8).
-              const int v = u - nB;
-              h = v >> 5;
-              k = (v & 31) >> 3;
-              ap = v & 7;
-              const int j0 = 16 * k + ap;
-              rows[0] = 2 * j0;          // re, a = ap
-              rows[1] = 2 * j0 + 1;      // im
-              rows[2] = 2 * j0 + 16;     // re, a = ap + 8
-              rows[3] = 2 * j0 + 17;     // im
-              base = st_base;
-              tile_bytes = Lay::kTileA;
-            }
-            // A quarter warp's first stores land in four distinct 16-byte bank groups
-            // (two-way conflicts): the swizzle XORs the chunk with (row / 2) & 3, which runs
-            // through 0..3 with cp or ap.
-#pragma unroll
-            for (int t = 0; t < 4; ++t) {
-              int X[4][4];  // [value][point]
-#pragma unroll
-              for (int jj = 0; jj < 4; ++jj) {
-                const int pp = 16 * h + 4 * t + jj;
-                float v0, v1, v2, v3;
-                if (isB) {
-                  const float2 z = ec[pp * kEcStride + cp];
-                  const float2 sq = e1[pp];
-                  v0 = z.x;
-                  v1 = z.y;
-                  v2 = fmaf(z.x, sq.x, -z.y * sq.y);
-                  v3 = fmaf(z.x, sq.y, z.y * sq.x);
-                } else {
-                  const float gg = gk[pp * 4 + k];
-                  const float2 z0 = ea[pp * kEaStride + ap];
-                  const float2 z1 = ea[pp * kEaStride + ap + 8];
-                  v0 = gg * z0.x;
-                  v1 = gg * z0.y;
-                  v2 = gg * z1.x;
-                  v3 = gg * z1.y;
-                }
-                X[0][jj] = quant(v0);
-                X[1][jj] = quant(v1);
-                X[2][jj] = quant(v2);
-                X[3][jj] = quant(v3);
-              }
-#pragma unroll
-              for (int e = 0; e < 4; ++e) {
-                // 4 x 4 byte transpose: slice s of the four points is byte (2 - s) of X.
-                const uint32_t t0 = __byte_perm((uint32_t)X[e][0], (uint32_t)X[e][1], 0x5140);
-                const uint32_t t1 = __byte_perm((uint32_t)X[e][0], (uint32_t)X[e][1], 0x7362);
-                const uint32_t u0 = __byte_perm((uint32_t)X[e][2], (uint32_t)X[e][3], 0x5140);
-                const uint32_t u1 = __byte_perm((uint32_t)X[e][2], (uint32_t)X[e][3], 0x7362);
-                w[e][0][t] = __byte_perm(t1, u1, 0x5410);
-                w[e][1][t] = __byte_perm(t0, u0, 0x7632);
-                w[e][2][t] = __byte_perm(t0, u0, 0x5410);
-              }
-            }
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-              uint8_t* rowp = base + rows[e] * 64 + ((h ^ ((rows[e] >> 1) & 3)) << 4);
-#pragma unroll
-              for (int sl = 0; sl < 3; ++sl)
-                *reinterpret_cast<uint4*>(rowp + sl * tile_bytes) =
-                    make_uint4(w[e][sl][0], w[e][sl][1], w[e][sl][2], w[e][sl][3]);
-            }
+          // One unit per thread; the B and A units are separate straight-line paths.
+          if (tid < nB) {
+            const int h = tid / (CH / 2), cp = tid % (CH / 2);
+            const int rows[4] = {2 * cp, CH + 2 * cp, 2 * cp + 1, CH + 2 * cp + 1};  // Re/Im of c, c+1
+            slice_unit(st_base + 3 * Lay::kTileA, Lay::kTileB, h, rows, [&](int pp, int* X) {
+              const int4 q = eb[pp * (kEbStride / 2) + cp];  // already fixed point
+              X[0] = q.x;
+              X[1] = q.y;
+              X[2] = q.z;
+              X[3] = q.w;
+            });
+          } else if (tid < nB + nA) {
+            // A rows 2 (16 k + a) + (re|im): the two halves of a complex row sit in
+            // neighbouring TMEM lanes, so the epilogue combines them with one shuffle.
+            // A unit takes the a pair (ap, ap + 8).
+            const int v = tid - nB;
+            const int h = v >> 5, k = (v & 31) >> 3, ap = v & 7;
+            const int j0 = 16 * k + ap;
+            const int rows[4] = {2 * j0, 2 * j0 + 1, 2 * j0 + 16, 2 * j0 + 17};
+            slice_unit(st_base, Lay::kTileA, h, rows, [&](int pp, int* X) {
+              const float gg = gk[pp * 4 + k];
+              const float2 z0 = ea[pp * kEaStride + ap];
+              const float2 z1 = ea[pp * kEaStride + ap + 8];
+              X[0] = quant(gg * z0.x);
+              X[1] = quant(gg * z0.y);
+              X[2] = quant(gg * z1.x);
+              X[3] = quant(gg * z1.y);
+            });
           }
         }
         tc::fence_async_smem();
@@ -414,8 +398,12 @@ bin_sums_tc_kernel(int Nl, int Cf, const double* __restrict__ pay, const int* __
         const uint32_t lane_off = (uint32_t)(warp * 32) << 16;
         float* out = partial + ((size_t)piece * 8 + 2 * k + ri) * Nl;
         const int m0 = Cf * a + cbase;
+        // D q^2 / 2^8 = 2^24 W0 + 2^16 W1 + 2^8 W2 + W3 is an exact integer below 2^50, so
+        // the re/im combination is done in int64 too and each output needs one conversion
+        // (through the bit pattern of 1.5 2^52: no conversion-pipe instruction).
+        const double fs = f * 256.0;
         for (int cb = 0; cb < CH; cb += 8) {
-          double d[2][8];
+          long long T[2][8];
 #pragma unroll
           for (int half = 0; half < 2; ++half) {
             uint32_t w[4][8];
@@ -426,15 +414,16 @@ bin_sums_tc_kernel(int Nl, int Cf, const double* __restrict__ pay, const int* __
             }
 #pragma unroll
             for (int i = 0; i < 8; ++i)
-              d[half][i] = ok ? (4294967296.0 * (double)(int)w[0][i] + 16777216.0 * (double)(int)w[1][i] +
-                                 65536.0 * (double)(int)w[2][i] + 256.0 * (double)(int)w[3][i]) * f
-                              : 0.0;
+              T[half][i] = ok ? ((long long)(int)w[0][i] << 24) + ((long long)(int)w[1][i] << 16) +
+                                    ((long long)(int)w[2][i] << 8) + (long long)(int)w[3][i]
+                              : 0ll;
           }
 #pragma unroll
           for (int i = 0; i < 8; ++i) {
-            const double x = __shfl_xor_sync(0xffffffffu, d[1][i], 1);
-            const double v = ri ? x + d[0][i] : d[0][i] - x;
-            if (m0 + cb + i < Nl) out[m0 + cb + i] = (float)v;
+            const long long x = __shfl_xor_sync(0xffffffffu, T[1][i], 1);
+            const long long v = ri ? x + T[0][i] : T[0][i] - x;
+            const double dv = __longlong_as_double(v + 0x4338000000000000ll) - 6755399441055744.0;
+            if (m0 + cb + i < Nl) out[m0 + cb + i] = (float)(dv * fs);
           }
         }
         tc::tc_fence_before();

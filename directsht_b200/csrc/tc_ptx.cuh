@@ -39,17 +39,29 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait for the phase with the given parity to complete; false on timeout.
-// After a few immediate polls the waiting thread sleeps between polls, so a waiter does
-// not take issue slots from the warps it waits for.  The bound is about 2^22 polls.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, const volatile int* abort,
-                                          uint32_t max_polls = (1u << 22)) {
-  for (uint32_t i = 0; i < max_polls; ++i) {
-    if (mbar_try_wait(bar, parity)) return true;
-    if (i >= 8) __nanosleep(i < 64 ? 32 : 128);
-    if ((i & 255u) == 255u && *abort) return false;
+// try_wait with a suspend-time hint: the thread is suspended in hardware until the phase
+// completes or about `ns` nanoseconds pass, so waiting costs no issue slots and resumes as
+// soon as the phase completes.
+__device__ __forceinline__ bool mbar_try_wait_for(uint64_t* bar, uint32_t parity, uint32_t ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity), "r"(ns)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait for the phase with the given parity to complete; false after about 2^31 SM
+// clock cycles (~1 s) or when *abort is set.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, const volatile int* abort) {
+  const long long t0 = clock64();
+  for (uint32_t i = 0;; ++i) {
+    if (mbar_try_wait_for(bar, parity, 10000u)) return true;
+    if ((i & 15u) == 15u && (*abort || clock64() - t0 > (1ll << 31))) return false;
   }
-  return false;
 }
 
 // Make this thread's generic-proxy shared-memory writes visible to the async proxy
