@@ -8,7 +8,7 @@ and has no batch layer; this module is the B200 batch runner around the library'
   not fit keep FP32 tables only;
 * the transforms of one plan are dealt into sub-batches (largest first, balanced by points)
   that run on their own CUDA streams; inside a sub-batch the library shares one read of the
-  tables between up to three transforms and one rotation recursion between up to eight;
+  tables between up to four transforms and one rotation recursion between up to eight;
 * the whole batch is enqueued without any host synchronisation, so it can be captured once
   into a CUDA graph and replayed with a single launch (``TransformBatch.capture``);
 * ``autotune`` picks, per plan, the piece size of the bin sums, the maps per contraction

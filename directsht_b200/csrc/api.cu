@@ -117,9 +117,12 @@ int plan_piece_max(const dsht_plan_s* p, int64_t N) {
   return p->tune_piece_max > 0 ? p->tune_piece_max : default_piece_max(p->g, N);
 }
 
+// Two folds per contraction pass unless tuned: the 32-row kernel keeps two maps' FP64
+// sums in registers; passes of three or four maps use 16-row items, whose extra fold
+// reloads cost more than the table reads they save (measured at Nl=1024, Nx=2048).
 int plan_maps_per_pass(const dsht_plan_s* p) {
   const int mx = contract_stream_max_maps(true);
-  return p->tune_maps_per_pass > 0 ? std::min(p->tune_maps_per_pass, mx) : mx;
+  return p->tune_maps_per_pass > 0 ? std::min(p->tune_maps_per_pass, mx) : std::min(2, mx);
 }
 
 Route plan_route(const dsht_plan_s* p, int64_t N) {
@@ -258,6 +261,7 @@ int run_items(dsht_plan_s* p, const Item* items, int n, int mode, const Workspac
           out.pol[k] = ws.alm_pol + nlm2 * (base + k);
         }
         launch_contract_pass(g, f32_tables, f32_tables ? p->tmYv32 : p->tmYv, f32_tables ? p->tmYd32 : p->tmYd,
+                             p->tmYv32h, p->tmYd32h,
                              ws.fold, fold_stride, (int)pass.size(), ws.tile_live2, out, ws.slot_flags + base, s);
       }
       for (int it : pass) pend.push_back(it);
@@ -428,7 +432,9 @@ int dsht_plan_create(int Nl, int Nx, double xmax, int flags, dsht_plan_t* plan) 
   if (f32_only) {
     if (!(contract_stream_ok(p->g, sizeof(float)) &&
           make_table_tmap(&p->tmYv32, p->Yv32, sizeof(float), Nx, p->g.Nlm) == DSHT_OK &&
-          make_table_tmap(&p->tmYd32, p->Yd32, sizeof(float), Nx, p->g.Nlm) == DSHT_OK)) {
+          make_table_tmap(&p->tmYd32, p->Yd32, sizeof(float), Nx, p->g.Nlm) == DSHT_OK &&
+          make_table_tmap(&p->tmYv32h, p->Yv32, sizeof(float), Nx, p->g.Nlm, 16) == DSHT_OK &&
+          make_table_tmap(&p->tmYd32h, p->Yd32, sizeof(float), Nx, p->g.Nlm, 16) == DSHT_OK)) {
       dsht_plan_destroy(p);
       return DSHT_ERR_CUDA;
     }
@@ -485,7 +491,9 @@ int dsht_set_precision(dsht_plan_t p, int precision) {
     DSHT_CUDA_OK(cudaDeviceSynchronize());
     if (contract_stream_ok(p->g, sizeof(float)) &&
         make_table_tmap(&p->tmYv32, p->Yv32, sizeof(float), p->g.Nx, p->g.Nlm) == DSHT_OK &&
-        make_table_tmap(&p->tmYd32, p->Yd32, sizeof(float), p->g.Nx, p->g.Nlm) == DSHT_OK)
+        make_table_tmap(&p->tmYd32, p->Yd32, sizeof(float), p->g.Nx, p->g.Nlm) == DSHT_OK &&
+        make_table_tmap(&p->tmYv32h, p->Yv32, sizeof(float), p->g.Nx, p->g.Nlm, 16) == DSHT_OK &&
+        make_table_tmap(&p->tmYd32h, p->Yd32, sizeof(float), p->g.Nx, p->g.Nlm, 16) == DSHT_OK)
       p->tm32 = true;
   }
   p->precision = precision;

@@ -77,11 +77,11 @@ __device__ __forceinline__ void item_of(int64_t item, int Nl, int* m_out, int* g
 // FP64 tables: double tables and fold, 16 rows per item, FP64 FMAs.  FP32 tables (the
 // DSHT_PREC_MIXED level): float tables and fold, 32 rows per item, FP32 FMAs within a
 // tile and FP64 sums across tiles -- half the HBM traffic.
-template <bool kMixed, int kG = 1>
+template <bool kMixed, int kG = 1, int kRowsSet = 0>
 struct StageLayout {
   using T = typename std::conditional<kMixed, float, double>::type;
   using F4 = typename std::conditional<kMixed, float4, double4>::type;
-  static constexpr int kRows = kMixed ? 32 : 16;
+  static constexpr int kRows = kRowsSet ? kRowsSet : kMixed ? 32 : 16;
   static constexpr int kRowsPerWarp = kRows / 8;               // same parity, stride 2
   static constexpr int kTab = kRows * kTJ * sizeof(T);         // one of Yv, Yd
   static constexpr int kFold = 4 * kTJ * sizeof(F4);           // 4 q x kTJ, one map
@@ -91,14 +91,16 @@ struct StageLayout {
 
 // kG maps per pass (multi-map transforms): map g's fold at fold_v + g * fold_stride (F4
 // elements) and its alm at out.equ[g], out.pol[g] (2 Nlm doubles each).  The
-// table tile in shared memory serves all kG maps, so a pass reads the tables once.
-template <bool kMixed, int kG>
+// table tile in shared memory serves all kG maps, so a pass reads the tables once.  Passes
+// of three or four maps take 16-row items (two rows per warp), which keeps the FP64
+// accumulators of all maps in registers.
+template <bool kMixed, int kG, int kRowsSet = 0>
 __global__ void __launch_bounds__(kThreads, 1)
 contract_stream_kernel(int Nl, int Nx, int64_t nitems, const __grid_constant__ CUtensorMap tmv,
                        const __grid_constant__ CUtensorMap tmd, const void* __restrict__ fold_v,
                        int64_t fold_stride, const uint8_t* __restrict__ live, int ntile,
                        const MapOut out, unsigned* __restrict__ err) {
-  using L = StageLayout<kMixed, kG>;
+  using L = StageLayout<kMixed, kG, kRowsSet>;
   using T = typename L::T;
   using F4 = typename L::F4;
   constexpr int kRows = L::kRows;
@@ -266,8 +268,8 @@ bool contract_stream_ok(const Geometry& g, size_t elem_bytes) {
   return ((size_t)g.Nx * elem_bytes) % 16 == 0;
 }
 
-int make_table_tmap(CUtensorMap* tm, const void* base, size_t elem_bytes, int Nx, int64_t Nlm) {
-  const int kRows = elem_bytes == 8 ? StageLayout<false, 1>::kRows : StageLayout<true, 1>::kRows;
+int make_table_tmap(CUtensorMap* tm, const void* base, size_t elem_bytes, int Nx, int64_t Nlm, int rows) {
+  const int kRows = rows > 0 ? rows : elem_bytes == 8 ? StageLayout<false, 1>::kRows : StageLayout<true, 1>::kRows;
   static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
   if (!encode) {
     void* fn = nullptr;
@@ -289,11 +291,11 @@ int make_table_tmap(CUtensorMap* tm, const void* base, size_t elem_bytes, int Nx
   return DSHT_OK;
 }
 
-template <bool kMixed, int kG>
+template <bool kMixed, int kG, int kRowsSet = 0>
 static void stream_launch(const Geometry& g, const CUtensorMap& tmv, const CUtensorMap& tmd, const void* fold,
                           int64_t fold_stride, const uint8_t* live, const MapOut& out, unsigned* flags,
                           cudaStream_t s) {
-  using L = StageLayout<kMixed, kG>;
+  using L = StageLayout<kMixed, kG, kRowsSet>;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -301,9 +303,10 @@ static void stream_launch(const Geometry& g, const CUtensorMap& tmv, const CUten
   int64_t nitems = 0;
   for (int m = 0; m < g.Nl; ++m) nitems += (g.Nl - m + L::kRows - 1) / L::kRows;
   const int64_t grid = nitems < sms ? nitems : sms;
-  cudaFuncSetAttribute(contract_stream_kernel<kMixed, kG>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kBytes);
-  contract_stream_kernel<kMixed, kG><<<(unsigned)grid, kThreads, L::kBytes, s>>>(
-      g.Nl, g.Nx, nitems, tmv, tmd, fold, fold_stride, live, ntile, out, flags);
+  auto kern = contract_stream_kernel<kMixed, kG, kRowsSet>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kBytes);
+  kern<<<(unsigned)grid, kThreads, L::kBytes, s>>>(g.Nl, g.Nx, nitems, tmv, tmd, fold, fold_stride, live, ntile,
+                                                   out, flags);
   count_launches(1);
 }
 
@@ -321,10 +324,12 @@ void launch_contract_stream(const Geometry& g, bool mixed, const CUtensorMap& tm
 int contract_stream_max_maps(bool mixed) { return mixed ? kMaxPass : 1; }
 
 void launch_contract_pass(const Geometry& g, bool mixed, const CUtensorMap& tmv, const CUtensorMap& tmd,
-                          const void* fold, int64_t fold_stride, int nmaps, const uint8_t* live, const MapOut& out,
-                          unsigned* flags, cudaStream_t s) {
-  if (mixed && nmaps == 3)
-    stream_launch<true, 3>(g, tmv, tmd, fold, fold_stride, live, out, flags, s);
+                          const CUtensorMap& tmv16, const CUtensorMap& tmd16, const void* fold, int64_t fold_stride,
+                          int nmaps, const uint8_t* live, const MapOut& out, unsigned* flags, cudaStream_t s) {
+  if (mixed && nmaps == 4)
+    stream_launch<true, 4, 16>(g, tmv16, tmd16, fold, fold_stride, live, out, flags, s);
+  else if (mixed && nmaps == 3)
+    stream_launch<true, 3, 16>(g, tmv16, tmd16, fold, fold_stride, live, out, flags, s);
   else if (mixed && nmaps == 2)
     stream_launch<true, 2>(g, tmv, tmd, fold, fold_stride, live, out, flags, s);
   else if (mixed)

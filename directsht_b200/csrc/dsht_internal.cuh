@@ -43,7 +43,7 @@ struct Geometry {
 };
 
 // Output pointers of one contraction pass (kernel parameter, passed by value).
-constexpr int kMaxPass = 3;
+constexpr int kMaxPass = 4;
 struct MapOut {
   double* equ[kMaxPass];
   double* pol[kMaxPass];
@@ -133,10 +133,12 @@ void launch_contract_stream(const Geometry& g, bool mixed, const CUtensorMap& tm
 // out.equ[k], out.pol[k].  FP64 tables take one fold per launch.
 int contract_stream_max_maps(bool mixed);
 void launch_contract_pass(const Geometry& g, bool mixed, const CUtensorMap& tmv, const CUtensorMap& tmd,
-                          const void* fold, int64_t fold_stride, int nmaps, const uint8_t* live, const MapOut& out,
-                          unsigned* flags, cudaStream_t s);
+                          const CUtensorMap& tmv16, const CUtensorMap& tmd16, const void* fold, int64_t fold_stride,
+                          int nmaps, const uint8_t* live, const MapOut& out, unsigned* flags, cudaStream_t s);
 // 2D tensor map over a (Nlm x Nx) table for the streaming contraction's TMA loads.
-int make_table_tmap(CUtensorMap* tm, const void* base, size_t elem_bytes, int Nx, int64_t Nlm);
+// 2D tensor map of a table (node x row) with boxes of 256 nodes x `rows` rows (0: the
+// single-map row count for the element size).
+int make_table_tmap(CUtensorMap* tm, const void* base, size_t elem_bytes, int Nx, int64_t Nlm, int rows = 0);
 void launch_tables_to_f32(const Geometry& g, const double* Yv, const double* Yd, float* Yv32, float* Yd32,
                           cudaStream_t s);
 void launch_rotate_back(const Geometry& g, const double* alm_rot, const double* alm_add,
@@ -176,6 +178,7 @@ struct dsht_plan_s {
   float* Yv32 = nullptr;  // FP32 copies streamed by mixed-precision executes (made on first use)
   float* Yd32 = nullptr;
   alignas(64) CUtensorMap tmYv, tmYd, tmYv32, tmYd32;
+  alignas(64) CUtensorMap tmYv32h, tmYd32h;  // FP32 tables, 16-row boxes (passes of 3-4 folds)
   bool tm64 = false, tm32 = false;
   // Plan-owned buffers, grown on demand (used when the caller passes no workspace and by
   // the host-pointer entry points).

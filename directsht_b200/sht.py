@@ -236,7 +236,7 @@ class DirectSHT:
         ``self(*point_sets[i])`` (or ``basic_sht`` with mode="basic").
 
         The reference has no batch call; its users loop ``__call__`` (``sht/sht.py:112-150``).
-        Here the contraction of up to three point sets shares one read of the tables and the
+        Here the contraction of up to four point sets shares one read of the tables and the
         rotation of up to eight shares one Wigner-d recursion.  Returns a list of complex128
         alm (numpy, or CUDA tensors when the inputs are CUDA tensors).  A transform whose polar
         points cannot be rotated into range gives zeros, as ``__call__`` does.

@@ -94,7 +94,7 @@ int dsht_get_precision(dsht_plan_t plan, int* precision);
 /* Launch-shape tuning of a plan (no counterpart in the reference; results do not depend on
  * it beyond rounding).  DSHT_TUNE_PIECE_MAX: points per bin piece of the per-bin sums, a
  * multiple of 32 in [256, 2048], 0 = chosen from N.  DSHT_TUNE_MAPS_PER_PASS: maps that
- * share one read of the tables in the multi-map contraction, 1..3, 0 = 3.  Workspace sizes
+ * share one read of the tables in the multi-map contraction, 1..4, 0 = 2.  Workspace sizes
  * depend on both: query them after tuning. */
 enum { DSHT_TUNE_PIECE_MAX = 1, DSHT_TUNE_MAPS_PER_PASS = 2 };
 int dsht_plan_tune(dsht_plan_t plan, int param, int value);
@@ -155,7 +155,7 @@ int dsht_status(unsigned flags, int mode);
  * users call DirectSHT.__call__ once per point set).  Transform i: N[i] points at the
  * DEVICE pointers theta[i], phi[i], w[i] (float64), alm to the DEVICE pointer alm[i]
  * (2*Nlm doubles); the pointer arrays themselves are HOST arrays read during the call.
- * Each point set is sorted on its own; the contraction serves up to 3 transforms per read
+ * Each point set is sorted on its own; the contraction serves up to 4 transforms per read
  * of the tables (DSHT_TUNE_MAPS_PER_PASS) and the rotation up to 8.  Results equal those of
  * one dsht_execute per transform.  The workspace (dsht_workspace_size_batch with the
  * largest N of the batch) is used in turn by every transform.  dsht_execute_batch
@@ -225,7 +225,7 @@ int dsht_do_transform(int Nl, int Nx, double xmax, double* Yv, double* Yd, int N
  * Stages: 0 points+sort, 1 bin sums, 2 fold, 3 contraction, 4 rotation.  For
  * dsht_execute_maps: stage 0 is the one sort, stages 1-2 are those of the last map
  * (stage 1 including its payload gather), stage 3 is the last contraction pass (it serves
- * up to 3 maps) and stage 4 the rotation of all maps. */
+ * up to 4 maps) and stage 4 the rotation of all maps. */
 enum { DSHT_STAGE_POINTS = 0, DSHT_STAGE_BIN_SUMS = 1, DSHT_STAGE_FOLD = 2, DSHT_STAGE_CONTRACT = 3,
        DSHT_STAGE_ROTATE = 4, DSHT_STAGE_COUNT = 5 };
 int dsht_profile_enable(dsht_plan_t plan, int enable);
