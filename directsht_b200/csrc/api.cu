@@ -81,7 +81,6 @@ size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* ba
   const bool maps = multi;
   if (maps) {
     w.sidx = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * n));
-    w.skey = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * n));
   }
   w.count = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * (g.nkeys + 1)));
   w.offset = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * (g.nkeys + 1)));
@@ -287,7 +286,6 @@ int run_items(dsht_plan_s* p, const Item* items, int n, int mode, const Workspac
         const bool shared = li + 1 < list.size() && items[list[li + 1]].same_points;
         if (!shared) {
           wp.sidx = nullptr;
-          wp.skey = nullptr;
         }
         launch_points(g, item.theta, item.phi, item.w, item.w_f32, item.N, mode, wp, s);
         sorted_item = i;

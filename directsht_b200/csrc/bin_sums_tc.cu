@@ -531,6 +531,7 @@ int tc_inner_factor(int Nl) {
 
 int launch_bin_sums_tc(const Geometry& g, const Workspace& ws, cudaStream_t s) {
   const int Cf = tc_inner_factor(g.Nl);
+  launch_piece_maxima(ws, s);
   switch (Cf) {
     case 8: return launch_ch<8>(g, ws, 8, s);
     case 16: return launch_ch<16>(g, ws, 16, s);

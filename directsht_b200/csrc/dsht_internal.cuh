@@ -69,7 +69,6 @@ struct Workspace {
   double* rec;          // [N][3]
   double* pay;          // [N][4] sorted records (cos phi, sin phi, w, t)
   uint32_t* sidx;       // [N] input index of each sorted slot (multi-map transforms)
-  uint32_t* skey;       // [N] key of each sorted slot
   uint32_t* piecemax;   // [pmax] largest |w h_k| of the piece's points (float bits)
   uint32_t* count;      // [nkeys + 1]
   uint32_t* offset;     // [nkeys + 1]
@@ -118,6 +117,8 @@ void launch_tables_f32(const Geometry& g, float* Yv, float* Yd, cudaStream_t s);
 void launch_points(const Geometry& g, const double* theta, const double* phi, const void* w, int w_f32,
                    int64_t N, int mode, const Workspace& ws, cudaStream_t s);
 void launch_gather(const Geometry& g, const void* w, int w_f32, int64_t N, const Workspace& ws, cudaStream_t s);
+// Largest |w h_k| of every piece of the sorted records (needed by the tensor-core sums).
+void launch_piece_maxima(const Workspace& ws, cudaStream_t s);
 void launch_publish_flags(const StatusOut& st, int n, unsigned* all, cudaStream_t s);
 void launch_bin_sums_fp64(const Geometry& g, const Workspace& ws, cudaStream_t s);
 int launch_bin_sums_tc(const Geometry& g, const Workspace& ws, cudaStream_t s);

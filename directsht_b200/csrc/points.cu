@@ -204,14 +204,11 @@ __device__ __forceinline__ uint32_t gmax_bits(const double* h) {
   return __float_as_uint((float)fmax(fmax(fabs(h[0]), fabs(h[1])), fmax(fabs(h[2]), fabs(h[3]))));
 }
 
-// The piece of a sorted slot is piece_first[k] + (pos - offset[k]) / piece_max; every
-// point raises its piece's maximum |w h_k| (the fixed-point scale of the tensor-core sums).
 template <typename WT>
 __global__ void __launch_bounds__(kPointThreads)
 scatter_kernel(Geometry g, const WT* __restrict__ w, int64_t N, const uint32_t* __restrict__ keys,
                const double* __restrict__ rec, uint32_t* __restrict__ cursor, double* __restrict__ pay,
-               const uint32_t* __restrict__ offset, const int* __restrict__ piece_first, int piece_max,
-               uint32_t* __restrict__ piecemax, uint32_t* __restrict__ sidx, uint32_t* __restrict__ skey) {
+               uint32_t* __restrict__ sidx) {
   extern __shared__ uint32_t loc[];  // [nkeys] local counts, then local bases
   const int64_t lo = (int64_t)blockIdx.x * kScatterTile;
   const int64_t hi = min(lo + (int64_t)kScatterTile, N);
@@ -236,34 +233,44 @@ scatter_kernel(Geometry g, const WT* __restrict__ w, int64_t N, const uint32_t* 
     double2* out = reinterpret_cast<double2*>(pay + (size_t)kRec * pos);  // one 32-byte sector
     out[0] = make_double2(rec[3 * i], rec[3 * i + 1]);
     out[1] = make_double2(wi, t);
-    double h[4];
-    hermite(t, wi, h);
-    atomicMax(&piecemax[piece_first[k] + (pos - offset[k]) / (uint32_t)piece_max], gmax_bits(h));
-    if (sidx) {
-      sidx[pos] = (uint32_t)i;
-      skey[pos] = k;
-    }
+    if (sidx) sidx[pos] = (uint32_t)i;
   }
 }
 
 // Another weight map on the same sorted points (multi-map transforms share the sort): the
-// record's w becomes w[sidx[pos]], and the piece maxima are rebuilt.
+// record's w becomes w[sidx[pos]].
 template <typename WT>
 __global__ void __launch_bounds__(kPointThreads)
 gather_kernel(int64_t N, const uint32_t* __restrict__ total, const uint32_t* __restrict__ sidx,
-              const uint32_t* __restrict__ skey, const WT* __restrict__ w, double* __restrict__ pay,
-              const uint32_t* __restrict__ offset, const int* __restrict__ piece_first, int piece_max,
-              uint32_t* __restrict__ piecemax) {
+              const WT* __restrict__ w, double* __restrict__ pay) {
   const int64_t n = (int64_t)*total;
   for (int64_t pos = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; pos < n && pos < N;
-       pos += (int64_t)gridDim.x * blockDim.x) {
-    double* r = pay + (size_t)kRec * pos;
-    const double wi = (double)w[sidx[pos]];
-    r[2] = wi;
-    double h[4];
-    hermite(r[3], wi, h);
-    const uint32_t k = skey[pos];
-    atomicMax(&piecemax[piece_first[k] + ((uint32_t)pos - offset[k]) / (uint32_t)piece_max], gmax_bits(h));
+       pos += (int64_t)gridDim.x * blockDim.x)
+    pay[(size_t)kRec * pos + 2] = (double)w[sidx[pos]];
+}
+
+// Largest |w h_k| of every piece (float bits; the fixed-point scale of the tensor-core
+// sums): one warp per piece reads its sorted records (w, t) in order.
+__global__ void __launch_bounds__(kPointThreads)
+piecemax_kernel(const double* __restrict__ pay, const int* __restrict__ npieces_p, int64_t pmax,
+                const int64_t* __restrict__ piece_start, const int* __restrict__ piece_len,
+                uint32_t* __restrict__ piecemax) {
+  const int lane = threadIdx.x & 31;
+  const int64_t np = min((int64_t)*npieces_p, pmax);
+  const int64_t wstride = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t pc = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); pc < np; pc += wstride) {
+    const int64_t st = piece_start[pc];
+    const int len = piece_len[pc];
+    uint32_t mx = 0;
+    for (int i = lane; i < len; i += 32) {
+      const double2 wt = reinterpret_cast<const double2*>(pay + (size_t)kRec * (st + i))[1];
+      double h[4];
+      hermite(wt.y, wt.x, h);
+      mx = max(mx, gmax_bits(h));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) piecemax[pc] = mx;
   }
 }
 
@@ -280,7 +287,6 @@ __global__ void publish_flags_kernel(const StatusOut st, int n, unsigned* all) {
 void launch_points(const Geometry& g, const double* theta, const double* phi, const void* w, int w_f32,
                    int64_t N, int mode, const Workspace& ws, cudaStream_t s) {
   cudaMemsetAsync(ws.count, 0, sizeof(uint32_t) * (g.nkeys + 1), s);
-  cudaMemsetAsync(ws.piecemax, 0, sizeof(uint32_t) * ws.pmax, s);
   cudaMemsetAsync(ws.flags, 0, sizeof(unsigned), s);
   const size_t hsmem = sizeof(uint32_t) * g.nkeys;
   cudaFuncSetAttribute(count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem);
@@ -299,9 +305,7 @@ void launch_points(const Geometry& g, const double* theta, const double* phi, co
     const int64_t blocks = (N + kScatterTile - 1) / kScatterTile;
     auto go = [&](auto kern, const auto* wp) {
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem);
-      kern<<<(unsigned)blocks, kPointThreads, hsmem, s>>>(g, wp, N, ws.key, ws.rec, ws.cursor, ws.pay, ws.offset,
-                                                          ws.piece_first, ws.piece_max, ws.piecemax, ws.sidx,
-                                                          ws.skey);
+      kern<<<(unsigned)blocks, kPointThreads, hsmem, s>>>(g, wp, N, ws.key, ws.rec, ws.cursor, ws.pay, ws.sidx);
     };
     if (w_f32) go(scatter_kernel<float>, reinterpret_cast<const float*>(w));
     else go(scatter_kernel<double>, reinterpret_cast<const double*>(w));
@@ -314,15 +318,21 @@ void launch_gather(const Geometry& g, const void* w, int w_f32, int64_t N, const
   int64_t blocks = (N + kPointThreads - 1) / kPointThreads;
   if (blocks > 148 * 16) blocks = 148 * 16;
   const uint32_t* total = ws.offset + g.nkeys;
-  cudaMemsetAsync(ws.piecemax, 0, sizeof(uint32_t) * ws.pmax, s);
   if (w_f32)
-    gather_kernel<float><<<(unsigned)blocks, kPointThreads, 0, s>>>(
-        N, total, ws.sidx, ws.skey, reinterpret_cast<const float*>(w), ws.pay, ws.offset, ws.piece_first,
-        ws.piece_max, ws.piecemax);
+    gather_kernel<float><<<(unsigned)blocks, kPointThreads, 0, s>>>(N, total, ws.sidx,
+                                                                    reinterpret_cast<const float*>(w), ws.pay);
   else
-    gather_kernel<double><<<(unsigned)blocks, kPointThreads, 0, s>>>(
-        N, total, ws.sidx, ws.skey, reinterpret_cast<const double*>(w), ws.pay, ws.offset, ws.piece_first,
-        ws.piece_max, ws.piecemax);
+    gather_kernel<double><<<(unsigned)blocks, kPointThreads, 0, s>>>(N, total, ws.sidx,
+                                                                     reinterpret_cast<const double*>(w), ws.pay);
+  count_launches(1);
+}
+
+void launch_piece_maxima(const Workspace& ws, cudaStream_t s) {
+  int64_t blocks = (ws.pmax + (kPointThreads / 32) - 1) / (kPointThreads / 32);
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  if (blocks < 1) blocks = 1;
+  piecemax_kernel<<<(unsigned)blocks, kPointThreads, 0, s>>>(ws.pay, ws.npieces, ws.pmax, ws.piece_start,
+                                                              ws.piece_len, ws.piecemax);
   count_launches(1);
 }
 
