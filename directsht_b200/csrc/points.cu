@@ -262,10 +262,24 @@ piecemax_kernel(const double* __restrict__ pay, const int* __restrict__ npieces_
     const int64_t st = piece_start[pc];
     const int len = piece_len[pc];
     uint32_t mx = 0;
-    for (int i = lane; i < len; i += 32) {
-      const double2 wt = reinterpret_cast<const double2*>(pay + (size_t)kRec * (st + i))[1];
+    const double2* base = reinterpret_cast<const double2*>(pay + (size_t)kRec * st) + 1;
+    int i = lane;
+    for (; i + 96 < len; i += 128) {  // four records in flight per lane
+      const double2 a = base[2 * i], b = base[2 * (i + 32)], c = base[2 * (i + 64)], d = base[2 * (i + 96)];
       double h[4];
-      hermite(wt.y, wt.x, h);
+      hermite(a.y, a.x, h);
+      mx = max(mx, gmax_bits(h));
+      hermite(b.y, b.x, h);
+      mx = max(mx, gmax_bits(h));
+      hermite(c.y, c.x, h);
+      mx = max(mx, gmax_bits(h));
+      hermite(d.y, d.x, h);
+      mx = max(mx, gmax_bits(h));
+    }
+    for (; i < len; i += 32) {
+      const double2 a = base[2 * i];
+      double h[4];
+      hermite(a.y, a.x, h);
       mx = max(mx, gmax_bits(h));
     }
 #pragma unroll
