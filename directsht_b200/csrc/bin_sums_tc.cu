@@ -15,9 +15,12 @@
 //
 // Operands: per point, FP64 anchors (powers of e^{i phi} by squaring and short
 // recurrences) stored as FP32; per value, X = rint(x q) with q = 2^22 - 2^10 by one FP32
-// FMA against 1.5*2^23, split into its bytes X = X0 2^16 + X1 2^8 + X2 (X0 signed,
-// X1, X2 unsigned).  Eight tcgen05.mma.kind::i8 per K step accumulate exactly in S32
-// TMEM: W0 = A0B0, W1 = A0B1 + A1B0, W2 = A0B2 + A1B1 + A2B0, W3 = A1B2 + A2B1, and
+// FMA against 1.5*2^23, written in balanced base-256 digits X = X0 2^16 + X1 2^8 + X2
+// with every digit a signed byte: the bytes of Z = (X + 0x8080) ^ 0x8080 (adding 128 to
+// the two low digit positions and flipping their top bits maps [0, 255] onto
+// [-128, 127]).  Five tcgen05.mma.kind::i8 per K step accumulate exactly in S32 TMEM:
+// W0 = A0B0, W1 = A0B1 + A1B0, W2 = A0B2 + A1B1 + A2B0, W3 = A1B2 + A2B1 (B0 and B1 form
+// one 2N-row operand, so A_i [B0|B1] adds to W_i and W_(i+1) in one instruction), and
 // D = (2^32 W0 + 2^24 W1 + 2^16 W2 + 2^8 W3) / q^2 in FP64.  Integer accumulation has no
 // rounding (FP32 tensor-core accumulation truncates and biases long sums), so the error
 // is the quantisation plus the dropped A2B2 term: about 5.6e-8 rms per product, relative
@@ -65,13 +68,19 @@ struct cplx {
 __device__ __forceinline__ cplx cmul(cplx a, cplx b) {
   return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
 }
-// rint(x q) of an FP64 value: one DFMA puts x q into the binade of 1.5*2^52, whose low
-// word is then the rounded integer (no conversion instruction).
-__device__ __forceinline__ int qfix(double x) { return __double2loint(fma(x, kQ, 6755399441055744.0)); }
+// Z = (rint(x q) + 0x8080) ^ 0x8080 of an FP64 value, whose bytes are the balanced
+// digits: one DFMA puts x q + 0x8080 into the binade of 1.5*2^52, whose low word is then
+// the rounded integer (no conversion instruction).
+__device__ __forceinline__ int zfix(double x) {
+  return __double2loint(fma(x, kQ, 6755399441055744.0 + 32896.0)) ^ 0x8080;
+}
 
-// rint(x q) for |x| <= 1: one FMA puts x q into the binade of 1.5*2^23, where the
-// float's bit pattern minus that of 1.5*2^23 is the rounded integer.
-__device__ __forceinline__ int quant(float x) { return __float_as_int(fmaf(x, kQf, kMagic)) - 0x4B400000; }
+// rint(x q) + 0x8080 for |x| <= 1: one FMA puts x q into the binade of 1.5*2^23, where
+// the float's bit pattern minus that of 1.5*2^23 is the rounded integer.  The flip of the
+// two low digits' top bits is applied to the packed slice words.
+__device__ __forceinline__ int quant(float x) {
+  return __float_as_int(fmaf(x, kQf, kMagic)) - (0x4B400000 - 0x8080);
+}
 
 // Byte B of a, b, c, d packed into one word (the slices of X are its bytes 2, 1, 0).
 template <int B>
@@ -114,8 +123,9 @@ __device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t adesc, uint64_t
 // writes the four fixed-point values of point pp into X[0..3]; they are byte-transposed
 // into the three slice tiles (slice s of four points is byte 2 - s of X) and stored as
 // 16-byte chunks of the 64-byte swizzled K-major rows (chunk h XOR (row / 2) & 3).  A
-// quarter warp's first stores land in four distinct 16-byte bank groups.
-template <typename F>
+// quarter warp's first stores land in four distinct 16-byte bank groups.  kFlip: X is
+// X + 0x8080 and the low slices' top bits are flipped here (else X is Z already).
+template <bool kFlip, typename F>
 __device__ __forceinline__ void slice_unit(uint8_t* base, int tile_bytes, int h, const int* rows, F values) {
   uint32_t w[4][3][4];  // [value][slice][word of 4 points]
 #pragma unroll
@@ -130,8 +140,8 @@ __device__ __forceinline__ void slice_unit(uint8_t* base, int tile_bytes, int h,
       const uint32_t u0 = __byte_perm((uint32_t)X[2][e], (uint32_t)X[3][e], 0x5140);
       const uint32_t u1 = __byte_perm((uint32_t)X[2][e], (uint32_t)X[3][e], 0x7362);
       w[e][0][t] = __byte_perm(t1, u1, 0x5410);
-      w[e][1][t] = __byte_perm(t0, u0, 0x7632);
-      w[e][2][t] = __byte_perm(t0, u0, 0x5410);
+      w[e][1][t] = __byte_perm(t0, u0, 0x7632) ^ (kFlip ? 0x80808080u : 0u);
+      w[e][2][t] = __byte_perm(t0, u0, 0x5410) ^ (kFlip ? 0x80808080u : 0u);
     }
   }
 #pragma unroll
@@ -288,8 +298,8 @@ bin_sums_tc_kernel(int Nl, int Cf, const double* __restrict__ pay, const int* __
             if (u < H) {
               // c = 2u, 2u + 1 and CH/2 + 2u, CH/2 + 2u + 1, straight to fixed point
               const cplx a1 = cmul(ea0, z1), b1 = cmul(eb0, z1);
-              eb[u] = make_int4(qfix(ea0.re), qfix(ea0.im), qfix(a1.re), qfix(a1.im));
-              eb[H + u] = make_int4(qfix(eb0.re), qfix(eb0.im), qfix(b1.re), qfix(b1.im));
+              eb[u] = make_int4(zfix(ea0.re), zfix(ea0.im), zfix(a1.re), zfix(a1.im));
+              eb[H + u] = make_int4(zfix(eb0.re), zfix(eb0.im), zfix(b1.re), zfix(b1.im));
               ea0 = cmul(ea0, st);
               eb0 = cmul(eb0, st);
             }
@@ -344,7 +354,7 @@ bin_sums_tc_kernel(int Nl, int Cf, const double* __restrict__ pay, const int* __
           if (tid < nB) {
             const int h = tid / (CH / 2), cp = tid % (CH / 2);
             const int rows[4] = {2 * cp, CH + 2 * cp, 2 * cp + 1, CH + 2 * cp + 1};  // Re/Im of c, c+1
-            slice_unit(st_base + 3 * Lay::kTileA, Lay::kTileB, h, rows, [&](int pp, int* X) {
+            slice_unit<false>(st_base + 3 * Lay::kTileA, Lay::kTileB, h, rows, [&](int pp, int* X) {
               const int4 q = eb[pp * (kEbStride / 2) + cp];  // already fixed point
               X[0] = q.x;
               X[1] = q.y;
@@ -359,7 +369,7 @@ bin_sums_tc_kernel(int Nl, int Cf, const double* __restrict__ pay, const int* __
             const int h = v >> 5, k = (v & 31) >> 3, ap = v & 7;
             const int j0 = 16 * k + ap;
             const int rows[4] = {2 * j0, 2 * j0 + 1, 2 * j0 + 16, 2 * j0 + 17};
-            slice_unit(st_base, Lay::kTileA, h, rows, [&](int pp, int* X) {
+            slice_unit<true>(st_base, Lay::kTileA, h, rows, [&](int pp, int* X) {
               const float gg = gk[pp * 4 + k];
               const float2 z0 = ea[pp * kEaStride + ap];
               const float2 z1 = ea[pp * kEaStride + ap + 8];
@@ -433,8 +443,8 @@ bin_sums_tc_kernel(int Nl, int Cf, const double* __restrict__ pay, const int* __
     }
   } else if (warp == kSlicerWarps + kAnchorWarps) {
     // ==== MMA issuer (one thread) ======================================================
-    constexpr uint32_t iSS = idesc_i8(kM, N, true, true), iSU = idesc_i8(kM, N, true, false),
-                       iUS = idesc_i8(kM, N, false, true), iUU = idesc_i8(kM, N, false, false);
+    constexpr uint32_t i1 = idesc_i8(kM, N, true, true), i2 = idesc_i8(kM, 2 * N, true, true);
+    static_assert(2 * N <= 256, "B0|B1 must be one MMA operand");
     if (lane == 0) {
       uint32_t g = 0, piece_iter = 0;
       for (int piece = blockIdx.x; piece < npieces; piece += gridDim.x, ++piece_iter) {
@@ -467,19 +477,17 @@ bin_sums_tc_kernel(int Nl, int Cf, const double* __restrict__ pay, const int* __
             for (int kk = 0; kk < kBK / 32; ++kk) {
               const uint32_t off = kk * 32;  // 32 int8 along K
               const bool acc = (b > 0) || (kk > 0);
-              const uint32_t W0 = tmem, W1 = tmem + N, W2 = tmem + 2 * N, W3 = tmem + 3 * N;
               const uint64_t a0 = desc_k_sw64(A[0] + off), a1 = desc_k_sw64(A[1] + off),
                              a2 = desc_k_sw64(A[2] + off);
-              const uint64_t b0 = desc_k_sw64(B[0] + off), b1 = desc_k_sw64(B[1] + off),
-                             b2 = desc_k_sw64(B[2] + off);
-              mma_i8(W0, a0, b0, iSS, acc);
-              mma_i8(W1, a0, b1, iSU, acc);
-              mma_i8(W1, a1, b0, iUS, true);
-              mma_i8(W2, a0, b2, iSU, acc);
-              mma_i8(W2, a1, b1, iUU, true);
-              mma_i8(W2, a2, b0, iUS, true);
-              mma_i8(W3, a1, b2, iUU, acc);
-              mma_i8(W3, a2, b1, iUU, true);
+              const uint64_t b01 = desc_k_sw64(B[0] + off), b2 = desc_k_sw64(B[2] + off);
+              // B0 and B1 are consecutive tiles, one 2N-row operand: A_i [B0|B1] lands on
+              // W_i, W_(i+1) (columns iN .. (i+2)N).  W2, W3 are started by the B2
+              // products, W0 and W1 by A0 [B0|B1].
+              mma_i8(tmem + 2 * N, a0, b2, i1, acc);
+              mma_i8(tmem + 3 * N, a1, b2, i1, acc);
+              mma_i8(tmem, a0, b01, i2, acc);
+              mma_i8(tmem + N, a1, b01, i2, true);
+              mma_i8(tmem + 2 * N, a2, b01, i2, true);
             }
           }
           tc::mma_commit(&empty[stage]);

@@ -28,9 +28,11 @@ struct PointOut {
   unsigned flag;
 };
 
-// kAngles: also compute cos/sin of the azimuth (the count pass only needs the key).
-template <bool kAngles>
-__device__ __forceinline__ PointOut classify(const Geometry& g, int mode, double th, double ph) {
+// sp, cp: sin and cos of the azimuth (both sets need them: computed once, before the
+// branch, so that a warp with polar points does not evaluate them twice); inv_dx = 1/dx
+// gives the bin guess that the exact comparisons below correct.
+__device__ __forceinline__ PointOut classify(const Geometry& g, double inv_dx, int mode, double th, double sp,
+                                             double cp) {
   PointOut o;
   o.flag = 0;
   o.key = DSHT_KEY_DROP;
@@ -44,8 +46,6 @@ __device__ __forceinline__ PointOut classify(const Geometry& g, int mode, double
     const double xv = fabs(c);
     if (xv >= g.xmax) {
       // Rotate n = (s cos p, s sin p, c) to (c, s sin p, -s cos p).
-      double sp, cp;
-      sincos(ph, &sp, &cp);
       const double st = sin(th);
       const double nx = st * cp, ny = st * sp;
       const double xr = -nx;
@@ -70,7 +70,8 @@ __device__ __forceinline__ PointOut classify(const Geometry& g, int mode, double
       }
       x = c;
       set = 0;
-      if (kAngles) sincos(ph, &o.sphi, &o.cphi);
+      o.cphi = cp;
+      o.sphi = sp;
     } else {
       return o;  // NaN theta: in neither set (sht/sht.py:129-130)
     }
@@ -81,12 +82,13 @@ __device__ __forceinline__ PointOut classify(const Geometry& g, int mode, double
     }
     x = c;
     set = 0;
-    if (kAngles) sincos(ph, &o.sphi, &o.cphi);
+    o.cphi = cp;
+    o.sphi = sp;
   }
   if (!(x >= 0.0)) set += 1;          // x < 0 half (sht/sht.py:193)
   const double ax = fabs(x);
   // digitize: x_j <= ax < x_{j+1} with x_j = j * dx exactly as numpy builds the grid.
-  int j = (int)(ax / g.dx);
+  int j = (int)(ax * inv_dx);
   if (j > g.nbins - 1) j = g.nbins - 1;
   if (j < 0) j = 0;
   if (ax < (double)j * g.dx) j -= 1;
@@ -108,9 +110,12 @@ count_kernel(Geometry g, int mode, const double* __restrict__ theta, const doubl
   for (int k = threadIdx.x; k < g.nkeys; k += blockDim.x) hist[k] = 0;
   __syncthreads();
   unsigned fl = 0;
+  const double inv_dx = 1.0 / g.dx;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
-    PointOut o = classify<true>(g, mode, theta[i], phi[i]);
+    double sp, cp;
+    sincos(phi[i], &sp, &cp);
+    PointOut o = classify(g, inv_dx, mode, theta[i], sp, cp);
     keys[i] = o.key;
     rec[3 * i] = o.cphi;
     rec[3 * i + 1] = o.sphi;
@@ -214,9 +219,20 @@ scatter_kernel(Geometry g, const WT* __restrict__ w, int64_t N, const uint32_t* 
   const int64_t hi = min(lo + (int64_t)kScatterTile, N);
   for (int k = threadIdx.x; k < g.nkeys; k += blockDim.x) loc[k] = 0;
   __syncthreads();
-  for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-    const uint32_t k = keys[i];
-    if (k != DSHT_KEY_DROP) atomicAdd(&loc[k], 1u);
+  // kUnroll points per thread and step: their loads are issued together, so each thread
+  // keeps several DRAM reads in flight (one point at a time leaves the pass latency bound).
+  constexpr int kUnroll = 8;
+  const int64_t step = (int64_t)kUnroll * blockDim.x;
+  for (int64_t b = lo + threadIdx.x; b < hi; b += step) {
+    uint32_t k[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      const int64_t i = b + (int64_t)u * blockDim.x;
+      k[u] = (i < hi) ? keys[i] : DSHT_KEY_DROP;
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u)
+      if (k[u] != DSHT_KEY_DROP) atomicAdd(&loc[k[u]], 1u);
   }
   __syncthreads();
   for (int k = threadIdx.x; k < g.nkeys; k += blockDim.x) {
@@ -224,16 +240,30 @@ scatter_kernel(Geometry g, const WT* __restrict__ w, int64_t N, const uint32_t* 
     if (c) loc[k] = atomicAdd(&cursor[k], c);
   }
   __syncthreads();
-  for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-    const uint32_t k = keys[i];
-    if (k == DSHT_KEY_DROP) continue;
-    const uint32_t pos = atomicAdd(&loc[k], 1u);
-    const double t = rec[3 * i + 2];
-    const double wi = (double)w[i];
-    double2* out = reinterpret_cast<double2*>(pay + (size_t)kRec * pos);  // one 32-byte sector
-    out[0] = make_double2(rec[3 * i], rec[3 * i + 1]);
-    out[1] = make_double2(wi, t);
-    if (sidx) sidx[pos] = (uint32_t)i;
+  for (int64_t b = lo + threadIdx.x; b < hi; b += step) {
+    uint32_t k[kUnroll];
+    double c[kUnroll], sn[kUnroll], t[kUnroll], wi[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      const int64_t i = b + (int64_t)u * blockDim.x;
+      k[u] = DSHT_KEY_DROP;
+      if (i < hi) {
+        k[u] = keys[i];
+        c[u] = rec[3 * i];
+        sn[u] = rec[3 * i + 1];
+        t[u] = rec[3 * i + 2];
+        wi[u] = (double)w[i];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      if (k[u] == DSHT_KEY_DROP) continue;
+      const uint32_t pos = atomicAdd(&loc[k[u]], 1u);
+      double2* out = reinterpret_cast<double2*>(pay + (size_t)kRec * pos);  // one 32-byte sector
+      out[0] = make_double2(c[u], sn[u]);
+      out[1] = make_double2(wi[u], t[u]);
+      if (sidx) sidx[pos] = (uint32_t)(b + (int64_t)u * blockDim.x);
+    }
   }
 }
 
