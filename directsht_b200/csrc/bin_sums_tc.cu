@@ -237,10 +237,13 @@ bin_sums_tc_kernel(int Nl, int Cf, const double* __restrict__ pay, const int* __
 
   if (warp >= kSlicerWarps && warp < kSlicerWarps + kAnchorWarps) {
     // ==== anchor warps: FP64 powers of e^{i phi} (FP32 storage) one block ahead ========
-    // Thread p: point p of the block.  It runs four interleaved recurrences (FP64 latency
-    // overlaps): the two halves of ec, e^{i (cbase + 2u) phi}, and of ea, e^{i Cf a phi};
-    // all starting powers are powers of two of e^{i phi}.  Then e1 and the Hermite weights
-    // g_k / scale.  The record of the point in the next block is loaded meanwhile.
+    // Thread p: point p of the block.  The powers come from Chebyshev recurrences
+    // E_(c+d) = 2 cos(d phi) E_c - E_(c-d) (one DFMA per component and value): four
+    // interleaved chains of step 2 give e^{i c phi} for c = cbase + {2u, 2u + 1, CH/2 + 2u,
+    // CH/2 + 2u + 1}, one chain of step Cf gives e^{i Cf a phi}; their seeds are products
+    // of powers of two of e^{i phi}.  FP64 throughout (the recurrences lose about
+    // steps^2 ulp, far below the 2^-22 fixed-point step).  Then the Hermite weights
+    // g_k / scale.  The records of the point in the next two blocks are loaded meanwhile.
     const int p = tid - kSlicers;
     uint32_t g = 0;
     for (int piece = blockIdx.x; piece < npieces && !*abort_flag; piece += gridDim.x) {
@@ -278,36 +281,47 @@ bin_sums_tc_kernel(int Nl, int Cf, const double* __restrict__ pay, const int* __
         int4* eb = reinterpret_cast<int4*>(eb_of(buf) + p * kEbStride);  // pairs of c
         float2* ea = ea_of(buf);
         float* gk = gk_of(buf);
-        constexpr int H = CH / 4;  // c pairs per chain
-        constexpr int L = H > 8 ? H : 8;
+        constexpr int H = CH / 4;  // c pairs per half of the c range
+        constexpr int L = H > 16 ? H : 16;
         if (b * kBK + p < len) {
           cplx zq = z1;
 #pragma unroll
           for (int q = 1; q < CH / 4; q <<= 1) zq = cmul(zq, zq);  // z^(CH/4)
           const cplx zh = cmul(zq, zq);                              // z^(CH/2)
           const cplx zf = cmul(zh, zh);                              // z^CH
-          const cplx st = cmul(z1, z1);
-          cplx ea0 = cbase ? zf : cplx{1.0, 0.0};                    // z^cbase
-          cplx eb0 = cmul(ea0, zh);                                  // z^(cbase + CH/2)
+          const cplx z2 = cmul(z1, z1);
+          const cplx zb = cbase ? zf : cplx{1.0, 0.0};               // z^cbase
+          const cplx zbh = cmul(zb, zh);                             // z^(cbase + CH/2)
           const cplx sc = (Cf == CH) ? zf : cmul(zf, zf);           // z^Cf, Cf in {CH, 2 CH}
-          const cplx s2 = cmul(sc, sc), s4 = cmul(s2, s2);
-          cplx aa = {1.0, 0.0};
-          cplx ab = cmul(s4, s4);                                    // z^(8 Cf)
+          // chains: P = z^(cbase + 2u), Q = P z, R = z^(cbase + CH/2 + 2u), S = R z, and
+          // the previous value of each (u - 1); A = z^(Cf a) with its predecessor.
+          cplx P = zb, Q = cbase ? cmul(zb, z1) : z1, R = zbh, S = cmul(zbh, z1);
+          cplx Pp = cbase ? cmul(zb, cplx{z2.re, -z2.im}) : cplx{z2.re, -z2.im};  // z^(cbase - 2)
+          cplx Qp = cbase ? cmul(zb, cplx{z1.re, -z1.im}) : cplx{z1.re, -z1.im};  // z^(cbase - 1)
+          cplx Rp = cmul(zbh, cplx{z2.re, -z2.im});
+          cplx Sp = cmul(zbh, cplx{z1.re, -z1.im});
+          const double m2 = 2.0 * z2.re;                             // 2 cos 2 phi
+          const double mf = 2.0 * sc.re;                             // 2 cos Cf phi
+          cplx Aa = {1.0, 0.0}, Ap = {sc.re, -sc.im};                // z^0, z^-Cf
 #pragma unroll
           for (int u = 0; u < L; ++u) {
             if (u < H) {
-              // c = 2u, 2u + 1 and CH/2 + 2u, CH/2 + 2u + 1, straight to fixed point
-              const cplx a1 = cmul(ea0, z1), b1 = cmul(eb0, z1);
-              eb[u] = make_int4(zfix(ea0.re), zfix(ea0.im), zfix(a1.re), zfix(a1.im));
-              eb[H + u] = make_int4(zfix(eb0.re), zfix(eb0.im), zfix(b1.re), zfix(b1.im));
-              ea0 = cmul(ea0, st);
-              eb0 = cmul(eb0, st);
+              eb[u] = make_int4(zfix(P.re), zfix(P.im), zfix(Q.re), zfix(Q.im));
+              eb[H + u] = make_int4(zfix(R.re), zfix(R.im), zfix(S.re), zfix(S.im));
+              if (u + 1 < H) {
+                const cplx Pn = {fma(m2, P.re, -Pp.re), fma(m2, P.im, -Pp.im)};
+                const cplx Qn = {fma(m2, Q.re, -Qp.re), fma(m2, Q.im, -Qp.im)};
+                const cplx Rn = {fma(m2, R.re, -Rp.re), fma(m2, R.im, -Rp.im)};
+                const cplx Sn = {fma(m2, S.re, -Sp.re), fma(m2, S.im, -Sp.im)};
+                Pp = P; Qp = Q; Rp = R; Sp = S;
+                P = Pn; Q = Qn; R = Rn; S = Sn;
+              }
             }
-            if (u < 8) {
-              ea[p * kEaStride + u] = make_float2((float)aa.re, (float)aa.im);
-              ea[p * kEaStride + 8 + u] = make_float2((float)ab.re, (float)ab.im);
-              aa = cmul(aa, sc);
-              ab = cmul(ab, sc);
+            if (u < 16) {
+              ea[p * kEaStride + u] = make_float2((float)Aa.re, (float)Aa.im);
+              const cplx An = {fma(mf, Aa.re, -Ap.re), fma(mf, Aa.im, -Ap.im)};
+              Ap = Aa;
+              Aa = An;
             }
           }
           double h[4];
