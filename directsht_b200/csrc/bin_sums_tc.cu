@@ -306,8 +306,12 @@ bin_sums_tc_kernel(int Nl, int Cf, const double* __restrict__ pay, const int* __
 #pragma unroll
           for (int u = 0; u < L; ++u) {
             if (u < H) {
-              eb[u] = make_int4(zfix(P.re), zfix(P.im), zfix(Q.re), zfix(Q.im));
-              eb[H + u] = make_int4(zfix(R.re), zfix(R.im), zfix(S.re), zfix(S.im));
+              // pair v = (c, c + 1) with c = 2v; pairs with bit 2 of v set are stored as
+              // (c + 1, c) (see the slicers' row order)
+              const int4 pq = make_int4(zfix(P.re), zfix(P.im), zfix(Q.re), zfix(Q.im));
+              const int4 rs = make_int4(zfix(R.re), zfix(R.im), zfix(S.re), zfix(S.im));
+              eb[u] = ((u >> 2) & 1) ? make_int4(pq.z, pq.w, pq.x, pq.y) : pq;
+              eb[H + u] = (((H + u) >> 2) & 1) ? make_int4(rs.z, rs.w, rs.x, rs.y) : rs;
               if (u + 1 < H) {
                 const cplx Pn = {fma(m2, P.re, -Pp.re), fma(m2, P.im, -Pp.im)};
                 const cplx Qn = {fma(m2, Q.re, -Qp.re), fma(m2, Q.im, -Qp.im)};
@@ -318,7 +322,9 @@ bin_sums_tc_kernel(int Nl, int Cf, const double* __restrict__ pay, const int* __
               }
             }
             if (u < 16) {
-              ea[p * kEaStride + u] = make_float2((float)Aa.re, (float)Aa.im);
+              // a with bit 2 set: stored as (im, re) (see the slicers' row order)
+              ea[p * kEaStride + u] = ((u >> 2) & 1) ? make_float2((float)Aa.im, (float)Aa.re)
+                                                     : make_float2((float)Aa.re, (float)Aa.im);
               const cplx An = {fma(mf, Aa.re, -Ap.re), fma(mf, Aa.im, -Ap.im)};
               Ap = Aa;
               Aa = An;
@@ -367,7 +373,11 @@ bin_sums_tc_kernel(int Nl, int Cf, const double* __restrict__ pay, const int* __
           // One unit per thread; the B and A units are separate straight-line paths.
           if (tid < nB) {
             const int h = tid / (CH / 2), cp = tid % (CH / 2);
-            const int rows[4] = {2 * cp, CH + 2 * cp, 2 * cp + 1, CH + 2 * cp + 1};  // Re/Im of c, c+1
+            // Re/Im of c = 2 cp and c + 1 (rows c and CH + c).  Lanes with bit 2 of cp set
+            // hold the pair as (c + 1, c), so a quarter warp's stores cover both rows of a
+            // 128-byte line and all four swizzle chunks: no bank conflicts.
+            const bool sw = (cp >> 2) & 1;
+            const int rows[4] = {2 * cp + sw, CH + 2 * cp + sw, 2 * cp + 1 - sw, CH + 2 * cp + 1 - sw};
             slice_unit<false>(st_base + 3 * Lay::kTileA, Lay::kTileB, h, rows, [&](int pp, int* X) {
               const int4 q = eb[pp * (kEbStride / 2) + cp];  // already fixed point
               X[0] = q.x;
@@ -382,7 +392,10 @@ bin_sums_tc_kernel(int Nl, int Cf, const double* __restrict__ pay, const int* __
             const int v = tid - nB;
             const int h = v >> 5, k = (v & 31) >> 3, ap = v & 7;
             const int j0 = 16 * k + ap;
-            const int rows[4] = {2 * j0, 2 * j0 + 1, 2 * j0 + 16, 2 * j0 + 17};
+            // lanes with bit 2 of ap set read (im, re) pairs and store rows (im, re): no
+            // bank conflicts (as for the B units)
+            const int sw = (ap >> 2) & 1;
+            const int rows[4] = {2 * j0 + sw, 2 * j0 + 1 - sw, 2 * j0 + 16 + sw, 2 * j0 + 17 - sw};
             slice_unit<true>(st_base, Lay::kTileA, h, rows, [&](int pp, int* X) {
               const float gg = gk[pp * 4 + k];
               const float2 z0 = ea[pp * kEaStride + ap];
@@ -426,6 +439,7 @@ bin_sums_tc_kernel(int Nl, int Cf, const double* __restrict__ pay, const int* __
         // the re/im combination is done in int64 too and each output needs one conversion
         // (through the bit pattern of 1.5 2^52: no conversion-pipe instruction).
         const double fs = f * 256.0;
+        const bool vec_out = (Nl & 3) == 0;
         for (int cb = 0; cb < CH; cb += 8) {
           long long T[2][8];
 #pragma unroll
@@ -442,12 +456,22 @@ bin_sums_tc_kernel(int Nl, int Cf, const double* __restrict__ pay, const int* __
                                     ((long long)(int)w[2][i] << 8) + (long long)(int)w[3][i]
                               : 0ll;
           }
+          float o8[8];
 #pragma unroll
           for (int i = 0; i < 8; ++i) {
             const long long x = __shfl_xor_sync(0xffffffffu, T[1][i], 1);
             const long long v = ri ? x + T[0][i] : T[0][i] - x;
             const double dv = __longlong_as_double(v + 0x4338000000000000ll) - 6755399441055744.0;
-            if (m0 + cb + i < Nl) out[m0 + cb + i] = (float)(dv * fs);
+            o8[i] = (float)(dv * fs);
+          }
+          if (vec_out && m0 + cb + 8 <= Nl) {  // 16-byte aligned: Nl % 4 == 0, m0 + cb % 8 == 0
+            float4* o4 = reinterpret_cast<float4*>(out + m0 + cb);
+            o4[0] = make_float4(o8[0], o8[1], o8[2], o8[3]);
+            o4[1] = make_float4(o8[4], o8[5], o8[6], o8[7]);
+          } else {
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+              if (m0 + cb + i < Nl) out[m0 + cb + i] = o8[i];
           }
         }
         tc::tc_fence_before();
