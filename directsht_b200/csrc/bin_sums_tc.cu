@@ -27,13 +27,19 @@
 // to the piece's largest |L|, mean below 1e-9.  Pieces of up to 2048 points keep every
 // S32 sum below 2^31.
 //
-// Warp roles: warps 8-9 compute the FP64 anchors of a block into one of two anchor
-// buffers, one block ahead; warps 0-7 quantise and slice them into a 3-stage ring of
-// 64-byte-swizzled K-major int8 tiles; warp 10 issues the MMAs from one thread; warps 0-3
-// run each piece's epilogue (TMEM lanes 0-127) while warps 4-7 and the anchor warps start
-// the next piece.  Hand-overs are mbarriers (afull/aempty: anchors <-> slicers, full/empty:
+// Warp roles: warps 6-9 (one per SM sub-partition) compute the FP64 anchors of a block
+// into one of two anchor buffers, one block ahead, two threads per point; warps 0-5
+// quantise and slice them into a ring of 64-byte-swizzled K-major int8 tiles (warps 0-1
+// the B tiles, 2-5 the A tiles); warp 10 issues the MMAs from one thread; warps 0-3 run
+// each piece's epilogue (TMEM lanes 0-127) while warps 4-5 and the anchor warps start the
+// next piece.  Hand-overs are mbarriers (afull/aempty: anchors <-> slicers, full/empty:
 // slicers <-> MMA via tcgen05.commit, done: MMA -> epilogue, tfree: epilogue -> MMA).
 // Every wait is bounded.
+//
+// FP64 is the limiting pipe: while int8 MMAs run, an SM sub-partition issues about one
+// FP64 warp instruction in 16 clocks (one in 2 on an SM that has not used its tensor
+// cores, about one in 5 after), while FP32 keeps its full rate.  So the FP64 work is
+// spread over all four sub-partitions and kept to recurrences of one DFMA per value.
 #include "dsht_internal.cuh"
 #include "tc_ptx.cuh"
 
@@ -41,8 +47,9 @@ namespace dsht {
 namespace {
 
 constexpr int kBK = 64;                 // points per stage: one 64-byte row of int8
-constexpr int kSlicerWarps = 8;         // warps 0-7: int8 slice tiles (0-3: epilogue too)
-constexpr int kAnchorWarps = 2;         // warps 8-9: FP64 anchors, one block ahead
+constexpr int kSlicerWarps = 6;         // warps 0-5: int8 slice tiles (0-3: epilogue too)
+constexpr int kAnchorWarps = 4;         // warps 6-9: FP64 anchors, one block ahead
+constexpr int kBThreads = 64;           // slicer threads 0-63: B tiles, 64-191: A tiles
 constexpr int kSlicers = 32 * kSlicerWarps;
 constexpr int kThreads = 32 * (kSlicerWarps + kAnchorWarps + 1);  // + warp 10: MMA issuer
 constexpr int kM = 128;
@@ -237,14 +244,17 @@ bin_sums_tc_kernel(int Nl, int Cf, const double* __restrict__ pay, const int* __
 
   if (warp >= kSlicerWarps && warp < kSlicerWarps + kAnchorWarps) {
     // ==== anchor warps: FP64 powers of e^{i phi} (FP32 storage) one block ahead ========
-    // Thread p: point p of the block.  The powers come from Chebyshev recurrences
+    // Two threads per point p of the block, one warp per SM sub-partition (FP64 is the
+    // scarce pipe while the MMAs run): half 0 the c chains below CH/2 and the Hermite
+    // weights, half 1 the c chains from CH/2 and e^{i Cf a phi}.  The powers come from
+    // Chebyshev recurrences
     // E_(c+d) = 2 cos(d phi) E_c - E_(c-d) (one DFMA per component and value): four
     // interleaved chains of step 2 give e^{i c phi} for c = cbase + {2u, 2u + 1, CH/2 + 2u,
     // CH/2 + 2u + 1}, one chain of step Cf gives e^{i Cf a phi}; their seeds are products
     // of powers of two of e^{i phi}.  FP64 throughout (the recurrences lose about
     // steps^2 ulp, far below the 2^-22 fixed-point step).  Then the Hermite weights
     // g_k / scale.  The records of the point in the next two blocks are loaded meanwhile.
-    const int p = tid - kSlicers;
+    const int p = (tid - kSlicers) & 63, half = (tid - kSlicers) >> 6;
     uint32_t g = 0;
     for (int piece = blockIdx.x; piece < npieces && !*abort_flag; piece += gridDim.x) {
       const int64_t start = piece_start[piece];
@@ -282,46 +292,44 @@ bin_sums_tc_kernel(int Nl, int Cf, const double* __restrict__ pay, const int* __
         float2* ea = ea_of(buf);
         float* gk = gk_of(buf);
         constexpr int H = CH / 4;  // c pairs per half of the c range
-        constexpr int L = H > 16 ? H : 16;
         if (b * kBK + p < len) {
           cplx zq = z1;
 #pragma unroll
           for (int q = 1; q < CH / 4; q <<= 1) zq = cmul(zq, zq);  // z^(CH/4)
           const cplx zh = cmul(zq, zq);                              // z^(CH/2)
-          const cplx zf = cmul(zh, zh);                              // z^CH
+          const cplx zf = (cbase || half) ? cmul(zh, zh) : cplx{0.0, 0.0};  // z^CH
           const cplx z2 = cmul(z1, z1);
           const cplx zb = cbase ? zf : cplx{1.0, 0.0};               // z^cbase
-          const cplx zbh = cmul(zb, zh);                             // z^(cbase + CH/2)
-          const cplx sc = (Cf == CH) ? zf : cmul(zf, zf);           // z^Cf, Cf in {CH, 2 CH}
-          // chains: P = z^(cbase + 2u), Q = P z, R = z^(cbase + CH/2 + 2u), S = R z, and
-          // the previous value of each (u - 1); A = z^(Cf a) with its predecessor.
-          cplx P = zb, Q = cbase ? cmul(zb, z1) : z1, R = zbh, S = cmul(zbh, z1);
-          cplx Pp = cbase ? cmul(zb, cplx{z2.re, -z2.im}) : cplx{z2.re, -z2.im};  // z^(cbase - 2)
-          cplx Qp = cbase ? cmul(zb, cplx{z1.re, -z1.im}) : cplx{z1.re, -z1.im};  // z^(cbase - 1)
-          cplx Rp = cmul(zbh, cplx{z2.re, -z2.im});
-          cplx Sp = cmul(zbh, cplx{z1.re, -z1.im});
           const double m2 = 2.0 * z2.re;                             // 2 cos 2 phi
-          const double mf = 2.0 * sc.re;                             // 2 cos Cf phi
-          cplx Aa = {1.0, 0.0}, Ap = {sc.re, -sc.im};                // z^0, z^-Cf
+          // chains: P = z^(c0 + 2u) and Q = P z with the previous value of each (u - 1);
+          // c0 = cbase (half 0) or cbase + CH/2 (half 1)
+          const cplx P0 = half ? cmul(zb, zh) : zb;
+          cplx P = P0, Q = cmul(P0, z1);
+          cplx Pp = cmul(P0, cplx{z2.re, -z2.im});                   // z^(c0 - 2)
+          cplx Qp = cmul(P0, cplx{z1.re, -z1.im});                   // z^(c0 - 1)
+          int4* ebh = eb + half * H;
 #pragma unroll
-          for (int u = 0; u < L; ++u) {
-            if (u < H) {
-              // pair v = (c, c + 1) with c = 2v; pairs with bit 2 of v set are stored as
-              // (c + 1, c) (see the slicers' row order)
-              const int4 pq = make_int4(zfix(P.re), zfix(P.im), zfix(Q.re), zfix(Q.im));
-              const int4 rs = make_int4(zfix(R.re), zfix(R.im), zfix(S.re), zfix(S.im));
-              eb[u] = ((u >> 2) & 1) ? make_int4(pq.z, pq.w, pq.x, pq.y) : pq;
-              eb[H + u] = (((H + u) >> 2) & 1) ? make_int4(rs.z, rs.w, rs.x, rs.y) : rs;
-              if (u + 1 < H) {
-                const cplx Pn = {fma(m2, P.re, -Pp.re), fma(m2, P.im, -Pp.im)};
-                const cplx Qn = {fma(m2, Q.re, -Qp.re), fma(m2, Q.im, -Qp.im)};
-                const cplx Rn = {fma(m2, R.re, -Rp.re), fma(m2, R.im, -Rp.im)};
-                const cplx Sn = {fma(m2, S.re, -Sp.re), fma(m2, S.im, -Sp.im)};
-                Pp = P; Qp = Q; Rp = R; Sp = S;
-                P = Pn; Q = Qn; R = Rn; S = Sn;
-              }
+          for (int u = 0; u < H; ++u) {
+            // pair v = (c, c + 1) with c = 2v; pairs with bit 2 of v set are stored as
+            // (c + 1, c) (see the slicers' row order)
+            const int4 pq = make_int4(zfix(P.re), zfix(P.im), zfix(Q.re), zfix(Q.im));
+            const bool swp = ((half * H + u) >> 2) & 1;
+            ebh[u] = swp ? make_int4(pq.z, pq.w, pq.x, pq.y) : pq;
+            if (u + 1 < H) {
+              const cplx Pn = {fma(m2, P.re, -Pp.re), fma(m2, P.im, -Pp.im)};
+              const cplx Qn = {fma(m2, Q.re, -Qp.re), fma(m2, Q.im, -Qp.im)};
+              Pp = P;
+              Qp = Q;
+              P = Pn;
+              Q = Qn;
             }
-            if (u < 16) {
+          }
+          if (half) {
+            const cplx sc = (Cf == CH) ? zf : cmul(zf, zf);         // z^Cf, Cf in {CH, 2 CH}
+            const double mf = 2.0 * sc.re;                           // 2 cos Cf phi
+            cplx Aa = {1.0, 0.0}, Ap = {sc.re, -sc.im};              // z^0, z^-Cf
+#pragma unroll
+            for (int u = 0; u < 16; ++u) {
               // a with bit 2 set: stored as (im, re) (see the slicers' row order)
               ea[p * kEaStride + u] = ((u >> 2) & 1) ? make_float2((float)Aa.im, (float)Aa.re)
                                                      : make_float2((float)Aa.re, (float)Aa.im);
@@ -329,16 +337,20 @@ bin_sums_tc_kernel(int Nl, int Cf, const double* __restrict__ pay, const int* __
               Ap = Aa;
               Aa = An;
             }
+          } else {
+            double h[4];
+            hermite(tv, wv, h);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) gk[p * 4 + k] = (float)(h[k] * inv_scale * kInvKScale[k]);
           }
-          double h[4];
-          hermite(tv, wv, h);
-#pragma unroll
-          for (int k = 0; k < 4; ++k) gk[p * 4 + k] = (float)(h[k] * inv_scale * kInvKScale[k]);
         } else {  // padding points contribute zero
-          for (int u = 0; u < CH / 2; ++u) eb[u] = make_int4(0, 0, 0, 0);
-          for (int u = 0; u < 16; ++u) ea[p * kEaStride + u] = make_float2(0.f, 0.f);
+          for (int u = 0; u < H; ++u) eb[half * H + u] = make_int4(0, 0, 0, 0);
+          if (half) {
+            for (int u = 0; u < 16; ++u) ea[p * kEaStride + u] = make_float2(0.f, 0.f);
+          } else {
 #pragma unroll
-          for (int k = 0; k < 4; ++k) gk[p * 4 + k] = 0.f;
+            for (int k = 0; k < 4; ++k) gk[p * 4 + k] = 0.f;
+          }
         }
         __syncwarp();
         if (lane == 0) tc::mbar_arrive(&afull[buf]);
@@ -368,28 +380,32 @@ bin_sums_tc_kernel(int Nl, int Cf, const double* __restrict__ pay, const int* __
           const int4* eb = reinterpret_cast<const int4*>(eb_of(buf));
           const float2* ea = ea_of(buf);
           const float* gk = gk_of(buf);
-          constexpr int nB = 4 * (CH / 2);  // (16-point chunk h, c pair)
+          constexpr int nB = 4 * (CH / 4);  // (16-point chunk h, c pairs cp and cp + CH/4)
           constexpr int nA = 4 * 32;        // (16-point chunk h, k, a pair)
-          // One unit per thread; the B and A units are separate straight-line paths.
+          // The B and A units are separate straight-line paths; a B thread takes two units.
           if (tid < nB) {
-            const int h = tid / (CH / 2), cp = tid % (CH / 2);
-            // Re/Im of c = 2 cp and c + 1 (rows c and CH + c).  Lanes with bit 2 of cp set
-            // hold the pair as (c + 1, c), so a quarter warp's stores cover both rows of a
-            // 128-byte line and all four swizzle chunks: no bank conflicts.
-            const bool sw = (cp >> 2) & 1;
-            const int rows[4] = {2 * cp + sw, CH + 2 * cp + sw, 2 * cp + 1 - sw, CH + 2 * cp + 1 - sw};
-            slice_unit<false>(st_base + 3 * Lay::kTileA, Lay::kTileB, h, rows, [&](int pp, int* X) {
-              const int4 q = eb[pp * (kEbStride / 2) + cp];  // already fixed point
-              X[0] = q.x;
-              X[1] = q.y;
-              X[2] = q.z;
-              X[3] = q.w;
-            });
-          } else if (tid < nB + nA) {
+            const int h = tid / (CH / 4);
+#pragma unroll
+            for (int e2 = 0; e2 < 2; ++e2) {
+              const int cp = tid % (CH / 4) + e2 * (CH / 4);
+              // Re/Im of c = 2 cp and c + 1 (rows c and CH + c).  Lanes with bit 2 of cp
+              // set hold the pair as (c + 1, c), so a quarter warp's stores cover both rows
+              // of a 128-byte line and all four swizzle chunks: no bank conflicts.
+              const bool sw = (cp >> 2) & 1;
+              const int rows[4] = {2 * cp + sw, CH + 2 * cp + sw, 2 * cp + 1 - sw, CH + 2 * cp + 1 - sw};
+              slice_unit<false>(st_base + 3 * Lay::kTileA, Lay::kTileB, h, rows, [&](int pp, int* X) {
+                const int4 q = eb[pp * (kEbStride / 2) + cp];  // already fixed point
+                X[0] = q.x;
+                X[1] = q.y;
+                X[2] = q.z;
+                X[3] = q.w;
+              });
+            }
+          } else if (tid >= kBThreads && tid < kBThreads + nA) {
             // A rows 2 (16 k + a) + (re|im): the two halves of a complex row sit in
             // neighbouring TMEM lanes, so the epilogue combines them with one shuffle.
             // A unit takes the a pair (ap, ap + 8).
-            const int v = tid - nB;
+            const int v = tid - kBThreads;
             const int h = v >> 5, k = (v & 31) >> 3, ap = v & 7;
             const int j0 = 16 * k + ap;
             // lanes with bit 2 of ap set read (im, re) pairs and store rows (im, re): no
