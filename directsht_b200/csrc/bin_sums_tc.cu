@@ -13,9 +13,11 @@
 // the K dimension, 64 per pipeline stage.  When Cf > CH the c range is covered by
 // Cf/CH column groups (grid.y).
 //
-// Operands: per point, FP64 anchors (powers of e^{i phi} by squaring and short
-// recurrences) stored as FP32; per value, X = rint(x q) with q = 2^22 - 2^10 by one FP32
-// FMA against 1.5*2^23, written in balanced base-256 digits X = X0 2^16 + X1 2^8 + X2
+// Operands: per point, FP64 anchors (powers of e^{i phi} by Chebyshev recurrences): the
+// B values e^{i c phi} rounded to fixed point in FP64, e^{i Cf a phi} stored as FP32 and
+// multiplied by g_k / scale in FP32 by the slicers; per value, X = rint(x q) with
+// q = 2^22 - 2^10 (one DFMA against 1.5*2^52, or one FP32 FMA against 1.5*2^23),
+// written in balanced base-256 digits X = X0 2^16 + X1 2^8 + X2
 // with every digit a signed byte: the bytes of Z = (X + 0x8080) ^ 0x8080 (adding 128 to
 // the two low digit positions and flipping their top bits maps [0, 255] onto
 // [-128, 127]).  Five tcgen05.mma.kind::i8 per K step accumulate exactly in S32 TMEM:
@@ -88,15 +90,6 @@ __device__ __forceinline__ int zfix(double x) {
 __device__ __forceinline__ int quant(float x) {
   return __float_as_int(fmaf(x, kQf, kMagic)) - (0x4B400000 - 0x8080);
 }
-
-// Byte B of a, b, c, d packed into one word (the slices of X are its bytes 2, 1, 0).
-template <int B>
-__device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
-  const uint32_t lo = __byte_perm((uint32_t)a, (uint32_t)b, B | ((4 + B) << 4));
-  const uint32_t hi = __byte_perm((uint32_t)c, (uint32_t)d, B | ((4 + B) << 4));
-  return __byte_perm(lo, hi, 0x5410);
-}
-
 
 // Shared-memory descriptor: K-major operand in the 64-byte swizzle layout (rows of 64 B,
 // 8-row atoms of 512 B packed: stride byte offset 512).
