@@ -30,7 +30,8 @@
 // S32 sum below 2^31.
 //
 // Warp roles: warps 6-9 (one per SM sub-partition) compute the FP64 anchors of a block
-// into one of two anchor buffers, one block ahead, two threads per point; warps 0-5
+// into one of two anchor buffers, one block ahead, two threads per point (warps 6-7 the
+// heavier half, on the sub-partitions without a B slicer warp); warps 0-5
 // quantise and slice them into a ring of 64-byte-swizzled K-major int8 tiles (warps 0-1
 // the B tiles, 2-5 the A tiles); warp 10 issues the MMAs from one thread; warps 0-3 run
 // each piece's epilogue (TMEM lanes 0-127) while warps 4-5 and the anchor warps start the
@@ -247,7 +248,8 @@ bin_sums_tc_kernel(int Nl, int Cf, const double* __restrict__ pay, const int* __
     // of powers of two of e^{i phi}.  FP64 throughout (the recurrences lose about
     // steps^2 ulp, far below the 2^-22 fixed-point step).  Then the Hermite weights
     // g_k / scale.  The records of the point in the next two blocks are loaded meanwhile.
-    const int p = (tid - kSlicers) & 63, half = (tid - kSlicers) >> 6;
+    // half 1 (the heavier) on warps 6-7, i.e. sub-partitions 2-3, where no B slicer warp runs
+    const int p = (tid - kSlicers) & 63, half = ((tid - kSlicers) >> 6) ^ 1;
     uint32_t g = 0;
     for (int piece = blockIdx.x; piece < npieces && !*abort_flag; piece += gridDim.x) {
       const int64_t start = piece_start[piece];
