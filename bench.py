@@ -414,8 +414,9 @@ def main(argv=None):
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-sample", type=int, default=200_000)
-    ap.add_argument("--ref-sample", type=int, default=100_000,
-                    help="points per step of --impl reference (about 11 s per step on 16 host cores)")
+    ap.add_argument("--ref-sample", type=int, default=200_000,
+                    help="points per step of --impl reference (about 22 s per step on 16 host cores; smaller "
+                         "samples understate its throughput: each call has a fixed table-contraction cost)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-fp64-compare", action="store_true")
