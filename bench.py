@@ -148,37 +148,68 @@ def measured_peaks():
 
 
 # ---------------------------------------------------------------------------------------
-def cpu_reference_run(spec, sample_n, steps, warmup, seed=0):
-    """The reference's own C/OpenMP transform (csht/sht_helper.c, built into oracle/_ref)
-    on a bounded sample of the workload's points.  The polar points are rotated before the
-    timed region and their alm rotated back after it (healpy's part in the reference)."""
+def cpu_reference_run(spec, sample_n, steps, warmup, seed=0, probe_n=1000):
+    """The reference's own C/OpenMP transform (csht/sht_helper.c, built into oracle/_ref) on a
+    bounded sample of the workload's points, the polar/equatorial split of csht/calc_alms.py
+    included.  Every timed step rotates the polar points, runs the four do_transform calls
+    (polar and equatorial sets, x >= 0 and x < 0 halves) and rotates the polar alm back with
+    precomputed Wigner d(pi/2) matrices (the oracle's restatement standing in for healpy's
+    rotate_alm, which is absent).  Each call has a fixed cost independent of the points (it
+    zeroes one 4 Nl Nx accumulator per thread and contracts every (l, m) over all nodes), so
+    the run also times `probe_n`-point steps for that fixed part and splits the step time into
+    fixed + per-point costs, from which the throughput at the workload's full N follows."""
     from oracle import dsht_oracle as O
     from oracle import ref_csht
     if not ref_csht.available():
         return None
-    th, ph, w = make_points(dict(spec, N=sample_n), seed + 1000)
-    if w.ndim == 2:  # the reference transforms one map per call; time the first
-        w = w[0].astype(np.float64)
+    Nl, Nx, N_full = spec["Nl"], spec["Nx"], spec["N"]
     t0 = time.time()
-    ref = ref_csht.RefCSHT(spec["Nl"], spec["Nx"])
+    ref = ref_csht.RefCSHT(Nl, Nx)
     t_tables = time.time() - t0
-    pol = np.abs(np.cos(th)) >= 0.75
-    tr, pr = O.rotate_points(th[pol], ph[pol])
-    equ = ~pol
-    times = []
-    for it in range(warmup + steps):
+    t0 = time.time()
+    rot = O.AlmRotator(Nl)
+    t_dmat = time.time() - t0
+
+    def points(n, sd):
+        th, ph, w = make_points(dict(spec, N=n), sd)
+        if w.ndim == 2:  # the reference transforms one map per call; time the first
+            w = np.ascontiguousarray(w[0], dtype=np.float64)
+        return th, ph, w
+
+    def one_step(th, ph, w):
         t0 = time.perf_counter()
-        ref.basic(tr, pr, w[pol])
-        ref.basic(th[equ], ph[equ], w[equ])
-        t1 = time.perf_counter()
-        if it >= warmup:
-            times.append(t1 - t0)
+        pol = np.abs(np.cos(th)) >= 0.75
+        alm = np.zeros(ref.Nlm, dtype=np.complex128)
+        if pol.any():
+            tr, pr = O.rotate_points(th[pol], ph[pol])
+            alm += rot(ref.basic(tr, pr, w[pol]))
+        equ = ~pol
+        if equ.any():
+            alm += ref.basic(th[equ], ph[equ], w[equ])
+        return time.perf_counter() - t0
+
+    probe = points(probe_n, seed + 999)
+    sample = points(sample_n, seed + 1000)
+    # Warm-up and fixed-cost probe: the CPU path has no state to warm beyond paging in its
+    # tables, so the W warm-up steps run the probe-sized sample and time the fixed part.
+    fixed = [one_step(*probe) for _ in range(max(warmup, 1))]
+    times = [one_step(*sample) for _ in range(steps)]
     sec = float(np.mean(times))
-    return {"value": sample_n * spec["Nl"] / sec, "unit": "points*ell/s", "cores": os.cpu_count(),
-            "kind": "reference", "seconds_per_step": sec, "table_build_s": t_tables,
-            "sample": f"{sample_n} points of the same distribution (one map) through csht/sht_helper.c "
-                      f"do_transform (OpenMP, {os.cpu_count()} threads) at Nl={spec['Nl']}, Nx={spec['Nx']}; "
-                      f"rotations untimed"}
+    t_fixed = float(np.median(fixed))
+    per_point = max(sec - t_fixed, 0.0) / sample_n
+    t_full = t_fixed + per_point * N_full if N_full else None
+    return {"value": sample_n * Nl / sec, "unit": "points*ell/s", "cores": os.cpu_count(),
+            "kind": "reference", "seconds_per_step": sec, "table_build_s": t_tables, "dmatrix_build_s": t_dmat,
+            "sample_points": sample_n, "same_config": sample_n == N_full,
+            "split": {"fixed_s_per_step": t_fixed, "per_point_s": per_point,
+                      "probe": f"{max(warmup, 1)} steps of {probe_n} points (the warm-up steps)",
+                      "note": "fixed = four do_transform calls and the alm rotation at ~no points"},
+            "at_config": None if t_full is None else {
+                "N": N_full, "seconds_per_transform": t_full, "value": N_full * Nl / t_full,
+                "how": "fixed + per_point x N from this run's split (extrapolated, not timed)"},
+            "sample": f"{sample_n} points of the same distribution (one map) per step through "
+                      f"csht/sht_helper.c do_transform (OpenMP, {os.cpu_count()} threads) at Nl={Nl}, Nx={Nx}, "
+                      f"polar point and alm rotations inside the timed region"}
 
 
 def run_reference_arm(args, spec):
@@ -195,9 +226,15 @@ def run_reference_arm(args, spec):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
             "config": {"workload": spec["name"], "Nl": spec["Nl"], "Nx": spec["Nx"], "N": args.ref_sample,
+                       "N_workload": spec["N"], "same_config": r["same_config"],
                        "maps": 1, "maps_note": "points*ell/s counts point x map x ell; one map per call"},
             "cpu_baseline": {"value": r["value"], "unit": r["unit"], "cores": r["cores"], "kind": r["kind"],
                              "sample": r["sample"]},
+            "split": r["split"], "at_config": r["at_config"],
+            "caveat": None if r["same_config"] else (
+                f"each step transforms {args.ref_sample} of the workload's {spec['N']} points (a full-size step "
+                f"takes minutes on the host); per-call fixed costs weigh more at this size, so the value "
+                f"understates the reference at the full N -- at_config gives the split-based estimate"),
             "e2e": {"value": r["value"], "unit": "points*ell/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -248,9 +285,7 @@ def run_batch(args, spec):
     t_plans = time.time() - t0
     b = TransformBatch(cache, ts)
     t0 = time.time()
-    tune_path = os.path.join(ROOT, "gpurun_out", "autotune_c4.json") if os.path.isdir(
-        os.path.join(ROOT, "gpurun_out")) else None
-    cfg = autotune(b, path=tune_path, reps=1)
+    cfg = autotune(b, path=args.tune_cache, reps=1)
     t_tune = time.time() - t0
     b.capture()
     stream = torch.cuda.current_stream(dev)
@@ -413,11 +448,16 @@ def main(argv=None):
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--cpu-sample", type=int, default=200_000)
-    ap.add_argument("--ref-sample", type=int, default=200_000,
-                    help="points per step of --impl reference (about 22 s per step on 16 host cores; smaller "
-                         "samples understate its throughput: each call has a fixed table-contraction cost)")
+    ap.add_argument("--cpu-sample", type=int, default=1_000_000,
+                    help="points of the cpu_baseline step (the reference's C transform on the host cores)")
+    ap.add_argument("--ref-sample", type=int, default=1_000_000,
+                    help="points per step of --impl reference (about 20 s per step on 16 host cores, most of it "
+                         "the reference's fixed per-call cost; the line also carries the fixed/per-point split "
+                         "and the throughput it implies at the workload's full N)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tune-cache", default=None,
+                    help="JSON file of the uneven-batch autotuner's choices (default: $DSHT_TUNE_CACHE or "
+                         "~/.cache/directsht_b200/autotune.json)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-fp64-compare", action="store_true")
     ap.add_argument("--maps-per-pass", type=int, default=0, help="DSHT_TUNE_MAPS_PER_PASS (0: automatic)")
@@ -586,19 +626,24 @@ def main(argv=None):
         C *= 2
 
     f32_tables = args.precision == "mixed"
+    # Stage times sum every launch of the step: with several maps, bin sums, fold and rotation
+    # ran once per map and the contraction once per pass of maps_per_pass maps.
+    per_pass = d.tune()["maps_per_pass"] or 2 if maps > 1 else 1
+    passes = -(-maps // per_pass)
 
     def stage_roof(name, ms):
-        """Roofline of one stage: algorithmic bytes or ops per launch / measured launch time."""
+        """Roofline of one stage: algorithmic bytes or flops of the whole step (the per-unit
+        figures below x the units the step processes) / the stage's measured time."""
         if ms <= 0:
             return None
         if name == "contract":
             eb = 4 if f32_tables else 8
-            alg = 2.0 * eb * d.Nlm * Nx
+            alg = 2.0 * eb * d.Nlm * Nx * passes
             a = alg / (ms * 1e-3) / 1e9
             return {"kernel": "contract_stream_kernel (TMA 2D tensor-map tiles)", "bound": "hbm", "achieved": a,
                     "peak": hbm_peak, "unit": "GB/s", "frac": a / hbm_peak, "peak_source": peak_src,
                     "algorithmic": f"{2 * eb} B of {'FP32' if f32_tables else 'FP64'} table (Yv, Yd) per "
-                                   f"(l, m, node)"}
+                                   f"(l, m, node) per pass ({passes} passes)"}
         if name == "points":
             alg = 56.0 * N
             a = alg / (ms * 1e-3) / 1e9
@@ -606,25 +651,30 @@ def main(argv=None):
                     "peak": hbm_peak, "unit": "GB/s", "frac": a / hbm_peak, "peak_source": peak_src,
                     "algorithmic": "24 B of inputs read + 32 B of sorted record written per point"}
         if name == "bin_sums" and args.precision != "fp64":
-            alg = 2.0 * 128 * (2 * C) * 8 * N
-            pk = 2 * bf16_peak
+            alg = 24.0 * N * Nl * maps
             a = alg / (ms * 1e-3) / 1e12
+            ops = 2.0 * 128 * (2 * C) * 8 * N * maps
+            a_ops = ops / (ms * 1e-3) / 1e12
             return {"kernel": "bin_sums_tc_kernel (tcgen05 kind::i8)", "bound": "tensor", "achieved": a,
-                    "peak": pk, "unit": "TOP/s", "frac": a / pk,
-                    "peak_source": f"derived: 2 x {peak_src} bf16 (dense int8 rate is twice bf16 on B200)",
-                    "algorithmic": f"8 int8 slice products of a 128 x {2 * C} x (points) GEMM, 2 op per MAC"}
+                    "peak": bf16_peak, "unit": "TFLOP/s", "frac": a / bf16_peak,
+                    "peak_source": f"{peak_src} dense bf16 tensor rate",
+                    "algorithmic": "24 flop per (point, m, map): 8 FMA sums + 4 FMA angle step",
+                    "int8_slice_ops": {"achieved": a_ops, "peak": 2 * bf16_peak, "unit": "TOP/s",
+                                       "frac": a_ops / (2 * bf16_peak),
+                                       "what": f"8 int8 slice products of a 128 x {2 * C} x (points) GEMM, "
+                                               f"2 op per MAC, against 2 x the bf16 rate (dense int8 on B200)"}}
         if name == "bin_sums":
-            alg = 24.0 * N * Nl
+            alg = 24.0 * N * Nl * maps
             a = alg / (ms * 1e-3) / 1e12
             return {"kernel": "bin_sums_fp64_kernel", "bound": "fp64", "achieved": a, "peak": 40.0,
                     "unit": "TFLOP/s", "frac": a / 40.0, "peak_source": "nominal (no measured FP64 figure)",
-                    "algorithmic": "24 flop per (point, m): 8 FMA sums + 4 FMA angle step"}
+                    "algorithmic": "24 flop per (point, m, map): 8 FMA sums + 4 FMA angle step"}
         if name == "rotate":
-            alg = 2.0 * 5 * sum((l + 1) ** 2 for l in range(Nl))
+            alg = 2.0 * 5 * sum((l + 1) ** 2 for l in range(Nl)) * maps
             a = alg / (ms * 1e-3) / 1e12
             return {"kernel": "rotate_back_kernel", "bound": "fp64", "achieved": a, "peak": 40.0,
                     "unit": "TFLOP/s", "frac": a / 40.0, "peak_source": "nominal (no measured FP64 figure)",
-                    "algorithmic": "5 FMA per (l, m, m') of the Wigner-d recursion and product"}
+                    "algorithmic": "5 FMA per (l, m, m', map) of the Wigner-d recursion and product"}
         return None
 
     roofs = {n: stage_roof(n, ms) for n, ms in stages.items()}
@@ -712,7 +762,7 @@ def main(argv=None):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cpu = cpu_reference_run(spec, args.cpu_sample, 1, 0)
+            cpu = cpu_reference_run(spec, args.cpu_sample, 1, 1)
         except Exception as exc:  # reported, not fatal
             cpu = {"value": None, "error": str(exc)}
 
@@ -732,8 +782,8 @@ def main(argv=None):
                        "parallelism": f"replicas x{world}"},
             "p50_ms": float(np.percentile(per_step, 50)), "p99_ms": float(np.percentile(per_step, 99)),
             "stages_ms": stages, "plan_build_s": t_plan, "roofline": roof,
-            "stages_note": ("one sort (points) for all maps; bin_sums..rotate are those of one map "
-                            "(bin_sums includes its payload gather)") if maps > 1 else (
+            "stages_note": ("one sort (points) for all maps; bin_sums, fold and rotate summed over all maps "
+                            "(bin_sums includes the payload gathers), contract over all passes") if maps > 1 else (
                 "stages of one single-transform step (the headline step holds %d point sets)" % batch
                 if batch > 1 else "all stages of one step"),
             "stage_rooflines": {k: v for k, v in roofs.items() if v}, "cpu_baseline": cpu, "e2e": e2e,

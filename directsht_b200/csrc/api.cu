@@ -90,6 +90,8 @@ size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* ba
   w.piece_start = reinterpret_cast<int64_t*>(take(sizeof(int64_t) * pmax));
   w.piece_len = reinterpret_cast<int*>(take(sizeof(int) * pmax));
   w.piecemax = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * pmax));
+  w.wsum = reinterpret_cast<double*>(take(sizeof(double) * pmax));
+  w.nodew = reinterpret_cast<double*>(take(sizeof(double) * 2 * (size_t)g.Nx));
   w.npieces = reinterpret_cast<int*>(take(sizeof(int)));
   w.flags = reinterpret_cast<unsigned*>(take(sizeof(unsigned)));
   if (maps) {
@@ -99,6 +101,9 @@ size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* ba
   w.partial = reinterpret_cast<double*>(take(sizeof(double) * 8 * (size_t)g.Nl * pmax));
   // One fold per map of a contraction pass (multi-map transforms).
   w.fold_slots = std::max(1, std::min(fold_slots, kMaxPass));
+  w.heavy_flag = reinterpret_cast<uint8_t*>(take(2 * (size_t)g.Nx * w.fold_slots));
+  w.heavy_list = reinterpret_cast<int*>(take(sizeof(int) * (size_t)kHeavyMax * w.fold_slots));
+  w.heavy_n = reinterpret_cast<int*>(take(sizeof(int) * w.fold_slots));
   w.fold = reinterpret_cast<double*>(take(sizeof(double) * 16 * (size_t)g.Nl * g.Nx * w.fold_slots));
   w.tile_live = reinterpret_cast<uint8_t*>(take(2 * (size_t)ntile));
   w.tile_live2 = reinterpret_cast<uint8_t*>(take(2 * (size_t)((g.Nx + 255) / 256)));
@@ -153,38 +158,41 @@ Geometry make_geometry(int Nl, int Nx, double xmax) {
 int run_after_sort(dsht_plan_s* p, int64_t N, int mode, double* alm, const Workspace& ws, cudaStream_t s,
                    bool marks) {
   const Geometry& g = p->g;
-  auto mark = [&](int i) {
-    if (marks && p->prof) cudaEventRecord(p->ev[i], s);
+  auto mark = [&](int stage) {
+    if (marks) prof_mark(p, stage, s);
   };
   Workspace w2 = ws;
   // Small transforms run the FP64 stages even on a mixed-precision plan.
   const Route rt = plan_route(p, N);
   const bool f32_tables = rt.f32_tables;
   if (rt.tc) {
-    int rc = launch_bin_sums_tc(g, ws, s);
+    int rc = launch_bin_sums_tc(g, ws, s);  // piece maxima and |w| sums first
     if (rc) return rc;
     w2.partial_f32 = 1;
   } else {
+    if (f32_tables) launch_piece_maxima(ws, s);  // the |w| sums of the heavy-node test
     launch_bin_sums_fp64(g, ws, s);
     w2.partial_f32 = 0;
   }
   w2.fold_f32 = f32_tables ? 1 : 0;
-  mark(2);
-  launch_fold(g, w2, s);
-  mark(3);
-  if (f32_tables)
-    launch_contract_stream(g, true, p->tmYv32, p->tmYd32, ws, s);
-  else if (p->tm64)
+  mark(DSHT_STAGE_FOLD);
+  if (f32_tables) launch_heavy_select(g, w2, 0, s);
+  launch_fold(g, w2, s, f32_tables ? w2.heavy_flag : nullptr);
+  mark(DSHT_STAGE_CONTRACT);
+  if (f32_tables) {
+    launch_heavy_otf(g, w2, 0, ws.alm_equ, ws.alm_pol, s);
+    launch_contract_stream(g, true, p->tmYv32, p->tmYd32, ws, s, ws.heavy_n);
+  } else if (p->tm64)
     launch_contract_stream(g, false, p->tmYv, p->tmYd, ws, s);
   else
     launch_contract_fp64(g, p->Yv, p->Yd, ws, s);
-  mark(4);
+  mark(DSHT_STAGE_ROTATE);
   if (mode == DSHT_MODE_CALL) {
     launch_rotate_back(g, ws.alm_pol, ws.alm_equ, alm, ws.flags, s);
   } else {
     DSHT_CUDA_OK(cudaMemcpyAsync(alm, ws.alm_equ, sizeof(double) * 2 * g.Nlm, cudaMemcpyDeviceToDevice, s));
   }
-  mark(5);
+  mark(-1);
   if (int rc = launch_error("kernel launch")) return rc;
   DSHT_CUDA_OK(cudaGetLastError());
   return DSHT_OK;
@@ -193,10 +201,10 @@ int run_after_sort(dsht_plan_s* p, int64_t N, int mode, double* alm, const Works
 // Runs the whole pipeline on `s`; leaves the device flags in ws.flags.
 int run_pipeline(dsht_plan_s* p, const double* theta, const double* phi, const double* w, int64_t N,
                         int mode, double* alm, const Workspace& ws, cudaStream_t s) {
-  p->prof_maps = false;
-  if (p->prof) cudaEventRecord(p->ev[0], s);
+  p->ev_n = 0;
+  prof_mark(p, DSHT_STAGE_POINTS, s);
   launch_points(p->g, theta, phi, w, 0, N, mode, ws, s);
-  if (p->prof) cudaEventRecord(p->ev[1], s);
+  prof_mark(p, DSHT_STAGE_BIN_SUMS, s);
   return run_after_sort(p, N, mode, alm, ws, s, true);
 }
 
@@ -213,17 +221,13 @@ int run_items(dsht_plan_s* p, const Item* items, int n, int mode, const Workspac
   const int64_t nlm2 = 2 * g.Nlm;
   const int64_t fold_stride = 4 * (int64_t)g.Nl * g.Nx;  // F4 elements per fold
   const int ntile2 = (g.Nx + 255) / 256;
-  auto ev = [&](int i) {
-    if (p->prof) cudaEventRecord(p->ev[i], s);
-  };
-  p->prof_maps = true;
+  p->ev_n = 0;
   DSHT_CUDA_OK(cudaMemsetAsync(ws.all_flags, 0, sizeof(unsigned), s));
   // Items in two classes by the precision their size selects; same_points chains stay whole
   // (they share N, hence the class).
   std::vector<int> order[2];
   for (int i = 0; i < n; ++i) order[plan_route(p, items[i].N).tc ? 1 : 0].push_back(i);
   int sorted_item = -1;  // item whose sort the workspace holds
-  bool first_ev = true;
   for (int cls = 0; cls < 2; ++cls) {
     const std::vector<int>& list = order[cls];
     if (list.empty()) continue;
@@ -245,6 +249,7 @@ int run_items(dsht_plan_s* p, const Item* items, int n, int mode, const Workspac
         so.slot[k] = ws.slot_flags + k;
         so.status[k] = items[pend[k]].status;
       }
+      prof_mark(p, DSHT_STAGE_ROTATE, s);
       if (mode == DSHT_MODE_CALL) launch_rotate_back_maps(g, rm, (int)pend.size(), s);
       launch_publish_flags(so, (int)pend.size(), ws.all_flags, s);
       pend.clear();
@@ -258,7 +263,9 @@ int run_items(dsht_plan_s* p, const Item* items, int n, int mode, const Workspac
         for (size_t k = 0; k < pass.size(); ++k) {
           out.equ[k] = items[pass[k]].alm;
           out.pol[k] = ws.alm_pol + nlm2 * (base + k);
+          out.heavy_n[k] = f32_tables ? ws.heavy_n + k : nullptr;  // fold slot k
         }
+        prof_mark(p, DSHT_STAGE_CONTRACT, s);
         launch_contract_pass(g, f32_tables, f32_tables ? p->tmYv32 : p->tmYv, f32_tables ? p->tmYd32 : p->tmYd,
                              p->tmYv32h, p->tmYd32h,
                              ws.fold, fold_stride, (int)pass.size(), ws.tile_live2, out, ws.slot_flags + base, s);
@@ -271,16 +278,14 @@ int run_items(dsht_plan_s* p, const Item* items, int n, int mode, const Workspac
     for (size_t li = 0; li < list.size(); ++li) {
       const int i = list[li];
       const Item& item = items[i];
-      const bool last = li + 1 == list.size() && cls == 1 - (order[1].empty() ? 1 : 0);
       const int slot = (int)(pend.size() + pass.size());
       Workspace w2 = ws;
       w2.flags = ws.slot_flags + slot;
-      if (p->prof && first_ev) {
-        ev(0);
-      }
       if (item.same_points && sorted_item >= 0) {
+        prof_mark(p, DSHT_STAGE_BIN_SUMS, s);  // the weight gather counts with the bin sums
         launch_gather(g, item.w, item.w_f32, item.N, ws, s);
       } else {
+        prof_mark(p, DSHT_STAGE_POINTS, s);
         // The sort keeps the input index and t of every slot when later items share it.
         Workspace wp = ws;
         const bool shared = li + 1 < list.size() && items[list[li + 1]].same_points;
@@ -290,11 +295,7 @@ int run_items(dsht_plan_s* p, const Item* items, int n, int mode, const Workspac
         launch_points(g, item.theta, item.phi, item.w, item.w_f32, item.N, mode, wp, s);
         sorted_item = i;
       }
-      if (p->prof && first_ev) {
-        ev(1);
-        first_ev = false;
-      }
-      if (last) ev(DSHT_STAGE_COUNT + 1);
+      prof_mark(p, DSHT_STAGE_BIN_SUMS, s);
       DSHT_CUDA_OK(cudaMemcpyAsync(w2.flags, ws.flags, sizeof(unsigned), cudaMemcpyDeviceToDevice, s));
       if (mixed) {
         int rc = launch_bin_sums_tc(g, w2, s);
@@ -304,14 +305,20 @@ int run_items(dsht_plan_s* p, const Item* items, int n, int mode, const Workspac
         launch_bin_sums_fp64(g, w2, s);
         w2.partial_f32 = 0;
       }
-      if (last) ev(2);
+      prof_mark(p, DSHT_STAGE_FOLD, s);
       if (streamed) {
         if (pass.empty()) DSHT_CUDA_OK(cudaMemsetAsync(ws.tile_live2, 0, 2 * (size_t)ntile2, s));
         w2.fold_f32 = f32_tables ? 1 : 0;
         w2.fold = reinterpret_cast<double*>(reinterpret_cast<uint8_t*>(ws.fold) + f4 * fold_stride * pass.size());
         w2.live_or = 1;
-        launch_fold(g, w2, s);
-        if (last) ev(3);
+        const int fslot = (int)pass.size();
+        if (f32_tables) {
+          if (!mixed) launch_piece_maxima(w2, s);  // the |w| sums of the heavy-node test
+          launch_heavy_select(g, w2, fslot, s);
+        }
+        launch_fold(g, w2, s, f32_tables ? w2.heavy_flag + (size_t)fslot * 2 * g.Nx : nullptr);
+        // heavy nodes in FP64 now, while this map's bin sums are in ws.partial; the pass adds
+        if (f32_tables) launch_heavy_otf(g, w2, fslot, item.alm, ws.alm_pol + nlm2 * slot, s);
         pass.push_back(i);
         if ((int)pass.size() == G || li + 1 == list.size()) {
           int rc = run_pass();
@@ -322,7 +329,7 @@ int run_items(dsht_plan_s* p, const Item* items, int n, int mode, const Workspac
         w2.alm_pol = ws.alm_pol + nlm2 * slot;
         w2.alm_equ = item.alm;
         launch_fold(g, w2, s);
-        if (last) ev(3);
+        prof_mark(p, DSHT_STAGE_CONTRACT, s);
         launch_contract_fp64(g, p->Yv, p->Yd, w2, s);
         pend.push_back(i);
         if (pend.size() + 1 > (size_t)kMaxRot) {
@@ -330,27 +337,37 @@ int run_items(dsht_plan_s* p, const Item* items, int n, int mode, const Workspac
           if (rc) return rc;
         }
       }
-      if (last) ev(4);
     }
     int rc = flush_rotation();
     if (rc) return rc;
   }
-  ev(5);
+  prof_mark(p, -1, s);
   if (int rc = launch_error("kernel launch")) return rc;
   DSHT_CUDA_OK(cudaGetLastError());
   return DSHT_OK;
 }
 
-// After the stream has been synchronised: fold the stage events into the totals.
+void prof_mark(dsht_plan_s* p, int stage, cudaStream_t s) {
+  if (!p->prof || !p->ev) return;
+  if (p->ev_n >= dsht_plan_s::kProfMarks) return;  // later stages of a huge call go uncounted
+  cudaEventRecord(p->ev[p->ev_n], s);
+  p->ev_stage[p->ev_n] = (int8_t)stage;
+  p->ev_n += 1;
+}
+
+// After the stream has been synchronised: add every interval between consecutive stage
+// marks to its stage's total.
 void collect_profile(dsht_plan_s* p) {
-  if (!p->prof) return;
-  for (int i = 0; i < DSHT_STAGE_COUNT; ++i) {
+  if (!p->prof || !p->ev) return;
+  for (int k = 0; k + 1 < p->ev_n; ++k) {
+    const int st = p->ev_stage[k];
     float ms = 0.f;
-    cudaEvent_t a = (p->prof_maps && i == DSHT_STAGE_BIN_SUMS) ? p->ev[DSHT_STAGE_COUNT + 1] : p->ev[i];
-    if (cudaEventElapsedTime(&ms, a, p->ev[i + 1]) == cudaSuccess) p->prof_ms[i] += ms;
+    if (st >= 0 && st < DSHT_STAGE_COUNT && cudaEventElapsedTime(&ms, p->ev[k], p->ev[k + 1]) == cudaSuccess)
+      p->prof_ms[st] += ms;
   }
+  cudaGetLastError();
+  p->ev_n = 0;
   p->prof_calls += 1;
-  p->prof_maps = false;
 }
 
 int flags_to_status(unsigned f, int mode) {
@@ -449,8 +466,11 @@ int dsht_plan_create(int Nl, int Nx, double xmax, int flags, dsht_plan_t* plan) 
 
 int dsht_plan_destroy(dsht_plan_t p) {
   if (!p) return DSHT_OK;
-  for (auto& e : p->ev)
-    if (e) cudaEventDestroy(e);
+  if (p->ev) {
+    for (int k = 0; k < dsht_plan_s::kProfMarks; ++k)
+      if (p->ev[k]) cudaEventDestroy(p->ev[k]);
+    delete[] p->ev;
+  }
   cudaFree(p->Yv);
   cudaFree(p->Yd);
   cudaFree(p->Yv32);
@@ -533,8 +553,11 @@ int dsht_get_precision(dsht_plan_t p, int* precision) {
 int dsht_profile_enable(dsht_plan_t p, int enable) {
   if (!p) return set_error(DSHT_ERR_INVALID, "plan is NULL");
   std::lock_guard<std::mutex> lock(p->mu);
-  if (enable && !p->ev[0])
-    for (auto& e : p->ev) DSHT_CUDA_OK(cudaEventCreate(&e));
+  if (enable && !p->ev) {
+    p->ev = new cudaEvent_t[dsht_plan_s::kProfMarks]();
+    for (int k = 0; k < dsht_plan_s::kProfMarks; ++k) DSHT_CUDA_OK(cudaEventCreate(&p->ev[k]));
+  }
+  p->ev_n = 0;
   p->prof = enable != 0;
   return DSHT_OK;
 }
@@ -838,6 +861,35 @@ int dsht_get_table(dsht_plan_t p, int which, double* out) {
       DSHT_CUDA_OK(cudaMemcpy(tmp.data(), t + i, sizeof(float) * c, cudaMemcpyDeviceToHost));
       for (size_t k = 0; k < c; ++k) out[i + k] = tmp[k];
     }
+  }
+  return DSHT_OK;
+}
+
+int dsht_get_table_mlayout(dsht_plan_t p, int which, double* out, int out_on_device, void* stream) {
+  if (!p || !out || which < 0 || which > 1) return set_error(DSHT_ERR_INVALID, "invalid arguments");
+  const int Nl = p->g.Nl, Nx = p->g.Nx;
+  const size_t plane = (size_t)Nl * Nx;  // one m: Nl rows of Nx
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (out_on_device) {
+    launch_table_mlayout(p->g, which == 0 ? p->Yv : p->Yd, which == 0 ? p->Yv32 : p->Yd32, out, s);
+    return launch_error("table_mlayout_kernel");
+  }
+  std::vector<float> tmp;
+  for (int m = 0; m < Nl; ++m) {
+    // Rows l = m..Nl-1 of column m are contiguous in Healpy order; they fill k = l - m.
+    const int64_t row0 = hp_index(m, m, Nl);
+    const size_t n = (size_t)(Nl - m) * Nx;
+    double* dst = out + (size_t)m * plane;
+    if (p->Yv) {
+      const double* t = (which == 0 ? p->Yv : p->Yd) + (size_t)row0 * Nx;
+      DSHT_CUDA_OK(cudaMemcpy(dst, t, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    } else {
+      const float* t = (which == 0 ? p->Yv32 : p->Yd32) + (size_t)row0 * Nx;
+      tmp.resize(n);
+      DSHT_CUDA_OK(cudaMemcpy(tmp.data(), t, sizeof(float) * n, cudaMemcpyDeviceToHost));
+      for (size_t k = 0; k < n; ++k) dst[k] = tmp[k];
+    }
+    std::memset(dst + n, 0, sizeof(double) * (plane - n));  // k >= Nl - m: l >= Nl (unphysical)
   }
   return DSHT_OK;
 }

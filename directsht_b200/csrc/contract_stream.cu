@@ -240,7 +240,9 @@ contract_stream_kernel(int Nl, int Nx, int64_t nitems, const __grid_constant__ C
             for (int o = 16; o > 0; o >>= 1) acc[gm][i][c] += __shfl_xor_sync(0xffffffffu, acc[gm][i][c], o);
       if (lane == 0) {
 #pragma unroll
-        for (int gm = 0; gm < kG; ++gm)
+        for (int gm = 0; gm < kG; ++gm) {
+          // outputs that already hold heavy-node FP64 sums (heavy.cu) are added to
+          const bool add = out.heavy_n[gm] != nullptr && *out.heavy_n[gm] > 0;
 #pragma unroll
           for (int i = 0; i < RW; ++i) {
             const int l = l0 + rbase + 2 * i;
@@ -248,12 +250,20 @@ contract_stream_kernel(int Nl, int Nx, int64_t nitems, const __grid_constant__ C
               const int64_t idx = hp_index(l, m, Nl);
               double* ae = out.equ[gm];
               double* ap = out.pol[gm];
-              ae[2 * idx] = acc[gm][i][0];
-              ae[2 * idx + 1] = acc[gm][i][1];
-              ap[2 * idx] = acc[gm][i][2];
-              ap[2 * idx + 1] = acc[gm][i][3];
+              if (add) {
+                ae[2 * idx] += acc[gm][i][0];
+                ae[2 * idx + 1] += acc[gm][i][1];
+                ap[2 * idx] += acc[gm][i][2];
+                ap[2 * idx + 1] += acc[gm][i][3];
+              } else {
+                ae[2 * idx] = acc[gm][i][0];
+                ae[2 * idx + 1] = acc[gm][i][1];
+                ap[2 * idx] = acc[gm][i][2];
+                ap[2 * idx + 1] = acc[gm][i][3];
+              }
             }
           }
+        }
       }
     }
   }
@@ -311,10 +321,11 @@ static void stream_launch(const Geometry& g, const CUtensorMap& tmv, const CUten
 }
 
 void launch_contract_stream(const Geometry& g, bool mixed, const CUtensorMap& tmv, const CUtensorMap& tmd,
-                            const Workspace& ws, cudaStream_t s) {
+                            const Workspace& ws, cudaStream_t s, const int* heavy_n) {
   MapOut out{};
   out.equ[0] = ws.alm_equ;
   out.pol[0] = ws.alm_pol;
+  out.heavy_n[0] = heavy_n;
   if (mixed)
     stream_launch<true, 1>(g, tmv, tmd, ws.fold, 0, ws.tile_live2, out, ws.flags, s);
   else
@@ -339,6 +350,7 @@ void launch_contract_pass(const Geometry& g, bool mixed, const CUtensorMap& tmv,
       MapOut o1{};
       o1.equ[0] = out.equ[k];
       o1.pol[0] = out.pol[k];
+      o1.heavy_n[0] = out.heavy_n[k];
       stream_launch<false, 1>(g, tmv, tmd, static_cast<const double4*>(fold) + fold_stride * k, 0, live, o1, flags,
                               s);
     }

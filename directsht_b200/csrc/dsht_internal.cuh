@@ -42,12 +42,21 @@ struct Geometry {
   int nkeys;          // kSets * nbins
 };
 
-// Output pointers of one contraction pass (kernel parameter, passed by value).
+// Output pointers of one contraction pass (kernel parameter, passed by value).  When
+// heavy_n[k] is set and *heavy_n[k] > 0, map k's outputs already hold its heavy nodes' FP64
+// contribution (heavy.cu) and the pass adds to them instead of storing.
 constexpr int kMaxPass = 4;
 struct MapOut {
   double* equ[kMaxPass];
   double* pol[kMaxPass];
+  const int* heavy_n[kMaxPass];
 };
+
+// Heavy nodes of the FP32-table contraction (heavy.cu): a (half, node) holding more than
+// 1/kHeavyDiv of a transform's total |w| is contracted in FP64 instead; at most kHeavyMax
+// of them (every point feeds two nodes, so fewer than 2 kHeavyDiv can exceed the share).
+constexpr int kHeavyDiv = 256;
+constexpr int kHeavyMax = 2 * kHeavyDiv;
 
 // Maps of one batched rotation: io[k] += R(rot[k]) when *flags[k] has polar points.
 constexpr int kMaxRot = 8;
@@ -70,6 +79,11 @@ struct Workspace {
   double* pay;          // [N][4] sorted records (cos phi, sin phi, w, t)
   uint32_t* sidx;       // [N] input index of each sorted slot (multi-map transforms)
   uint32_t* piecemax;   // [pmax] largest |w h_k| of the piece's points (float bits)
+  double* wsum;         // [pmax] sum of |w| of the piece's points
+  double* nodew;        // [2][Nx] sum of |w| feeding each (half, node)
+  uint8_t* heavy_flag;  // [fold_slots][2][Nx] node contracted in FP64 (FP32-table route)
+  int* heavy_list;      // [fold_slots][kHeavyMax] heavy entries h * Nx + j in order
+  int* heavy_n;         // [fold_slots] number of heavy entries
   uint32_t* count;      // [nkeys + 1]
   uint32_t* offset;     // [nkeys + 1]
   uint32_t* cursor;     // [nkeys]
@@ -123,12 +137,20 @@ void launch_publish_flags(const StatusOut& st, int n, unsigned* all, cudaStream_
 void launch_bin_sums_fp64(const Geometry& g, const Workspace& ws, cudaStream_t s);
 int launch_bin_sums_tc(const Geometry& g, const Workspace& ws, cudaStream_t s);
 int tc_inner_factor(int Nl);
-void launch_fold(const Geometry& g, const Workspace& ws, cudaStream_t s);
+// Fold of the current map into ws.fold; with an FP32 fold, `heavy` ([2][Nx] flags or null)
+// marks the (half, node) entries written as zeros.
+void launch_fold(const Geometry& g, const Workspace& ws, cudaStream_t s, const uint8_t* heavy = nullptr);
+// Heavy nodes of fold slot `slot`: flags and list from the per-piece |w| sums (ws.wsum).
+void launch_heavy_select(const Geometry& g, const Workspace& ws, int slot, cudaStream_t s);
+// Their FP64 contribution for every (l, m) stored (not added) into alm_equ / alm_pol, from
+// the per-piece bin sums ws.partial; does nothing when the slot has no heavy node.
+void launch_heavy_otf(const Geometry& g, const Workspace& ws, int slot, double* alm_equ, double* alm_pol,
+                      cudaStream_t s);
 void launch_contract_fp64(const Geometry& g, const double* Yv, const double* Yd,
                           const Workspace& ws, cudaStream_t s);
 bool contract_stream_ok(const Geometry& g, size_t elem_bytes);
 void launch_contract_stream(const Geometry& g, bool mixed, const CUtensorMap& tmv, const CUtensorMap& tmd,
-                            const Workspace& ws, cudaStream_t s);
+                            const Workspace& ws, cudaStream_t s, const int* heavy_n = nullptr);
 // One contraction pass over up to contract_stream_max_maps(mixed) folds (fold k at fold +
 // k * fold_stride F4 elements) that share one read of the tables; alm of fold k to
 // out.equ[k], out.pol[k].  FP64 tables take one fold per launch.
@@ -142,6 +164,9 @@ void launch_contract_pass(const Geometry& g, bool mixed, const CUtensorMap& tmv,
 int make_table_tmap(CUtensorMap* tm, const void* base, size_t elem_bytes, int Nx, int64_t Nlm, int rows = 0);
 void launch_tables_to_f32(const Geometry& g, const double* Yv, const double* Yd, float* Yv32, float* Yd32,
                           cudaStream_t s);
+// A table in the JAX path's layout out[m][l - m][j] (Nl x Nl x Nx doubles, zeros where
+// l >= Nl) on the device, from the FP64 table t64 or, when it is null, the FP32 table t32.
+void launch_table_mlayout(const Geometry& g, const double* t64, const float* t32, double* out, cudaStream_t s);
 void launch_rotate_back(const Geometry& g, const double* alm_rot, const double* alm_add,
                         double* alm_out, const unsigned* flags, cudaStream_t s);
 // alm io[k] += R(rot[k]) for k < nmaps <= kMaxRot (a map without polar points is left as it is).
@@ -192,12 +217,14 @@ struct dsht_plan_s {
   int precision = DSHT_PREC_FP64;
   int tune_piece_max = 0;      // points per bin piece (0: chosen from N)
   int tune_maps_per_pass = 0;  // maps per multi-map contraction pass (0: the most that fit)
-  // Stage timers.
+  // Stage timers: one event per stage boundary of a call, in stream order; the interval
+  // from mark k to mark k+1 belongs to stage ev_stage[k] (-1: no stage).  Summed per stage
+  // into prof_ms when the call has synchronised.
+  static constexpr int kProfMarks = 4096;
   bool prof = false;
-  // ev[0..5]: stage boundaries; ev[6]: start of the last map's bin sums (multi-map calls,
-  // where stage 0 covers the sort alone and stages 1-4 the last map).
-  cudaEvent_t ev[DSHT_STAGE_COUNT + 2] = {};
-  bool prof_maps = false;
+  cudaEvent_t* ev = nullptr;  // [kProfMarks], created by dsht_profile_enable
+  int8_t ev_stage[kProfMarks] = {};
+  int ev_n = 0;
   double prof_ms[DSHT_STAGE_COUNT] = {};
   int64_t prof_calls = 0;
   std::mutex mu;
@@ -227,6 +254,8 @@ struct Item {
 int run_items(dsht_plan_s* p, const Item* items, int n, int mode, const Workspace& ws, cudaStream_t s);
 // After the stream has been synchronised: fold the stage events into the plan's totals.
 void collect_profile(dsht_plan_s* p);
+// Stage boundary on stream s when profiling: what follows belongs to `stage` (-1: none).
+void prof_mark(dsht_plan_s* p, int stage, cudaStream_t s);
 // Map device flag bits to a DSHT status code (and set the error message).
 int flags_to_status(unsigned f, int mode);
 }  // namespace dsht

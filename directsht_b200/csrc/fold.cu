@@ -18,7 +18,7 @@ constexpr int kFoldThreads = 128;
 template <typename T, typename F4>
 __global__ void __launch_bounds__(kFoldThreads)
 fold_kernel(int Nl, int Nx, int nbins, double dx, const int* __restrict__ piece_first,
-            const T* __restrict__ partial, F4* __restrict__ fold) {
+            const T* __restrict__ partial, F4* __restrict__ fold, const uint8_t* __restrict__ heavy) {
   const int j = blockIdx.x;
   const int m = blockIdx.y * blockDim.x + threadIdx.x;
   if (m >= Nl) return;
@@ -52,6 +52,14 @@ fold_kernel(int Nl, int Nx, int nbins, double dx, const int* __restrict__ piece_
     B[s][1] = dx * bi;
   }
   using E = decltype(F4::x);
+  // Heavy (half, node) entries are contracted in FP64 elsewhere (heavy.cu): zero here.
+  if (heavy) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+      if (heavy[h * Nx + j])
+#pragma unroll
+        for (int s = 2 * h; s < 2 * h + 2; ++s) A[s][0] = A[s][1] = B[s][0] = B[s][1] = 0.0;
+  }
   F4* out = fold + ((size_t)m * 4) * Nx + j;
   out[0] = F4{(E)(A[0][0] + A[1][0]), (E)(A[0][1] + A[1][1]), (E)(B[0][0] + B[1][0]), (E)(B[0][1] + B[1][1])};
   out[(size_t)Nx] = F4{(E)(A[0][0] - A[1][0]), (E)(A[0][1] - A[1][1]), (E)(B[0][0] - B[1][0]), (E)(B[0][1] - B[1][1])};
@@ -81,21 +89,21 @@ __global__ void tile_live_kernel(int nbins, int ntile, int tile, const uint32_t*
 
 int contract_tile();
 
-void launch_fold(const Geometry& g, const Workspace& ws, cudaStream_t s) {
+void launch_fold(const Geometry& g, const Workspace& ws, cudaStream_t s, const uint8_t* heavy) {
   dim3 grid(g.Nx, (g.Nl + kFoldThreads - 1) / kFoldThreads);
   const float* pf = reinterpret_cast<const float*>(ws.partial);
   float4* f32 = reinterpret_cast<float4*>(ws.fold);
   double4* f64 = reinterpret_cast<double4*>(ws.fold);
   if (ws.partial_f32 && ws.fold_f32)
-    fold_kernel<float, float4><<<grid, kFoldThreads, 0, s>>>(g.Nl, g.Nx, g.nbins, g.dx, ws.piece_first, pf, f32);
+    fold_kernel<float, float4><<<grid, kFoldThreads, 0, s>>>(g.Nl, g.Nx, g.nbins, g.dx, ws.piece_first, pf, f32, heavy);
   else if (ws.fold_f32)
     fold_kernel<double, float4><<<grid, kFoldThreads, 0, s>>>(g.Nl, g.Nx, g.nbins, g.dx, ws.piece_first,
-                                                             ws.partial, f32);
+                                                             ws.partial, f32, heavy);
   else if (ws.partial_f32)
-    fold_kernel<float, double4><<<grid, kFoldThreads, 0, s>>>(g.Nl, g.Nx, g.nbins, g.dx, ws.piece_first, pf, f64);
+    fold_kernel<float, double4><<<grid, kFoldThreads, 0, s>>>(g.Nl, g.Nx, g.nbins, g.dx, ws.piece_first, pf, f64, nullptr);
   else
     fold_kernel<double, double4><<<grid, kFoldThreads, 0, s>>>(g.Nl, g.Nx, g.nbins, g.dx, ws.piece_first,
-                                                              ws.partial, f64);
+                                                              ws.partial, f64, nullptr);
   count_launches(1);
   const int tile = contract_tile();
   const int ntile = (g.Nx + tile - 1) / tile;

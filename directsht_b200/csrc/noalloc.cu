@@ -65,6 +65,7 @@ int dsht_execute_noalloc(dsht_plan_t p, const double* theta, const double* phi, 
   if (!p || !alm || N < 0 || (N > 0 && (!theta || !phi || !w)))
     return set_error(DSHT_ERR_INVALID, "invalid arguments");
   if (mode != DSHT_MODE_CALL && mode != DSHT_MODE_BASIC) return set_error(DSHT_ERR_INVALID, "bad mode %d", mode);
+  if (N > (int64_t)0xfffffff0LL) return set_error(DSHT_ERR_INVALID, "too many points (%lld)", (long long)N);
   if (N == 0 && mode == DSHT_MODE_BASIC) return set_error(DSHT_ERR_EMPTY, "The theta array seems to be empty!");
   const int piece_max = plan_piece_max(p, N);
   const size_t need = workspace_layout(p->g, N, piece_max, nullptr, nullptr);

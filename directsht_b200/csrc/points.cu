@@ -284,7 +284,7 @@ gather_kernel(int64_t N, const uint32_t* __restrict__ total, const uint32_t* __r
 __global__ void __launch_bounds__(kPointThreads)
 piecemax_kernel(const double* __restrict__ pay, const int* __restrict__ npieces_p, int64_t pmax,
                 const int64_t* __restrict__ piece_start, const int* __restrict__ piece_len,
-                uint32_t* __restrict__ piecemax) {
+                uint32_t* __restrict__ piecemax, double* __restrict__ wsum) {
   const int lane = threadIdx.x & 31;
   const int64_t np = min((int64_t)*npieces_p, pmax);
   const int64_t wstride = (int64_t)gridDim.x * (blockDim.x >> 5);
@@ -292,6 +292,7 @@ piecemax_kernel(const double* __restrict__ pay, const int* __restrict__ npieces_
     const int64_t st = piece_start[pc];
     const int len = piece_len[pc];
     uint32_t mx = 0;
+    double ws = 0.0;
     const double2* base = reinterpret_cast<const double2*>(pay + (size_t)kRec * st) + 1;
     int i = lane;
     for (; i + 96 < len; i += 128) {  // four records in flight per lane
@@ -305,16 +306,24 @@ piecemax_kernel(const double* __restrict__ pay, const int* __restrict__ npieces_
       mx = max(mx, gmax_bits(h));
       hermite(d.y, d.x, h);
       mx = max(mx, gmax_bits(h));
+      ws += (fabs(a.x) + fabs(b.x)) + (fabs(c.x) + fabs(d.x));
     }
     for (; i < len; i += 32) {
       const double2 a = base[2 * i];
       double h[4];
       hermite(a.y, a.x, h);
       mx = max(mx, gmax_bits(h));
+      ws += fabs(a.x);
     }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    if (lane == 0) piecemax[pc] = mx;
+    for (int o = 16; o > 0; o >>= 1) {
+      mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      ws += __shfl_xor_sync(0xffffffffu, ws, o);
+    }
+    if (lane == 0) {
+      piecemax[pc] = mx;
+      wsum[pc] = ws;
+    }
   }
 }
 
@@ -376,7 +385,7 @@ void launch_piece_maxima(const Workspace& ws, cudaStream_t s) {
   if (blocks > 148 * 16) blocks = 148 * 16;
   if (blocks < 1) blocks = 1;
   piecemax_kernel<<<(unsigned)blocks, kPointThreads, 0, s>>>(ws.pay, ws.npieces, ws.pmax, ws.piece_start,
-                                                              ws.piece_len, ws.piecemax);
+                                                              ws.piece_len, ws.piecemax, ws.wsum);
   count_launches(1);
 }
 

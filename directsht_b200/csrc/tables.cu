@@ -6,19 +6,12 @@
 // Every product and sum is a separately rounded __dmul_rn/__dadd_rn in the reference's
 // order, so the tables come out as the numpy/numba path computes them.
 // Roofline: HBM write bound, 16 B written per (l, m, j).
-#include "dsht_internal.cuh"
+#include "recurrence.cuh"
 
 namespace dsht {
 namespace {
 
 constexpr int kTableThreads = 256;
-
-// Per-l coefficients of the column m, built once per block in shared memory:
-//   a = 2l-1, b = l+m-1, f2 = sqrt((l-m-1)/(l+m-1)), q = sqrt((l-m)/(l+m))/(l-m),
-//   dc = (l+m) * sqrt((l-m)/(l+m)), nrm = sqrt((2l+1)/4/pi)
-struct Coef {
-  double a, b, f2, q, dc, nrm;
-};
 
 // TO = double: the FP64 tables; TO = float: the same FP64 values rounded once to float.
 template <typename TO>
@@ -28,86 +21,34 @@ table_kernel(int Nl, int Nx, double step, TO* __restrict__ Yv, TO* __restrict__ 
   const int m = blockIdx.y;
   Coef* cf = reinterpret_cast<Coef*>(smem_raw);       // [Nl]
   double* smm = smem_raw + (size_t)Nl * 6;            // [m+1] sqrt(1 - 1/(2m'))
-  for (int l = threadIdx.x; l < Nl; l += blockDim.x) {
-    Coef c;
-    c.a = (double)(2 * l - 1);
-    c.b = (double)(l + m - 1);
-    c.f2 = (l >= m + 2) ? sqrt((double)(l - m - 1) / (double)(l + m - 1)) : 0.0;
-    double f1 = (l > m) ? sqrt((double)(l - m) / (double)(l + m)) : 0.0;
-    c.q = (l > m) ? f1 / (double)(l - m) : 0.0;
-    c.dc = (double)(l + m) * f1;
-    c.nrm = sqrt((double)(2 * l + 1) / 4.0 / M_PI);
-    cf[l] = c;
-  }
-  for (int k = threadIdx.x + 1; k <= m; k += blockDim.x) smm[k] = sqrt(1.0 - 1.0 / (double)(2 * k));
+  for (int l = threadIdx.x; l < Nl; l += blockDim.x) cf[l] = make_coef(l, m);
+  for (int k = threadIdx.x + 1; k <= m; k += blockDim.x) smm[k] = diag_factor(k);
   __syncthreads();
 
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= Nx) return;
-  const double x = (double)j * step;               // numpy: arange(Nx) * (xmax/(Nx-1))
-  const double x2 = __dmul_rn(x, x);
-  const double omx2 = __dadd_rn(1.0, -x2);
-  const double sx = sqrt(omx2);
-
-  // Y_mm by the diagonal recurrence (sht/legendre_py.py:28-30).
-  double ymm = 1.0;
-  for (int k = 1; k <= m; ++k) ymm = __dmul_rn(__dmul_rn(-smm[k], sx), ymm);
+  double x, omx2, sx;
+  node_x(j, step, &x, &omx2, &sx);               // numpy: arange(Nx) * (xmax/(Nx-1))
+  const double ymm = diag_value(m, sx, smm);     // Y_mm (sht/legendre_py.py:28-30)
 
   const int64_t row0 = hp_index(m, m, Nl);
   TO* yv = Yv + row0 * Nx + j;
   TO* yd = Yd + row0 * Nx + j;
-
-  // l = m
-  double y2 = 0.0, y1 = ymm;  // y2 = Y_{l-2}, y1 = Y_{l-1}
-  {
-    double d;
-    if (m == 0) {
-      d = 0.0;
-    } else {  // ((l+m) f1) Y_{l-1} with f1 = 0, minus (l x) Y_l, over 1-x^2
-      d = __ddiv_rn(__dadd_rn(0.0, -__dmul_rn(__dmul_rn((double)m, x), ymm)), omx2);
-    }
-    const double n = cf[m].nrm;
-    yv[0] = (TO)__dmul_rn(ymm, n);
-    yd[0] = (TO)__dmul_rn(d, n);
-  }
+  ColumnState st;
+  double y, d;
+  column_first(m, x, omx2, ymm, &st, &y, &d);
+  yv[0] = (TO)__dmul_rn(y, cf[m].nrm);
+  yd[0] = (TO)__dmul_rn(d, cf[m].nrm);
   if (m + 1 >= Nl) return;
-  // l = m + 1: Y = sqrt(2m+1) x Y_mm (sht/legendre_py.py:32-34); m = 0 row is x itself.
-  double y;
-  if (m == 0) {
-    y = x;
-  } else {
-    y = __dmul_rn(__dmul_rn(sqrt(2.0 * m + 1.0), x), ymm);
-  }
-  {
-    const int l = m + 1;
-    double d;
-    if (m == 0) {
-      d = 1.0;
-    } else {
-      d = __ddiv_rn(__dadd_rn(__dmul_rn(cf[l].dc, y1), -__dmul_rn(__dmul_rn((double)l, x), y)), omx2);
-    }
-    const double n = cf[l].nrm;
-    yv[(size_t)Nx] = (TO)__dmul_rn(y, n);
-    yd[(size_t)Nx] = (TO)__dmul_rn(d, n);
-  }
-  y2 = y1;
-  y1 = y;
+  column_second(m, cf[m + 1], &st, &y, &d);
+  yv[(size_t)Nx] = (TO)__dmul_rn(y, cf[m + 1].nrm);
+  yd[(size_t)Nx] = (TO)__dmul_rn(d, cf[m + 1].nrm);
   for (int l = m + 2; l < Nl; ++l) {
     const Coef c = cf[l];
-    // ((2l-1) x) Y_{l-1} - ((l+m-1) Y_{l-2}) f2, times f1/(l-m)  (sht/legendre_py.py:98-100)
-    double t = __dadd_rn(__dmul_rn(__dmul_rn(c.a, x), y1), -__dmul_rn(__dmul_rn(c.b, y2), c.f2));
-    y = __dmul_rn(t, c.q);
-    double d;
-    if (m == 0) {  // l/(1-x^2) (Y_{l-1} - x Y_l)  (sht/legendre_py.py:56)
-      d = __dmul_rn(__ddiv_rn((double)l, omx2), __dadd_rn(y1, -__dmul_rn(x, y)));
-    } else {       // ((l+m) f1 Y_{l-1} - l x Y_l) / (1-x^2)  (sht/legendre_py.py:115-116)
-      d = __ddiv_rn(__dadd_rn(__dmul_rn(c.dc, y1), -__dmul_rn(__dmul_rn((double)l, x), y)), omx2);
-    }
+    column_step(m, l, c, &st, &y, &d);
     const size_t off = (size_t)(l - m) * Nx;
     yv[off] = (TO)__dmul_rn(y, c.nrm);
     yd[off] = (TO)__dmul_rn(d, c.nrm);
-    y2 = y1;
-    y1 = y;
   }
 }
 
@@ -119,7 +60,28 @@ __global__ void to_f32_kernel(int64_t n, const double* __restrict__ a, const dou
   }
 }
 
+// out[m][k][j] = table row (l = m + k, m) at node j for k < Nl - m, else 0 (the JAX path's
+// Yv[m, l-m, :] layout with its unphysical entries nulled, sht/legendre_jax.py:14-25).
+// Grid: x over node chunks, y = k, z = m; consecutive threads take consecutive nodes.
+template <typename TI>
+__global__ void table_mlayout_kernel(int Nl, int Nx, const TI* __restrict__ t, double* __restrict__ out) {
+  const int m = blockIdx.z, k = blockIdx.y;
+  double* o = out + ((size_t)m * Nl + k) * Nx;
+  const TI* src = k < Nl - m ? t + (size_t)hp_index(m + k, m, Nl) * Nx : nullptr;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < Nx; j += gridDim.x * blockDim.x)
+    o[j] = src ? (double)src[j] : 0.0;
+}
+
 }  // namespace
+
+void launch_table_mlayout(const Geometry& g, const double* t64, const float* t32, double* out, cudaStream_t s) {
+  dim3 grid((g.Nx + 255) / 256 < 8 ? (g.Nx + 255) / 256 : 8, g.Nl, g.Nl);
+  if (t64)
+    table_mlayout_kernel<double><<<grid, 256, 0, s>>>(g.Nl, g.Nx, t64, out);
+  else
+    table_mlayout_kernel<float><<<grid, 256, 0, s>>>(g.Nl, g.Nx, t32, out);
+  count_launches(1);
+}
 
 void launch_tables_to_f32(const Geometry& g, const double* Yv, const double* Yd, float* Yv32, float* Yd32,
                           cudaStream_t s) {

@@ -29,14 +29,15 @@ class DirectSHT:
     """Brute-force spherical harmonic transforms on a B200 (``sht/sht.py:30``)."""
 
     def __init__(self, Nell, Nx, xmax=0.75, dflt_type="float64", null_unphysical=True, device=None,
-                 precision="fp64", f32_tables=False):
+                 precision="fp64", f32_tables=False, table_layout="healpix"):
         """Build the FP64 Ylm/dYlm tables on the GPU (``sht/sht.py:32-56``).
 
         :param Nell: number of ells (and m's).
         :param Nx: number of x = |cos theta| grid points in [0, xmax].
         :param xmax: largest |cos theta| handled without rotation.
         :param dflt_type: dtype of the host copy of the x grid (the tables are FP64).
-        :param null_unphysical: accepted for compatibility; rows l < m are never stored.
+        :param null_unphysical: accepted for compatibility; rows l < m are never stored, and
+            the JAX layout's unphysical entries (l >= Nell) always read as zero.
         :param device: CUDA device (default: the current one).
         :param precision: "fp64" (agrees with the reference to ~1e-15), "mixed" (tensor-core
             per-bin sums and FP32 tables: fastest, <= 1e-7 x max|alm| for point sets spread over
@@ -44,7 +45,13 @@ class DirectSHT:
             the weight concentrates in one bin).
         :param f32_tables: keep only FP32 copies of the tables (half the memory; the plan then
             runs at precision "mixed" only).
+        :param table_layout: layout of the host attributes ``Yv``/``Yd``: "healpix" (Nlm, Nx) rows
+            in Healpy order, as the reference's numpy path stores them, or "jax" (Nell, Nell, Nx)
+            indexed [m, ell - m, :], as its JAX path stores them (``sht/legendre_jax.py:14-25``).
         """
+        if table_layout not in ("healpix", "jax"):
+            raise ValueError(f"table_layout must be 'healpix' or 'jax', not {table_layout!r}")
+        self.table_layout = table_layout
         self._lib = L.load()
         if not torch.cuda.is_available():
             raise RuntimeError("DirectSHT (directsht_b200) needs a CUDA device; there is no CPU fallback")
@@ -119,14 +126,31 @@ class DirectSHT:
         return self._row(1, ell, m)
 
     def _table(self, which):
+        if self.table_layout == "jax":
+            out = np.empty((self.Nell, self.Nell, self.Nx), dtype=np.float64)
+            with torch.cuda.device(self.device):
+                L.check(self._lib.dsht_get_table_mlayout(self._plan, which, L.ptr(out), 0, None))
+            return out
         out = np.empty((self.Nlm, self.Nx), dtype=np.float64)
         with torch.cuda.device(self.device):
             L.check(self._lib.dsht_get_table(self._plan, which, L.dptr(out)))
         return out
 
+    def table_on_device(self, which="Yv"):
+        """A float64 CUDA tensor (Nell, Nell, Nx) of a table (``which`` = "Yv" or "Yd") in the
+        JAX path's layout [m, ell - m, :] (``sht/legendre_jax.py:14-25``), zero where ell >=
+        Nell, made on the device without passing through host memory."""
+        code = {"Yv": 0, "Yd": 1}[which]
+        out = torch.empty((self.Nell, self.Nell, self.Nx), dtype=torch.float64, device=self.device)
+        with torch.cuda.device(self.device):
+            stream = torch.cuda.current_stream(self.device).cuda_stream
+            L.check(self._lib.dsht_get_table_mlayout(self._plan, code, L.ptr(out), 1, ct.c_void_p(stream)))
+        return out
+
     @property
     def Yv(self):
-        """Host copy of the Ylm table, (Nlm, Nx) in Healpy row order (made on first use)."""
+        """Host copy of the Ylm table (made on first use): (Nlm, Nx) in Healpy row order, or
+        (Nell, Nell, Nx) indexed [m, ell - m] with table_layout="jax"."""
         if self._Yv is None:
             self._Yv = self._table(0)
         return self._Yv
@@ -139,9 +163,28 @@ class DirectSHT:
         return self._Yd
 
     def alm2cl(self, alm):
-        """1/(2l+1) sum_m |alm|^2 (``sht/sht.py:95-109``)."""
+        """1/(2l+1) sum_m |alm|^2 (``sht/sht.py:95-109``).
+
+        A numpy alm gives a numpy spectrum (computed on the host).  A CUDA tensor of complex128
+        alm, shape (Nlm,) or (nmaps, Nlm), is reduced on its device without a copy to the host
+        and gives a CUDA float64 tensor of shape (Nell,) or (nmaps, Nell)."""
+        if isinstance(alm, torch.Tensor) and alm.is_cuda:
+            a = alm.detach()
+            if a.dtype != torch.complex128:
+                a = a.to(torch.complex128)
+            squeeze = a.dim() == 1
+            a = a.reshape(-1, a.shape[-1])
+            if a.shape[-1] != self.Nlm:
+                raise ValueError(f"alm has {a.shape[-1]} entries per map, expected Nlm={self.Nlm}")
+            a = a.contiguous()
+            cl = torch.empty((a.shape[0], self.Nell), dtype=torch.float64, device=a.device)
+            with torch.cuda.device(a.device):
+                stream = torch.cuda.current_stream(a.device).cuda_stream
+                L.check(self._lib.dsht_alm2cl_device(self.Nell, a.shape[0], L.ptr(a), 2 * self.Nlm, L.ptr(cl),
+                                                     ct.c_void_p(stream)))
+            return cl[0] if squeeze else cl
         if isinstance(alm, torch.Tensor):
-            alm = alm.detach().cpu().numpy()
+            alm = alm.detach().numpy()
         a = np.ascontiguousarray(np.asarray(alm, dtype=np.complex128))
         cl = np.zeros(self.Nell)
         L.check(self._lib.dsht_alm2cl(self.Nell, a.view(np.float64).ctypes.data_as(ct.POINTER(ct.c_double)),
@@ -188,8 +231,9 @@ class DirectSHT:
         L.check(rc)
         return alm
 
-    def call_maps(self, t, p, wts):
-        """alm of several weight maps on one point set: row k is ``self(t, p, wts[k])``.
+    def call_maps(self, t, p, wts, mode="call"):
+        """alm of several weight maps on one point set: row k is ``self(t, p, wts[k])``
+        (or ``self.basic_sht(t, p, wts[k])`` with mode="basic").
 
         The reference has no multi-map call; its users loop ``__call__``
         (``sht/sht.py:112-150``) over the maps.  ``wts`` has shape (nmaps, N), float64 or
@@ -219,14 +263,17 @@ class DirectSHT:
             L.check(self._lib.dsht_workspace_size_maps(self._plan, n, nmaps, ct.byref(nbytes)))
             ws = torch.empty(max(int(nbytes.value), 1), dtype=torch.uint8, device=self.device)
             stream = torch.cuda.current_stream(self.device).cuda_stream
+            code = L.DSHT_MODE_CALL if mode == "call" else L.DSHT_MODE_BASIC
             rc = self._lib.dsht_execute_maps(self._plan, L.ptr(td), L.ptr(pd), L.ptr(wd), dtype, n, nmaps,
-                                             wd.stride(0), L.DSHT_MODE_CALL, L.ptr(alm), L.ptr(ws), ws.numel(),
+                                             wd.stride(0), code, L.ptr(alm), L.ptr(ws), ws.numel(),
                                              ct.c_void_p(stream))
         if rc == L.DSHT_ERR_POLAR_RANGE:
             print(f"AssertionError in basic_sht: theta must be in [ACos[xmax],ACos[-xmax]).")
             alm.zero_()
         elif rc == L.DSHT_ERR_THETA_RANGE:
             raise AssertionError("theta must be in [ACos[xmax],ACos[-xmax]).")
+        elif rc == L.DSHT_ERR_EMPTY:
+            raise ValueError("The theta array seems to be empty!")
         else:
             L.check(rc)
         return alm if on_device else alm.cpu().numpy()

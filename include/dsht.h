@@ -186,7 +186,11 @@ int dsht_rotate_back(dsht_plan_t plan, const double* alm_rot, const double* alm_
  * cudaMalloc/cudaFree.  Same arguments and results as dsht_execute (DEVICE pointers), but
  * all scratch lives in one fixed device array of dsht_noalloc_scratch_bytes() = 64 MiB
  * that every GPU loading this library holds until exit; problems whose workspace is larger
- * (e.g. beyond Nl=256, Nx=512, N=1e5) return DSHT_ERR_NOMEM.  The first call on a device
+ * return DSHT_ERR_NOMEM.  With the default piece size, Nl=256, Nx=512, N=1e5 fits (63.8 MB);
+ * a plan tuned to smaller pieces (DSHT_TUNE_PIECE_MAX) needs more: check a problem with
+ * dsht_workspace_size(plan, N) <= dsht_noalloc_scratch_bytes() beforehand.  Like
+ * dsht_execute, each call waits for its stream once at the end to read the error flags,
+ * and N is limited to 0xfffffff0 points.  The first call on a device
  * looks up the array's device address and should come before any stream capture.  All
  * calls share the array (it keeps the last call's contents; what must start at zero is
  * cleared), so calls that overlap on the GPU race and must be serialised by the caller. */
@@ -205,9 +209,23 @@ int dsht_get_row(dsht_plan_t plan, int which, int ell, int m, double* out);
 /* Whole table (Nlm x Nx doubles) to a HOST buffer. */
 int dsht_get_table(dsht_plan_t plan, int which, double* out);
 
+/* Whole table in the JAX path's layout, out[m][l - m][j] (Nl x Nl x Nx doubles), with the
+ * entries l >= Nl set to zero (null_unphysical).  Replaces the (Nell, Nell, Nx) Yv/Yd
+ * attributes of DirectSHT when JAX is present (sht/sht.py:49-55, sht/legendre_jax.py:14-25;
+ * get_Ylm reads Yv[m, ell-m, :] there, sht/sht.py:77-80).  out_on_device = 0: out is a HOST
+ * buffer (synchronous); 1: a DEVICE buffer, filled by a kernel on `stream`. */
+int dsht_get_table_mlayout(dsht_plan_t plan, int which, double* out, int out_on_device, void* stream);
+
 /* Pseudo-spectrum cl[l] = (|a_l0|^2 + 2 sum_{m>0} |a_lm|^2)/(2l+1) of a HOST alm vector.
  * Replaces DirectSHT.alm2cl (sht/sht.py:95-109). */
 int dsht_alm2cl(int Nl, const double* alm, double* cl);
+
+/* The same pseudo-spectrum for nmaps alm vectors already on the device, without copying
+ * them to the host.  alm: DEVICE pointer, map k at alm + k * alm_stride doubles (each 2*Nlm
+ * doubles, complex128 Healpy order); cl: DEVICE pointer to nmaps * Nl doubles, map k's
+ * spectrum at cl + k * Nl.  Stream-ordered on `stream` (NULL = default), no synchronisation.
+ * Replaces DirectSHT.alm2cl (sht/sht.py:95-109) for device-resident alm. */
+int dsht_alm2cl_device(int Nl, int nmaps, const double* alm, int64_t alm_stride, double* cl, void* stream);
 
 /* Drop-ins for the reference's ctypes library csht/sht_helper.so (HOST arrays).
  * dsht_make_table fills Yv, Yd (Nlm*Nx doubles each) like make_table
@@ -221,11 +239,13 @@ int dsht_make_table(int Nl, int Nx, double xmax, double* Yv, double* Yd);
 int dsht_do_transform(int Nl, int Nx, double xmax, double* Yv, double* Yd, int Np,
                       double* cost, double* phi, double* wt, double* carr, double* sarr);
 
-/* Stage timers (CUDA events recorded on the execute stream around every stage).
- * Stages: 0 points+sort, 1 bin sums, 2 fold, 3 contraction, 4 rotation.  For
- * dsht_execute_maps: stage 0 is the one sort, stages 1-2 are those of the last map
- * (stage 1 including its payload gather), stage 3 is the last contraction pass (it serves
- * up to 4 maps) and stage 4 the rotation of all maps. */
+/* Stage timers (CUDA events recorded on the execute stream at every stage boundary).
+ * Stages: 0 points+sort, 1 bin sums, 2 fold, 3 contraction, 4 rotation.  Each stage's time
+ * is the sum over all its launches in the call: for multi-map and batch calls stage 0 is
+ * every sort, stage 1 every bin-sum launch (with the weight gathers of later maps), stage 2
+ * every fold, stage 3 every contraction pass and stage 4 every rotation.  Timed only for
+ * the synchronising entry points (dsht_execute*, not dsht_enqueue_*); calls on one plan must
+ * not overlap while profiling. */
 enum { DSHT_STAGE_POINTS = 0, DSHT_STAGE_BIN_SUMS = 1, DSHT_STAGE_FOLD = 2, DSHT_STAGE_CONTRACT = 3,
        DSHT_STAGE_ROTATE = 4, DSHT_STAGE_COUNT = 5 };
 int dsht_profile_enable(dsht_plan_t plan, int enable);

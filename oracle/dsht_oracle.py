@@ -384,6 +384,41 @@ def rotate_alm_back(alm_rot: np.ndarray, Nl: int) -> np.ndarray:
     return out
 
 
+class AlmRotator:
+    """``rotate_alm_back`` with the d^l(pi/2) matrices computed once (the CPU baseline's
+    stand-in for healpy's ``rotate_alm`` inside its timed region).
+
+    For each l the sums of ``rotate_alm_back`` split by the parities of k and m: with
+    p = l % 2, Re a_lm takes k = m + p (mod 2) and Im a_lm the other k, so each l is four
+    dense matrix-vector products over strided views of one stored matrix."""
+
+    def __init__(self, Nl: int):
+        self.Nl = Nl
+        self.D = [wigner_d_halfpi_column(ell) for ell in range(Nl)]
+
+    def __call__(self, alm_rot: np.ndarray) -> np.ndarray:
+        Nl = self.Nl
+        out = np.zeros_like(alm_rot)
+        for ell in range(Nl):
+            idx = healpy_index(ell, np.arange(ell + 1), Nl)
+            a = alm_rot[idx]
+            D = self.D[ell]
+            wre = a.real.copy()
+            wre[1:] *= 2.0
+            wim = 2.0 * a.imag
+            wim[0] = 0.0
+            re = np.empty(ell + 1)
+            im = np.empty(ell + 1)
+            p = ell % 2
+            for mp in (0, 1):              # parity of m
+                ke = (mp + p) % 2          # k parity of the real part (l + m + k even)
+                ko = 1 - ke
+                re[mp::2] = wre[ke::2] @ D[ke::2, mp::2]
+                im[mp::2] = wim[ko::2] @ D[ko::2, mp::2]
+            out[idx] = re + 1j * im
+        return out
+
+
 def direct_sht(tab: Tables, t, p, w) -> np.ndarray:
     """``DirectSHT.__call__`` (``sht/sht.py:112-150``): polar/equatorial split,
     rotation of the polar points, transform, rotation of their alm back."""

@@ -10,7 +10,7 @@ from __future__ import annotations
 import numpy as np
 
 CASES = {
-    # full sky, Nl=256, Nx=512, N=1e5, w=1, seed 0.
+    # Full sky, Nl=256, Nx=512, N=1e5, w=1, seed 0 (the CPU-runnable reference case).
     "c1_full_sky": dict(Nl=256, Nx=512, N=100_000, seed=0, kind="full", wkind="ones", entry="call"),
     "small_call": dict(Nl=48, Nx=96, N=3000, seed=1, kind="full", wkind="uniform", entry="call"),
     "small_basic_mixed_sign": dict(Nl=32, Nx=64, N=2000, seed=2, kind="band", lo=-0.74, hi=0.74,

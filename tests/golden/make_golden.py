@@ -7,7 +7,7 @@ for its polar branch, and saves inputs and outputs as compressed .npz files.  In
 are regenerated from their seeds by ``tests/golden/inputs.py`` so that the fixtures
 stay small.  Needs the reference checkout; the fixtures it writes are committed.
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py --ref <reference checkout>   (or DSHT_REFERENCE=<checkout>)
 """
 from __future__ import annotations
 
@@ -36,9 +36,12 @@ def _quiet(fn, *a, **k):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("DSHT_REFERENCE"),
+                    help="the reference checkout (default: $DSHT_REFERENCE)")
     ap.add_argument("--skip-c1", action="store_true")
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("give the reference checkout with --ref or DSHT_REFERENCE")
     sys.path.insert(0, args.ref)
     with contextlib.redirect_stdout(io.StringIO()):
         from sht.sht import DirectSHT  # noqa: E402

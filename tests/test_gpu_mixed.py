@@ -80,20 +80,86 @@ def test_mixed_heavy_bin_and_wide_weights():
     w = rng.lognormal(0.0, 1.0, N)
     d = DirectSHT(256, 512)
     ref = d.basic_sht(th, ph, w.copy(), verbose=False)
-    # Half of the weight sits in one bin: the FP32 table rounding does not average out, so
-    # the level with FP64 tables is the one held to 1e-7; the FP32-table level stays within
-    # a few 1e-7.
-    d.set_precision("mixed_f64_tables")
+    # Half of the weight sits in one bin: the FP32-table level contracts that bin's two
+    # nodes in FP64 (heavy nodes), so both levels hold 1e-7.
+    for level in ("mixed_f64_tables", "mixed"):
+        d.set_precision(level)
+        a = d.basic_sht(th, ph, w.copy(), verbose=False)
+        assert _rel(a, ref) <= TOL_MIXED, level
+
+
+def _oracle_basic(Nl, Nx, th, ph, w):
+    return O.basic_sht(O.build_tables(Nl, Nx), th, ph, w)
+
+
+@pytest.mark.parametrize("case", ["one_bin", "dominant_bin", "two_bins_signed", "few_points"])
+def test_mixed_concentrated_weight_vs_oracle(case):
+    """Weight concentrated at a few nodes, against the oracle: the FP32-table level holds
+    1e-7 because the heavy nodes are contracted in FP64 with regenerated table values."""
+    rng = np.random.default_rng(11)
+    Nl, Nx = 200, 400
+    if case == "one_bin":          # every point in one x bin
+        N = 30000
+        cost = rng.uniform(0.5001, 0.5006, N)
+        w = rng.uniform(0.5, 1.5, N)
+    elif case == "dominant_bin":    # a fifth of the points in one bin, the rest spread
+        N = 40000
+        cost = np.concatenate([rng.uniform(-0.1502, -0.15, N // 5), rng.uniform(-0.74, 0.74, N - N // 5)])
+        w = rng.lognormal(0.0, 0.5, N)
+    elif case == "two_bins_signed":  # two bins on either side of the equator, signed weights
+        N = 20000
+        cost = np.concatenate([rng.uniform(0.3, 0.3004, N // 2), rng.uniform(-0.6004, -0.6, N // 2)])
+        w = rng.normal(1.0, 2.0, N)
+    else:                           # fewer points than the tensor-core threshold
+        N = 300
+        cost = rng.uniform(-0.2, 0.2, N)
+        w = rng.uniform(0.5, 1.5, N)
+    th = np.arccos(cost)
+    ph = rng.uniform(0, 2 * np.pi, N)
+    ref = _oracle_basic(Nl, Nx, th, ph, w)
+    for kwargs in (dict(precision="mixed"), dict(f32_tables=True)):
+        d = DirectSHT(Nl, Nx, **kwargs)
+        a = d.basic_sht(th, ph, w.copy(), verbose=False)
+        assert _rel(a, ref) <= TOL_MIXED, (case, kwargs)
+
+
+@pytest.mark.parametrize("N,seed", [(1, 0), (700, 1), (5000, 2)])
+def test_f32_only_plan_few_points_call_vs_oracle(N, seed):
+    """An FP32-only plan (no FP64 tables at all) on a handful of points, polar ones
+    included: every node is heavy, so the result is FP64 throughout."""
+    rng = np.random.default_rng(seed)
+    Nl, Nx = 96, 192
+    th = np.arccos(rng.uniform(-1, 1, N))
+    ph = rng.uniform(0, 2 * np.pi, N)
+    w = rng.uniform(0.5, 1.5, N)
+    ref = O.direct_sht(O.build_tables(Nl, Nx), th, ph, w)
+    d = DirectSHT(Nl, Nx, f32_tables=True)
+    assert _rel(d(th, ph, w), ref) <= TOL_MIXED
+
+
+@pytest.mark.slow
+def test_f32_only_plan_nl2048_concentrated_columns_vs_oracle():
+    """Nl=2048, Nx=4096 with FP32 tables only (68.7 GB, the uneven-batch and serving plans at
+    that size): 40 % of the weight in one bin, the rest spread; columns against the per-m
+    oracle."""
+    rng = np.random.default_rng(12)
+    Nl, Nx, N = 2048, 4096, 400_000
+    cost = np.concatenate([rng.uniform(0.2000, 0.2001, 2 * N // 5), rng.uniform(-0.74, 0.74, N - 2 * N // 5)])
+    th = np.arccos(cost)
+    ph = rng.uniform(0, 2 * np.pi, N)
+    w = rng.uniform(0.5, 1.5, N)
+    d = DirectSHT(Nl, Nx, f32_tables=True)
     a = d.basic_sht(th, ph, w.copy(), verbose=False)
-    assert _rel(a, ref) <= TOL_MIXED
-    d.set_precision("mixed")
-    a = d.basic_sht(th, ph, w.copy(), verbose=False)
-    assert _rel(a, ref) <= 5 * TOL_MIXED
+    cols = {m: O.basic_sht_column(Nl, Nx, 0.75, m, th, ph, w) for m in (0, 1, 2, 700, 1500, 2047)}
+    scale = max(np.abs(c).max() for c in cols.values())
+    for m, col in cols.items():
+        r0 = O.healpy_index(m, m, Nl)
+        assert np.abs(a[r0:r0 + Nl - m] - col).max() <= TOL_MIXED * scale, m
 
 
 @pytest.mark.slow
 def test_mixed_c2_full_size():
-    """Nl=1024, Nx=2048, N=1e7 -- mixed within 1e-7 of FP64."""
+    """Survey-like single map, Nl=1024, Nx=2048, N=1e7: mixed within 1e-7 of FP64."""
     rng = np.random.default_rng(0)
     N = 10_000_000
     th = np.arccos(rng.uniform(np.cos(1.2), np.cos(0.3), N))

@@ -47,6 +47,26 @@ def test_full_tables_match_oracle():
     assert _rel(d.Yd, tab.Yd) <= 1e-14
 
 
+@pytest.mark.parametrize("f32_tables", [False, True])
+def test_jax_layout_tables(f32_tables):
+    """Yv/Yd in the JAX path's [m, l-m, :] layout with the unphysical entries nulled
+    (sht/legendre_jax.py:14-25): the same rows as the Healpy-order tables, host and device."""
+    Nl, Nx = 70, 132
+    d = DirectSHT(Nl, Nx, table_layout="jax", f32_tables=f32_tables)
+    tab = O.build_tables(Nl, Nx)
+    for which, ref, host in (("Yv", tab.Yv, d.Yv), ("Yd", tab.Yd, d.Yd)):
+        assert host.shape == (Nl, Nl, Nx)
+        dev = d.table_on_device(which).cpu().numpy()
+        assert np.array_equal(dev, host)
+        tol = 1e-7 if f32_tables else 1e-14
+        for m in range(Nl):
+            r0 = O.healpy_index(m, m, Nl)
+            assert _rel(host[m, :Nl - m], ref[r0:r0 + Nl - m]) <= tol, (which, m)
+            assert not np.any(host[m, Nl - m:])
+    # get_Ylm is layout independent (sht/sht.py:69-93)
+    assert np.array_equal(d.get_Ylm(5, 3), d.Yv[3, 2])
+
+
 @pytest.mark.parametrize("name", list(I.CASES))
 def test_golden_cases(name):
     s = I.CASES[name]
@@ -60,6 +80,31 @@ def test_golden_cases(name):
     assert a.dtype == np.complex128 and a.shape == (d.Nlm,)
     assert _rel(a, g["alm"]) <= TOL_FP64
     np.testing.assert_allclose(d.alm2cl(a), g["cl"], rtol=1e-10, atol=1e-13 * np.abs(g["alm"]).max() ** 2)
+
+
+@pytest.mark.parametrize("name", ["c1_full_sky", "small_call", "cap_c2like", "single_point", "xmax_0p8"])
+def test_alm2cl_on_device_matches_reference_golden(name):
+    """DirectSHT.alm2cl of device alm (dsht_alm2cl_device) against the cl the reference's own
+    alm2cl (sht/sht.py:95-109) produced for the same case; the alm never leave the GPU."""
+    s = I.CASES[name]
+    g = _golden(name)
+    th, ph, w = I.make_inputs(name)
+    d = DirectSHT(s["Nl"], s["Nx"], s.get("xmax", 0.75))
+    dev = [torch.from_numpy(x).cuda() for x in (th, ph, w)]
+    if s["entry"] == "call":
+        a = d(*dev)
+    else:
+        a = d.basic_sht(dev[0], dev[1], dev[2].clone(), reg_factor=s.get("reg", 1.0), verbose=False)
+    assert a.is_cuda
+    cl = d.alm2cl(a)
+    assert cl.is_cuda and cl.dtype == torch.float64 and cl.shape == (d.Nell,)
+    scale = np.abs(g["alm"]).max() ** 2
+    np.testing.assert_allclose(cl.cpu().numpy(), g["cl"], rtol=1e-10, atol=1e-13 * scale)
+    # several maps at once: rows of a (nmaps, Nlm) tensor, each the single-map spectrum
+    two = torch.stack([a, 2.0 * a])
+    cl2 = d.alm2cl(two).cpu().numpy()
+    np.testing.assert_allclose(cl2[0], cl.cpu().numpy(), rtol=1e-15, atol=0)
+    np.testing.assert_allclose(cl2[1], 4.0 * cl.cpu().numpy(), rtol=1e-14, atol=0)
 
 
 @pytest.mark.parametrize("Nl,Nx,N,seed", [(1, 2, 10, 0), (2, 3, 50, 1), (3, 5, 1, 2), (37, 50, 1000, 3),
@@ -208,7 +253,7 @@ def test_do_transform_drop_in_matches_reference_c():
     assert np.abs(sarr - sref).max() <= 1e-12 * scale
 
 
-# ---- full size: BASELINE config 2 (Nl=1024, Nx=2048, N=1e7) ----------------------------
+# ---- full size: survey-like single map (Nl=1024, Nx=2048, N=1e7) ------------------------
 def _c2_points(N, seed=0):
     rng = np.random.default_rng(seed)
     th = np.arccos(rng.uniform(np.cos(1.2), np.cos(0.3), N))

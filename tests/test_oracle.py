@@ -32,7 +32,7 @@ def test_oracle_matches_reference_golden(name):
 
 
 def test_oracle_matches_reference_c1():
-    """BASELINE config 1 (Nl=256, Nx=512, N=1e5 full sky) through the reference's __call__."""
+    """Full sky, Nl=256, Nx=512, N=1e5, unit weights, seed 0, through the reference's __call__."""
     g = _golden("c1_full_sky")
     a = _oracle_alm("c1_full_sky")
     assert np.abs(a - g["alm"]).max() <= 1e-13 * np.abs(g["alm"]).max()
@@ -123,6 +123,16 @@ def test_rotation_matches_exact_definition(seed):
     # the rotated polar points land inside the table range
     pol = np.abs(np.cos(th)) >= 0.75
     assert np.all(np.abs(np.cos(t2[pol])) < 0.75)
+
+
+@pytest.mark.parametrize("Nl", [1, 2, 5, 40, 97])
+def test_precomputed_rotator_matches_rotate_alm_back(Nl):
+    """AlmRotator (the CPU baseline's timed alm rotation) is rotate_alm_back regrouped."""
+    rng = np.random.default_rng(Nl)
+    Nlm = Nl * (Nl + 1) // 2
+    a = rng.normal(size=Nlm) + 1j * rng.normal(size=Nlm)
+    ref = O.rotate_alm_back(a, Nl)
+    assert np.abs(O.AlmRotator(Nl)(a) - ref).max() <= 1e-14 * np.abs(ref).max()
 
 
 def test_direct_sht_matches_exact_definition():

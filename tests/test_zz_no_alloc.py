@@ -20,6 +20,7 @@ from directsht_b200 import _lib as L
 pytestmark = pytest.mark.gpu
 
 TOL_FP64 = 1e-12
+TOL_MIXED = 1e-7
 
 
 def _points(N, seed):
@@ -52,12 +53,27 @@ def _no_alloc(lib, d, th, ph, w):
 def test_no_alloc_matches_execute_on_two_calls_in_a_row():
     lib = L.load()
     assert lib.dsht_noalloc_scratch_bytes() == 64 << 20
-    d = DirectSHT(256, 512)  # BASELINE config 1 sizes: fits the fixed scratch
+    d = DirectSHT(256, 512)  # Nl=256, Nx=512, N=1e5 fits the fixed scratch
     for seed, N in ((0, 100_000), (1, 37_000)):  # two calls, different sizes, back to back
         th, ph, w = _points(N, seed)
         ref = _with_workspace(lib, d, th, ph, w)
         got = _no_alloc(lib, d, th, ph, w)
         assert np.abs(got - ref).max() <= TOL_FP64 * np.abs(ref).max()
+
+
+def test_no_alloc_mixed_precision_two_calls():
+    """The tensor-core level keeps FP32 partial sums and piece maxima in the same fixed
+    array; its results equal dsht_execute's on the same plan within the mixed tolerance."""
+    lib = L.load()
+    d = DirectSHT(256, 512, precision="mixed")
+    for seed, N in ((3, 100_000), (4, 52_000)):
+        th, ph, w = _points(N, seed)
+        nb = ct.c_size_t()
+        L.check(lib.dsht_workspace_size(d._plan, N, ct.byref(nb)))
+        assert nb.value <= lib.dsht_noalloc_scratch_bytes()
+        ref = _with_workspace(lib, d, th, ph, w)
+        got = _no_alloc(lib, d, th, ph, w)
+        assert np.abs(got - ref).max() <= TOL_MIXED * np.abs(ref).max()
 
 
 def test_no_alloc_rejects_problems_beyond_its_scratch():
