@@ -279,7 +279,7 @@ def run_batch(args, spec):
     lib = L.load()
     ts = batch_transforms(spec, seed=rank)
     t0 = time.time()
-    cache = PlanCache(device=dev, precision="mixed", f32_tables_min_nl=1024)
+    cache = PlanCache(device=dev, precision="mixed", compact_min_nl=1024)
     for Nl in spec["nls"]:
         cache.get(Nl, 2 * Nl)
     t_plans = time.time() - t0
@@ -361,7 +361,7 @@ def run_batch(args, spec):
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "i8 tensor sums + f32 tables + f64", "data": "synthetic",
                 "config": {"workload": spec["name"], "transforms": len(ts), "points": int(sum(b.Ns)),
-                           "points_ell": pe, "precision": "mixed (FP32-only tables for Nl >= 1024)",
+                           "points_ell": pe, "precision": "mixed (compact digit tables only for Nl >= 1024)",
                            "l2": "inputs (GBs) and tables (79 GB) exceed L2", "parallelism": f"replicas x{world}",
                            "groups": groups},
                 "p50_ms": float(np.percentile(per_step, 50)), "p99_ms": float(np.percentile(per_step, 99)),
@@ -383,7 +383,7 @@ def run_serve(args, spec):
     world, rank, local, dev = _dist_setup()
     lib = L.load()
     t0 = time.time()
-    cache = PlanCache(device=dev, precision="mixed", f32_tables_min_nl=1024)
+    cache = PlanCache(device=dev, precision="mixed", compact_min_nl=1024)
     for Nl in spec["nls"]:
         cache.get(Nl, 2 * Nl)
     t_plans = time.time() - t0
@@ -628,7 +628,9 @@ def main(argv=None):
     f32_tables = args.precision == "mixed"
     # Stage times sum every launch of the step: with several maps, bin sums, fold and rotation
     # ran once per map and the contraction once per pass of maps_per_pass maps.
-    per_pass = d.tune()["maps_per_pass"] or 2 if maps > 1 else 1
+    # maps per contraction pass: the tensor-core contraction serves up to 8 per table read,
+    # the FP64 CUDA-core contraction one
+    per_pass = (d.tune()["maps_per_pass"] or (8 if args.precision == "mixed" else 1)) if maps > 1 else 1
     passes = -(-maps // per_pass)
 
     def stage_roof(name, ms):
@@ -640,9 +642,11 @@ def main(argv=None):
             eb = 4 if f32_tables else 8
             alg = 2.0 * eb * d.Nlm * Nx * passes
             a = alg / (ms * 1e-3) / 1e9
-            return {"kernel": "contract_stream_kernel (TMA 2D tensor-map tiles)", "bound": "hbm", "achieved": a,
+            kern = ("contract_tc_kernel (tcgen05 kind::i8 on 4-byte digit tables, TMA 3D boxes)" if f32_tables
+                    else "contract_stream_kernel (FP64 tables, TMA 2D tiles)")
+            return {"kernel": kern, "bound": "hbm", "achieved": a,
                     "peak": hbm_peak, "unit": "GB/s", "frac": a / hbm_peak, "peak_source": peak_src,
-                    "algorithmic": f"{2 * eb} B of {'FP32' if f32_tables else 'FP64'} table (Yv, Yd) per "
+                    "algorithmic": f"{2 * eb} B of {'digit' if f32_tables else 'FP64'} table (Yv, Yd) per "
                                    f"(l, m, node) per pass ({passes} passes)"}
         if name == "points":
             alg = 56.0 * N

@@ -5,10 +5,11 @@ and has no batch layer; this module is the B200 batch runner around the library'
 ``dsht_enqueue_batch``:
 
 * one plan per (Nl, Nx, xmax) stays resident (``PlanCache``); plans whose FP64 tables would
-  not fit keep FP32 tables only;
+  not fit keep the compact 4-byte fixed-point tables only;
 * the transforms of one plan are dealt into sub-batches (largest first, balanced by points)
-  that run on their own CUDA streams; inside a sub-batch the library shares one read of the
-  tables between up to four transforms and one rotation recursion between up to eight;
+  that run on their own CUDA streams; inside a sub-batch the library's tensor-core
+  contraction shares one read of the tables between up to eight transforms, and one
+  rotation recursion serves them all;
 * the whole batch is enqueued without any host synchronisation, so it can be captured once
   into a CUDA graph and replayed with a single launch (``TransformBatch.capture``);
 * ``autotune`` picks, per plan, the piece size of the bin sums, the maps per contraction
@@ -31,23 +32,30 @@ from . import _lib as L
 from .sht import DirectSHT
 
 
-def table_bytes(Nl: int, Nx: int, f32: bool) -> int:
-    """Device bytes of a plan's two tables."""
-    return 2 * (Nl * (Nl + 1) // 2) * Nx * (4 if f32 else 8)
+def table_bytes(Nl: int, Nx: int, compact: bool, mixed: bool = False) -> int:
+    """Device bytes of a plan's tables: the FP64 pair (16 B per entry pair) unless compact,
+    plus the 4-byte fixed-point digit tables (4 planes of 2 Nx bytes per row, rounded up to
+    64) when the plan is compact or runs at the mixed level."""
+    nlm = Nl * (Nl + 1) // 2
+    digits = 4 * nlm * ((2 * Nx + 63) // 64 * 64)
+    if compact:
+        return digits
+    return 2 * nlm * Nx * 8 + (digits if mixed else 0)
 
 
 class PlanCache:
     """Resident plans keyed by (Nl, Nx, xmax) on one device.
 
-    ``f32_tables_min_nl``: plans with Nl at or above it keep FP32 tables only (at Nl=2048,
-    Nx=4096 the FP64 pair alone is 137 GB).  Plans are built on first use and kept.
+    ``compact_min_nl``: plans with Nl at or above it keep the compact (4-byte fixed-point)
+    tables only (at Nl=2048, Nx=4096 the FP64 pair alone is 137 GB, the compact tables 69 GB).
+    Plans are built on first use and kept.
     """
 
-    def __init__(self, device=None, precision="mixed", f32_tables_min_nl=2048):
+    def __init__(self, device=None, precision="mixed", compact_min_nl=2048):
         self.device = torch.device("cuda", torch.cuda.current_device() if device is None
                                    else torch.device(device).index or 0)
         self.precision = precision
-        self.f32_tables_min_nl = f32_tables_min_nl
+        self.compact_min_nl = compact_min_nl
         self._plans: dict = {}
         self._lock = threading.Lock()
 
@@ -56,13 +64,13 @@ class PlanCache:
         with self._lock:
             d = self._plans.get(key)
             if d is None:
-                f32 = self.precision == "mixed" and Nl >= self.f32_tables_min_nl and Nx % 4 == 0
-                d = DirectSHT(Nl, Nx, xmax, device=self.device, precision=self.precision, f32_tables=f32)
+                compact = self.precision == "mixed" and Nl >= self.compact_min_nl and Nx <= 8192
+                d = DirectSHT(Nl, Nx, xmax, device=self.device, precision=self.precision, compact_tables=compact)
                 self._plans[key] = d
             return d
 
     def resident_bytes(self) -> int:
-        return sum(table_bytes(d.Nell, d.Nx, d._f32_only) for d in self._plans.values())
+        return sum(table_bytes(d.Nell, d.Nx, d._f32_only, d.precision == "mixed") for d in self._plans.values())
 
     def plans(self):
         return dict(self._plans)
@@ -243,7 +251,7 @@ def autotune(batch: TransformBatch, path: str | None = None, reps: int = 2, verb
         f32 = plan.precision == "mixed"
         n = len(batch.groups[key])
         pieces = [0, 512, 1024, 2048]
-        per_pass = [3, 2] if f32 else [0]
+        per_pass = [0, 4] if f32 else [0]  # mixed plans: 8 (0) or 4 transforms per table read
         streams = [s for s in (1, 2, 4) if s <= n]
         best = None
         for pm, mp, ns in itertools.product(pieces, per_pass, streams):

@@ -63,7 +63,7 @@ int default_piece_max(const Geometry& g, int64_t N) {
 }
 
 size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* base, Workspace* ws, int fold_slots,
-                        bool multi) {
+                        bool multi, int tc_maps) {
   size_t off = 0;
   auto take = [&](size_t bytes) -> uint8_t* {
     uint8_t* p = base ? base + off : nullptr;
@@ -104,7 +104,12 @@ size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* ba
   w.heavy_flag = reinterpret_cast<uint8_t*>(take(2 * (size_t)g.Nx * w.fold_slots));
   w.heavy_list = reinterpret_cast<int*>(take(sizeof(int) * (size_t)kHeavyMax * w.fold_slots));
   w.heavy_n = reinterpret_cast<int*>(take(sizeof(int) * w.fold_slots));
-  w.fold = reinterpret_cast<double*>(take(sizeof(double) * 16 * (size_t)g.Nl * g.Nx * w.fold_slots));
+  // The tensor-core route's fold digits ([Nl][2][4][4 tc_maps][Kp] int8) use the same region.
+  w.tc_maps = std::max(1, std::min(tc_maps, kTcMaxMaps));
+  const size_t fold_bytes = sizeof(double) * 16 * (size_t)g.Nl * g.Nx * w.fold_slots;
+  const size_t fdig_bytes = (size_t)g.Nl * 8 * 4 * w.tc_maps * (size_t)digit_kp(g.Nx);
+  w.fold = reinterpret_cast<double*>(take(std::max(fold_bytes, fdig_bytes)));
+  w.cexp = reinterpret_cast<int16_t*>(take(sizeof(int16_t) * 2 * w.tc_maps));
   w.tile_live = reinterpret_cast<uint8_t*>(take(2 * (size_t)ntile));
   w.tile_live2 = reinterpret_cast<uint8_t*>(take(2 * (size_t)((g.Nx + 255) / 256)));
   w.alm_equ = reinterpret_cast<double*>(take(sizeof(double) * 2 * (size_t)g.Nlm));
@@ -132,11 +137,79 @@ int plan_maps_per_pass(const dsht_plan_s* p) {
 Route plan_route(const dsht_plan_s* p, int64_t N) {
   Route r{};
   r.tc = p->precision != DSHT_PREC_FP64 && N >= DSHT_MIXED_MIN_POINTS;
-  // FP32 tables for tensor-core transforms at the MIXED level, and for every transform of a
-  // plan that holds no FP64 tables.
-  r.f32_tables = p->tm32 && ((r.tc && p->precision == DSHT_PREC_MIXED) || !p->Yv);
-  r.streamed = r.f32_tables || p->tm64;
+  // The compact tables (digits, else FP32) serve tensor-core transforms at the MIXED level
+  // and every transform of a plan that holds no FP64 tables.
+  const bool compact = (r.tc && p->precision == DSHT_PREC_MIXED) || !p->Yv;
+  r.digits = p->tmdig && compact;
+  r.f32_tables = !r.digits && p->tm32 && compact;
+  r.streamed = r.digits || r.f32_tables || p->tm64;
   return r;
+}
+
+// Builds the digit tables of rows [row0, row0 + nrows) from FP64 tables (Healpy order)
+// held at Yv, Yd for exactly those rows.
+static void digits_from_rows(dsht_plan_s* p, int64_t row0, int64_t nrows, const double* Yv, const double* Yd,
+                             cudaStream_t s) {
+  launch_table_rowexp(p->g, row0, nrows, Yv, Yd, p->rexp, s);
+  launch_table_digits(p->g, row0, nrows, Yv, Yd, p->rexp, p->dig, s);
+}
+
+// Allocates the digit tables, the tensor-core work items and the tensor map; fills the
+// tables from the plan's FP64 tables, or (plans without them) from FP64 columns built a
+// few m at a time into temporary buffers.
+static int build_digits(dsht_plan_s* p) {
+  const Geometry& g = p->g;
+  if (g.Nx > kTcMaxNx || g.Nl > 2048) return set_error(DSHT_ERR_INVALID, "digit tables need Nx <= %d", kTcMaxNx);
+  const size_t kp = (size_t)digit_kp(g.Nx);
+  cudaError_t e = cudaMalloc(&p->dig, 4 * (size_t)g.Nlm * kp);
+  if (e == cudaSuccess) e = cudaMalloc(&p->rexp, sizeof(int16_t) * (size_t)g.Nlm);
+  const std::vector<uint32_t> items = tc_items(g.Nl);
+  if (e == cudaSuccess) e = cudaMalloc(&p->tc_items, sizeof(uint32_t) * items.size());
+  if (e == cudaSuccess)
+    e = cudaMemcpy(p->tc_items, items.data(), sizeof(uint32_t) * items.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(p->dig);
+    cudaFree(p->rexp);
+    cudaFree(p->tc_items);
+    p->dig = nullptr;
+    p->rexp = nullptr;
+    p->tc_items = nullptr;
+    cudaGetLastError();
+    return set_cuda_error(e, "digit table allocation", __FILE__, __LINE__);
+  }
+  p->tc_nitems = (int)items.size();
+  if (p->Yv) {
+    digits_from_rows(p, 0, g.Nlm, p->Yv, p->Yd, 0);
+  } else {
+    // columns m0 .. m1 - 1 with at most ~2^26 table entries per pass through the buffers
+    const int64_t cap = std::max<int64_t>((int64_t)1 << 26, (int64_t)g.Nl * g.Nx);
+    double *tv = nullptr, *td = nullptr;
+    e = cudaMalloc(&tv, sizeof(double) * cap);
+    if (e == cudaSuccess) e = cudaMalloc(&td, sizeof(double) * cap);
+    if (e != cudaSuccess) {
+      cudaFree(tv);
+      cudaFree(td);
+      cudaGetLastError();
+      return set_cuda_error(e, "digit table build buffers", __FILE__, __LINE__);
+    }
+    for (int m0 = 0; m0 < g.Nl;) {
+      int m1 = m0 + 1;
+      while (m1 < g.Nl && (hp_index(m1 + 1, m1 + 1, g.Nl) - hp_index(m0, m0, g.Nl)) * g.Nx <= cap) ++m1;
+      const int64_t r0 = hp_index(m0, m0, g.Nl), r1 = hp_index(m1, m1, g.Nl);
+      launch_tables_cols(g, m0, m1, tv, td, 0);
+      digits_from_rows(p, r0, r1 - r0, tv, td, 0);
+      m0 = m1;
+    }
+    e = cudaDeviceSynchronize();
+    cudaFree(tv);
+    cudaFree(td);
+    if (e != cudaSuccess) return set_cuda_error(e, "digit table build", __FILE__, __LINE__);
+  }
+  DSHT_CUDA_OK(cudaDeviceSynchronize());
+  DSHT_CUDA_OK(cudaGetLastError());
+  if (int rc = make_table_digit_tmap(&p->tmDig, p->dig, g.Nx, g.Nlm)) return rc;
+  p->tmdig = true;
+  return DSHT_OK;
 }
 
 Geometry make_geometry(int Nl, int Nx, double xmax) {
@@ -170,10 +243,23 @@ int run_after_sort(dsht_plan_s* p, int64_t N, int mode, double* alm, const Works
     if (rc) return rc;
     w2.partial_f32 = 1;
   } else {
-    if (f32_tables) launch_piece_maxima(ws, s);  // the |w| sums of the heavy-node test
+    if (f32_tables || rt.digits) launch_piece_maxima(ws, s);  // the |w| sums (node weights)
     launch_bin_sums_fp64(g, ws, s);
     w2.partial_f32 = 0;
   }
+  if (rt.digits) {
+    mark(DSHT_STAGE_FOLD);
+    uint8_t* fdig = reinterpret_cast<uint8_t*>(ws.fold);
+    launch_fold_scale(g, w2, ws.cexp, s);
+    launch_fold_digits(g, w2, ws.cexp, 0, 4, fdig, s);
+    mark(DSHT_STAGE_CONTRACT);
+    TcOut out{};
+    out.equ[0] = ws.alm_equ;
+    out.pol[0] = ws.alm_pol;
+    if (int rc = launch_contract_tc(g, p->tmDig, p->tc_items, p->tc_nitems, p->rexp, fdig, 4, ws.cexp, 1, out,
+                                    ws.flags, s))
+      return rc;
+  } else {
   w2.fold_f32 = f32_tables ? 1 : 0;
   mark(DSHT_STAGE_FOLD);
   if (f32_tables) launch_heavy_select(g, w2, 0, s);
@@ -186,6 +272,7 @@ int run_after_sort(dsht_plan_s* p, int64_t N, int mode, double* alm, const Works
     launch_contract_stream(g, false, p->tmYv, p->tmYd, ws, s);
   else
     launch_contract_fp64(g, p->Yv, p->Yd, ws, s);
+  }
   mark(DSHT_STAGE_ROTATE);
   if (mode == DSHT_MODE_CALL) {
     launch_rotate_back(g, ws.alm_pol, ws.alm_equ, alm, ws.flags, s);
@@ -206,6 +293,74 @@ int run_pipeline(dsht_plan_s* p, const double* theta, const double* phi, const d
   launch_points(p->g, theta, phi, w, 0, N, mode, ws, s);
   prof_mark(p, DSHT_STAGE_BIN_SUMS, s);
   return run_after_sort(p, N, mode, alm, ws, s, true);
+}
+
+// Items of one class on the tensor-core route: passes of up to ws.tc_maps items (at most
+// kMaxRot, the rotation batch); each item's fold goes straight to digits in its column slot,
+// and one contraction launch per pass reads every table tile once for all of them.
+static int run_class_digits(dsht_plan_s* p, const Item* items, const std::vector<int>& list, int mode,
+                            const Workspace& ws, cudaStream_t s, int* sorted_item) {
+  const Geometry& g = p->g;
+  const int64_t nlm2 = 2 * g.Nlm;
+  const Route rt = plan_route(p, items[list[0]].N);
+  const int G = std::min(ws.tc_maps, kMaxRot);
+  const int fcols = 4 * ws.tc_maps;
+  uint8_t* fdig = reinterpret_cast<uint8_t*>(ws.fold);
+  std::vector<int> pass;
+  for (size_t li = 0; li < list.size(); ++li) {
+    const int i = list[li];
+    const Item& item = items[i];
+    const int slot = (int)pass.size();
+    Workspace w2 = ws;
+    w2.flags = ws.slot_flags + slot;
+    if (item.same_points && *sorted_item >= 0) {
+      prof_mark(p, DSHT_STAGE_BIN_SUMS, s);  // the weight gather counts with the bin sums
+      launch_gather(g, item.w, item.w_f32, item.N, ws, s);
+    } else {
+      prof_mark(p, DSHT_STAGE_POINTS, s);
+      Workspace wp = ws;
+      if (!(li + 1 < list.size() && items[list[li + 1]].same_points)) wp.sidx = nullptr;
+      launch_points(g, item.theta, item.phi, item.w, item.w_f32, item.N, mode, wp, s);
+      *sorted_item = i;
+    }
+    prof_mark(p, DSHT_STAGE_BIN_SUMS, s);
+    DSHT_CUDA_OK(cudaMemcpyAsync(w2.flags, ws.flags, sizeof(unsigned), cudaMemcpyDeviceToDevice, s));
+    if (rt.tc) {
+      int rc = launch_bin_sums_tc(g, w2, s);
+      if (rc) return rc;
+      w2.partial_f32 = 1;
+    } else {
+      launch_piece_maxima(w2, s);
+      launch_bin_sums_fp64(g, w2, s);
+      w2.partial_f32 = 0;
+    }
+    prof_mark(p, DSHT_STAGE_FOLD, s);
+    launch_fold_scale(g, w2, ws.cexp + 2 * slot, s);
+    launch_fold_digits(g, w2, ws.cexp + 2 * slot, slot, fcols, fdig, s);
+    pass.push_back(i);
+    if ((int)pass.size() < G && li + 1 < list.size()) continue;
+    TcOut out{};
+    RotMaps rm{};
+    StatusOut so{};
+    for (size_t k = 0; k < pass.size(); ++k) {
+      out.equ[k] = items[pass[k]].alm;
+      out.pol[k] = ws.alm_pol + nlm2 * k;
+      rm.rot[k] = out.pol[k];
+      rm.io[k] = items[pass[k]].alm;
+      rm.flags[k] = ws.slot_flags + k;
+      so.slot[k] = ws.slot_flags + k;
+      so.status[k] = items[pass[k]].status;
+    }
+    prof_mark(p, DSHT_STAGE_CONTRACT, s);
+    if (int rc = launch_contract_tc(g, p->tmDig, p->tc_items, p->tc_nitems, p->rexp, fdig, fcols, ws.cexp,
+                                    (int)pass.size(), out, ws.slot_flags, s))
+      return rc;
+    prof_mark(p, DSHT_STAGE_ROTATE, s);
+    if (mode == DSHT_MODE_CALL) launch_rotate_back_maps(g, rm, (int)pass.size(), s);
+    launch_publish_flags(so, (int)pass.size(), ws.all_flags, s);
+    pass.clear();
+  }
+  return DSHT_OK;
 }
 
 // Several transforms in one call: multi-map transforms (one point set, the later maps marked
@@ -232,6 +387,11 @@ int run_items(dsht_plan_s* p, const Item* items, int n, int mode, const Workspac
     const std::vector<int>& list = order[cls];
     if (list.empty()) continue;
     const Route rt = plan_route(p, items[list[0]].N);
+    if (rt.digits) {
+      int rc = run_class_digits(p, items, list, mode, ws, s, &sorted_item);
+      if (rc) return rc;
+      continue;
+    }
     const bool mixed = rt.tc;
     const bool f32_tables = rt.f32_tables;
     const bool streamed = rt.streamed;
@@ -412,8 +572,9 @@ int dsht_plan_create(int Nl, int Nx, double xmax, int flags, dsht_plan_t* plan) 
     return set_error(DSHT_ERR_INVALID, "invalid sizes Nl=%d Nx=%d xmax=%g", Nl, Nx, xmax);
   if (flags & ~DSHT_PLAN_F32_TABLES) return set_error(DSHT_ERR_INVALID, "unknown plan flags %d", flags);
   const bool f32_only = (flags & DSHT_PLAN_F32_TABLES) != 0;
-  if (f32_only && (Nx % 4 != 0 || Nl > 2048))
-    return set_error(DSHT_ERR_INVALID, "FP32-table plans need Nx %% 4 == 0 and Nl <= 2048 (Nl=%d Nx=%d)", Nl, Nx);
+  if (f32_only && (Nx > kTcMaxNx || Nl > 2048))
+    return set_error(DSHT_ERR_INVALID, "compact-table plans need Nx <= %d and Nl <= 2048 (Nl=%d Nx=%d)", kTcMaxNx,
+                     Nl, Nx);
   dsht_plan_s* p = new dsht_plan_s();
   p->g = make_geometry(Nl, Nx, xmax);
   cudaGetDevice(&p->device);
@@ -428,12 +589,16 @@ int dsht_plan_create(int Nl, int Nx, double xmax, int flags, dsht_plan_t* plan) 
     return set_cuda_error(e, what, __FILE__, __LINE__);
   };
   cudaError_t e = cudaMallocHost(&p->h_flags, sizeof(unsigned));
+  if (e != cudaSuccess) return fail(e, "plan allocation");
   if (f32_only) {
-    const size_t tb = sizeof(float) * (size_t)p->g.Nlm * Nx;
-    if (e == cudaSuccess) e = cudaMalloc(&p->Yv32, tb);
-    if (e == cudaSuccess) e = cudaMalloc(&p->Yd32, tb);
-    if (e != cudaSuccess) return fail(e, "plan allocation");
-    launch_tables_f32(p->g, p->Yv32, p->Yd32, 0);
+    // compact plan: the digit tables alone, built from FP64 columns a few m at a time
+    if (int rc = build_digits(p)) {
+      dsht_plan_destroy(p);
+      return rc;
+    }
+    p->precision = DSHT_PREC_MIXED;
+    *plan = p;
+    return DSHT_OK;
   } else {
     const size_t tb = sizeof(double) * (size_t)p->g.Nlm * Nx;
     if (e == cudaSuccess) e = cudaMalloc(&p->Yv, tb);
@@ -444,18 +609,7 @@ int dsht_plan_create(int Nl, int Nx, double xmax, int flags, dsht_plan_t* plan) 
   e = cudaDeviceSynchronize();
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) return fail(e, "table build");
-  if (f32_only) {
-    if (!(contract_stream_ok(p->g, sizeof(float)) &&
-          make_table_tmap(&p->tmYv32, p->Yv32, sizeof(float), Nx, p->g.Nlm) == DSHT_OK &&
-          make_table_tmap(&p->tmYd32, p->Yd32, sizeof(float), Nx, p->g.Nlm) == DSHT_OK &&
-          make_table_tmap(&p->tmYv32h, p->Yv32, sizeof(float), Nx, p->g.Nlm, 16) == DSHT_OK &&
-          make_table_tmap(&p->tmYd32h, p->Yd32, sizeof(float), Nx, p->g.Nlm, 16) == DSHT_OK)) {
-      dsht_plan_destroy(p);
-      return DSHT_ERR_CUDA;
-    }
-    p->tm32 = true;
-    p->precision = DSHT_PREC_MIXED;
-  } else if (contract_stream_ok(p->g, sizeof(double)) &&
+  if (contract_stream_ok(p->g, sizeof(double)) &&
              make_table_tmap(&p->tmYv, p->Yv, sizeof(double), Nx, p->g.Nlm) == DSHT_OK &&
              make_table_tmap(&p->tmYd, p->Yd, sizeof(double), Nx, p->g.Nlm) == DSHT_OK) {
     p->tm64 = true;
@@ -475,6 +629,9 @@ int dsht_plan_destroy(dsht_plan_t p) {
   cudaFree(p->Yd);
   cudaFree(p->Yv32);
   cudaFree(p->Yd32);
+  cudaFree(p->dig);
+  cudaFree(p->rexp);
+  cudaFree(p->tc_items);
   cudaFree(p->ws);
   cudaFree(p->in);
   cudaFree(p->alm);
@@ -490,9 +647,18 @@ int dsht_set_precision(dsht_plan_t p, int precision) {
   if (precision != DSHT_PREC_FP64 && p->g.Nl > 2048)
     return set_error(DSHT_ERR_INVALID, "mixed precision supports Nl <= 2048 (Nl=%d)", p->g.Nl);
   if (!p->Yv && precision != DSHT_PREC_MIXED)
-    return set_error(DSHT_ERR_INVALID, "this plan holds FP32 tables only (DSHT_PLAN_F32_TABLES): precision MIXED");
+    return set_error(DSHT_ERR_INVALID, "this plan holds compact tables only (DSHT_PLAN_F32_TABLES): precision MIXED");
   std::lock_guard<std::mutex> lock(p->mu);
-  if (precision == DSHT_PREC_MIXED && !p->Yv32) {
+  // MIXED streams the digit tables through the tensor-core contraction (built on first use);
+  // where they do not fit, an FP32 copy streamed by the CUDA-core contraction, else FP64.
+  if (precision == DSHT_PREC_MIXED && !p->tmdig && !p->Yv32 && p->g.Nx <= kTcMaxNx) {
+    if (build_digits(p) == DSHT_OK) {
+      p->precision = precision;
+      return DSHT_OK;
+    }
+    cudaGetLastError();
+  }
+  if (precision == DSHT_PREC_MIXED && !p->tmdig && !p->Yv32) {
     const size_t tb = sizeof(float) * (size_t)p->g.Nlm * p->g.Nx;
     cudaError_t e = cudaMalloc(&p->Yv32, tb);
     if (e == cudaSuccess) e = cudaMalloc(&p->Yd32, tb);
@@ -528,8 +694,8 @@ int dsht_plan_tune(dsht_plan_t p, int param, int value) {
       p->tune_piece_max = value;
       return DSHT_OK;
     case DSHT_TUNE_MAPS_PER_PASS:
-      if (value < 0 || value > contract_stream_max_maps(true))
-        return set_error(DSHT_ERR_INVALID, "maps per pass %d: 0 (most) or 1..%d", value, contract_stream_max_maps(true));
+      if (value < 0 || value > kTcMaxMaps)
+        return set_error(DSHT_ERR_INVALID, "maps per pass %d: 0 (most) or 1..%d", value, kTcMaxMaps);
       p->tune_maps_per_pass = value;
       return DSHT_OK;
   }
@@ -598,7 +764,10 @@ int dsht_workspace_size(dsht_plan_t p, int64_t N, size_t* bytes) {
 // the gather records, fold slots, rotation slots and flag slots.
 static size_t call_layout(dsht_plan_s* p, int64_t N, int ntrans, bool multi, uint8_t* base, Workspace* ws) {
   const int slots = multi ? std::min(std::max(ntrans, 1), plan_maps_per_pass(p)) : 1;
-  return workspace_layout(p->g, N, plan_piece_max(p, N), base, ws, slots, multi);
+  // maps per tensor-core contraction pass (digit tables): up to kTcMaxMaps unless tuned
+  const int tc = multi ? std::min(std::max(ntrans, 1), p->tune_maps_per_pass > 0 ? p->tune_maps_per_pass
+                                                                                  : kTcMaxMaps) : 1;
+  return workspace_layout(p->g, N, plan_piece_max(p, N), base, ws, slots, multi, tc);
 }
 
 // Resolves the workspace (caller's or the plan's, grown on demand) for a call.
@@ -830,20 +999,34 @@ int dsht_rotate_back(dsht_plan_t p, const double* alm_rot, const double* alm_add
   return DSHT_OK;
 }
 
+// Rows [r0, r0 + n) (Healpy order) of a compact plan's table, decoded from the digits, to
+// host memory (through a device buffer of at most 2^24 values at a time).
+static int decode_rows_to_host(dsht_plan_s* p, int which, int64_t r0, int64_t n, double* out) {
+  const int Nx = p->g.Nx;
+  const int64_t per = std::max<int64_t>(1, ((int64_t)1 << 24) / Nx);
+  double* buf = nullptr;
+  DSHT_CUDA_OK(cudaMalloc(&buf, sizeof(double) * (size_t)std::min(per, n) * Nx));
+  int rc = DSHT_OK;
+  for (int64_t i = 0; i < n && rc == DSHT_OK; i += per) {
+    const int64_t c = std::min(per, n - i);
+    launch_table_decode(p->g, which, r0 + i, c, p->dig, p->rexp, buf, 0);
+    const cudaError_t e = cudaMemcpy(out + i * Nx, buf, sizeof(double) * (size_t)c * Nx, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) rc = set_cuda_error(e, "table decode", __FILE__, __LINE__);
+  }
+  cudaFree(buf);
+  return rc;
+}
+
 int dsht_get_row(dsht_plan_t p, int which, int ell, int m, double* out) {
   if (!p || !out || which < 0 || which > 1 || m < 0 || ell < m || ell >= p->g.Nl)
     return set_error(DSHT_ERR_INVALID, "invalid row (which=%d, l=%d, m=%d)", which, ell, m);
-  const int64_t off = hp_index(ell, m, p->g.Nl) * p->g.Nx;
+  const int64_t row = hp_index(ell, m, p->g.Nl);
   if (p->Yv) {
     const double* t = which == 0 ? p->Yv : p->Yd;
-    DSHT_CUDA_OK(cudaMemcpy(out, t + off, sizeof(double) * p->g.Nx, cudaMemcpyDeviceToHost));
-  } else {  // FP32-table plan: the stored values, widened
-    std::vector<float> tmp(p->g.Nx);
-    const float* t = which == 0 ? p->Yv32 : p->Yd32;
-    DSHT_CUDA_OK(cudaMemcpy(tmp.data(), t + off, sizeof(float) * p->g.Nx, cudaMemcpyDeviceToHost));
-    for (int j = 0; j < p->g.Nx; ++j) out[j] = tmp[j];
+    DSHT_CUDA_OK(cudaMemcpy(out, t + row * p->g.Nx, sizeof(double) * p->g.Nx, cudaMemcpyDeviceToHost));
+    return DSHT_OK;
   }
-  return DSHT_OK;
+  return decode_rows_to_host(p, which, row, 1, out);
 }
 
 int dsht_get_table(dsht_plan_t p, int which, double* out) {
@@ -852,17 +1035,9 @@ int dsht_get_table(dsht_plan_t p, int which, double* out) {
   if (p->Yv) {
     const double* t = which == 0 ? p->Yv : p->Yd;
     DSHT_CUDA_OK(cudaMemcpy(out, t, sizeof(double) * n, cudaMemcpyDeviceToHost));
-  } else {
-    const float* t = which == 0 ? p->Yv32 : p->Yd32;
-    const size_t chunk = (size_t)1 << 24;
-    std::vector<float> tmp(std::min(n, chunk));
-    for (size_t i = 0; i < n; i += chunk) {
-      const size_t c = std::min(chunk, n - i);
-      DSHT_CUDA_OK(cudaMemcpy(tmp.data(), t + i, sizeof(float) * c, cudaMemcpyDeviceToHost));
-      for (size_t k = 0; k < c; ++k) out[i + k] = tmp[k];
-    }
+    return DSHT_OK;
   }
-  return DSHT_OK;
+  return decode_rows_to_host(p, which, 0, p->g.Nlm, out);
 }
 
 int dsht_get_table_mlayout(dsht_plan_t p, int which, double* out, int out_on_device, void* stream) {
@@ -871,10 +1046,15 @@ int dsht_get_table_mlayout(dsht_plan_t p, int which, double* out, int out_on_dev
   const size_t plane = (size_t)Nl * Nx;  // one m: Nl rows of Nx
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   if (out_on_device) {
-    launch_table_mlayout(p->g, which == 0 ? p->Yv : p->Yd, which == 0 ? p->Yv32 : p->Yd32, out, s);
+    if (p->Yv) {
+      launch_table_mlayout(p->g, which == 0 ? p->Yv : p->Yd, out, s);
+    } else {  // compact plan: decode each column's rows into its slice of out
+      DSHT_CUDA_OK(cudaMemsetAsync(out, 0, sizeof(double) * plane * Nl, s));
+      for (int m = 0; m < Nl; ++m)
+        launch_table_decode(p->g, which, hp_index(m, m, Nl), Nl - m, p->dig, p->rexp, out + (size_t)m * plane, s);
+    }
     return launch_error("table_mlayout_kernel");
   }
-  std::vector<float> tmp;
   for (int m = 0; m < Nl; ++m) {
     // Rows l = m..Nl-1 of column m are contiguous in Healpy order; they fill k = l - m.
     const int64_t row0 = hp_index(m, m, Nl);
@@ -883,11 +1063,8 @@ int dsht_get_table_mlayout(dsht_plan_t p, int which, double* out, int out_on_dev
     if (p->Yv) {
       const double* t = (which == 0 ? p->Yv : p->Yd) + (size_t)row0 * Nx;
       DSHT_CUDA_OK(cudaMemcpy(dst, t, sizeof(double) * n, cudaMemcpyDeviceToHost));
-    } else {
-      const float* t = (which == 0 ? p->Yv32 : p->Yd32) + (size_t)row0 * Nx;
-      tmp.resize(n);
-      DSHT_CUDA_OK(cudaMemcpy(tmp.data(), t, sizeof(float) * n, cudaMemcpyDeviceToHost));
-      for (size_t k = 0; k < n; ++k) dst[k] = tmp[k];
+    } else if (int rc = decode_rows_to_host(p, which, row0, Nl - m, dst)) {
+      return rc;
     }
     std::memset(dst + n, 0, sizeof(double) * (plane - n));  // k >= Nl - m: l >= Nl (unphysical)
   }

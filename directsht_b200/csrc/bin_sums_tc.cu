@@ -92,33 +92,9 @@ __device__ __forceinline__ int quant(float x) {
   return __float_as_int(fmaf(x, kQf, kMagic)) - (0x4B400000 - 0x8080);
 }
 
-// Shared-memory descriptor: K-major operand in the 64-byte swizzle layout (rows of 64 B,
-// 8-row atoms of 512 B packed: stride byte offset 512).
-__device__ __forceinline__ uint64_t desc_k_sw64(uint32_t saddr) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
-  d |= (uint64_t)1u << 16;
-  d |= (uint64_t)(512u >> 4) << 32;
-  d |= (uint64_t)1u << 46;
-  d |= (uint64_t)4u << 61;  // 64-byte swizzle
-  return d;
-}
-
-// Instruction descriptor of kind::i8 (D s32, both K-major, M x N); a/b signed or not.
-__host__ __device__ constexpr uint32_t idesc_i8(int M, int N, bool a_signed, bool b_signed) {
-  return (2u << 4) | ((a_signed ? 1u : 0u) << 7) | ((b_signed ? 1u : 0u) << 10) | ((uint32_t)(N >> 3) << 17) |
-         ((uint32_t)(M >> 4) << 24);
-}
-
-__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                                       bool accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
-      "l"(adesc), "l"(bdesc), "r"(idesc), "r"((uint32_t)accumulate)
-      : "memory");
-}
+using tc::desc_k_sw64;
+using tc::idesc_i8;
+using tc::mma_i8;
 
 // One slicing unit: 16 points (chunk h of the 64-point block) x 4 operand rows.  `values`
 // writes the four fixed-point values of point pp into X[0..3]; they are byte-transposed

@@ -1,0 +1,319 @@
+// Fixed-point digit tables and folds for the tensor-core contraction (contract_tc.cu).
+//
+// The contraction alm[lm] = sum_j Yv[lm,j] A[m,j] + Yd[lm,j] B[m,j] (sht/sht.py:266-277,
+// sht/interp_funcs_py.py:46-60) is a dot product over K = 2 Nx entries per row:
+//   T[r, k] = Yv[r, k] (k < Nx),  dx Yd[r, k - Nx] (Nx <= k < 2 Nx),
+//   F[k, c] = A_c[k]   (k < Nx),  B_c[k - Nx] / dx.
+// Both sides are stored as 31-bit fixed point with one power-of-two scale per table row
+// (2^er > 1.01 max_k |T[r, k]|) and per fold column (2^ec > 1.01 x the largest node weight,
+// which bounds |A| and |B/dx| for every m): X = rint(T 2^(31 - er)), |X| < 2^31 - 2^24.
+// X is written as four balanced base-256 digits, X = d0 2^24 + d1 2^16 + d2 2^8 + d3 with
+// every digit a signed byte: the bytes of (X + 0x808080) ^ 0x808080.  Digit d of every
+// entry forms plane d (int8, K-major rows of Kp bytes, Kp = 2 Nx rounded up to 64).
+//
+// Table rows are stored grouped by the parity of l - m: for each m the rows l = m, m+2, ...
+// (n_e(m) = (Nl - m + 1)/2 of them) and then l = m+1, m+3, ... -- the even and odd rows
+// contract with different folds (the x < 0 half enters with (-1)^(l-m), sht/sht.py:279).
+// Fold digits of a pass of G maps: plane-major [m][parity][digit][4 G columns][Kp] with
+// column 4 g + 2 h + ri = (map g, half h = equatorial / rotated polar, re | im).
+//
+// Quantisation error of an entry: <= 2^-32 of its row's (column's) scale; a contraction sum
+// errs by at most about 2^-30 (max|T| sum|F| + max|F| sum|T|), far less for spread sets.
+#include "recurrence.cuh"
+
+namespace dsht {
+namespace {
+
+constexpr double kScaleMargin = 1.01;  // scale > 1.01 x bound: |X| < 2^31 / 1.01 < 2^31 - 2^24
+
+// Smallest e with kScaleMargin * v <= 2^e (v >= 0; 0 for v = 0).
+__device__ __forceinline__ int scale_exp(double v) {
+  if (!(v > 0.0) || !isfinite(v)) return 0;
+  int e;
+  frexp(v * kScaleMargin, &e);  // v * margin = f 2^e with f in [0.5, 1)
+  return e;
+}
+
+// The four signed digit bytes of rint(v 2^sh) packed little-endian: byte i = digit 3 - i.
+__device__ __forceinline__ uint32_t digit_word(double v, int sh) {
+  const long long X = __double2ll_rn(ldexp(v, sh));
+  return (uint32_t)((int)X + 0x808080) ^ 0x808080u;
+}
+
+// Grouped row of Healpy row (l, m).
+__device__ __forceinline__ int64_t grouped_row(int l, int m, int Nl) {
+  const int64_t base = hp_index(m, m, Nl);
+  const int k = l - m;
+  const int ne = (Nl - m + 1) / 2;
+  return base + ((k & 1) ? ne + (k >> 1) : (k >> 1));
+}
+
+// Row exponents of the FP64 tables rows [row0, row0 + nrows) (Healpy order, row r at
+// Y + (r - row0) * Nx): one warp per row.
+__global__ void table_rowexp_kernel(int Nl, int Nx, double dx, int64_t row0, int64_t nrows, const double* __restrict__ Yv,
+                                    const double* __restrict__ Yd, int16_t* __restrict__ rexp) {
+  const int lane = threadIdx.x & 31;
+  const int64_t wstride = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t i = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < nrows; i += wstride) {
+    const double* v = Yv + i * Nx;
+    const double* d = Yd + i * Nx;
+    double mx = 0.0;
+    for (int j = lane; j < Nx; j += 32) mx = fmax(mx, fmax(fabs(v[j]), fabs(dx * d[j])));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) {
+      // Healpy row r = row0 + i -> (l, m)
+      const int64_t r = row0 + i;
+      int m = (int)((2.0 * Nl + 1.0 - sqrt((2.0 * Nl + 1.0) * (2.0 * Nl + 1.0) - 8.0 * (double)r)) / 2.0);
+      if (m < 0) m = 0;
+      while (m > 0 && hp_index(m, m, Nl) > r) --m;
+      while (m + 1 < Nl && hp_index(m + 1, m + 1, Nl) <= r) ++m;
+      const int l = (int)(r - hp_index(m, m, Nl)) + m;
+      rexp[grouped_row(l, m, Nl)] = (int16_t)scale_exp(mx);
+    }
+  }
+}
+
+// Digits of rows [row0, row0 + nrows): one thread per (row, 4 consecutive k).
+__global__ void table_digits_kernel(int Nl, int Nx, int Kp, double dx, int64_t row0, int64_t nrows,
+                                    const double* __restrict__ Yv, const double* __restrict__ Yd,
+                                    const int16_t* __restrict__ rexp, int64_t plane, uint8_t* __restrict__ dig) {
+  const int words = Kp / 4;
+  const int64_t total = nrows * words;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = t / words;
+    const int k0 = (int)(t - i * words) * 4;
+    const int64_t r = row0 + i;
+    int m = (int)((2.0 * Nl + 1.0 - sqrt((2.0 * Nl + 1.0) * (2.0 * Nl + 1.0) - 8.0 * (double)r)) / 2.0);
+    if (m < 0) m = 0;
+    while (m > 0 && hp_index(m, m, Nl) > r) --m;
+    while (m + 1 < Nl && hp_index(m + 1, m + 1, Nl) <= r) ++m;
+    const int l = (int)(r - hp_index(m, m, Nl)) + m;
+    const int64_t g = grouped_row(l, m, Nl);
+    const int sh = 31 - rexp[g];
+    uint32_t b[4] = {0u, 0u, 0u, 0u};  // plane d: byte e = digit d of entry k0 + e
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int k = k0 + e;
+      double v = 0.0;
+      if (k < Nx) v = Yv[i * Nx + k];
+      else if (k < 2 * Nx) v = dx * Yd[i * Nx + (k - Nx)];
+      const uint32_t w = digit_word(v, sh);
+#pragma unroll
+      for (int d = 0; d < 4; ++d) b[d] |= ((w >> (8 * (3 - d))) & 0xffu) << (8 * e);
+    }
+#pragma unroll
+    for (int d = 0; d < 4; ++d) *reinterpret_cast<uint32_t*>(dig + d * plane + g * Kp + k0) = b[d];
+  }
+}
+
+// Table values back from the digits (rows in Healpy order r0.. r0 + n, both tables):
+// Y = 2^(er - 31) X with X from the four digit bytes.  which = 0: Yv, 1: Yd.
+__global__ void table_decode_kernel(int Nl, int Nx, int Kp, double dx, int which, int64_t r0, int64_t n,
+                                    const uint8_t* __restrict__ dig, int64_t plane, const int16_t* __restrict__ rexp,
+                                    double* __restrict__ out) {
+  const int64_t total = n * Nx;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = t / Nx;
+    const int j = (int)(t - i * Nx);
+    const int64_t r = r0 + i;
+    int m = (int)((2.0 * Nl + 1.0 - sqrt((2.0 * Nl + 1.0) * (2.0 * Nl + 1.0) - 8.0 * (double)r)) / 2.0);
+    if (m < 0) m = 0;
+    while (m > 0 && hp_index(m, m, Nl) > r) --m;
+    while (m + 1 < Nl && hp_index(m + 1, m + 1, Nl) <= r) ++m;
+    const int l = (int)(r - hp_index(m, m, Nl)) + m;
+    const int64_t g = grouped_row(l, m, Nl);
+    const int k = which == 0 ? j : Nx + j;
+    long long X = 0;
+#pragma unroll
+    for (int d = 0; d < 4; ++d) X = X * 256 + (long long)(int8_t)dig[d * plane + g * Kp + k];
+    double v = ldexp((double)X, rexp[g] - 31);
+    if (which == 1) v /= dx;
+    out[t] = v;
+  }
+}
+
+// Per-map fold scales: exponent of the largest |w| sum feeding a node of each half (the
+// node sums as heavy_select_kernel forms them), which bounds |A| and |B/dx| for every m.
+constexpr int kScaleThreads = 1024;
+__global__ void __launch_bounds__(kScaleThreads)
+fold_scale_kernel(int nbins, int Nx, const int* __restrict__ piece_first, const double* __restrict__ wsum,
+                  int16_t* __restrict__ cexp) {
+  __shared__ double red[2][32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  double mx[2] = {0.0, 0.0};
+  for (int e = warp; e < 2 * Nx; e += blockDim.x >> 5) {
+    const int h = e / Nx, j = e - h * Nx;
+    double s = 0.0;
+    for (int sset = 2 * h; sset < 2 * h + 2; ++sset)
+      for (int b = j - 1; b <= j; ++b) {
+        if (b < 0 || b >= nbins) continue;
+        const int key = sset * nbins + b;
+        for (int pc = piece_first[key] + lane; pc < piece_first[key + 1]; pc += 32) s += wsum[pc];
+      }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    mx[h] = fmax(mx[h], s);
+  }
+  if (lane == 0) {
+    red[0][warp] = mx[0];
+    red[1][warp] = mx[1];
+  }
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      double v = lane < (int)(blockDim.x >> 5) ? red[h][lane] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+      if (lane == 0) cexp[h] = (int16_t)scale_exp(v);
+    }
+  }
+}
+
+// Fold of one map straight into digits.  A block covers 32 m x 32 nodes: warp = node,
+// lane = m while the per-piece sums are read (consecutive m: coalesced), then the digit
+// bytes go through shared memory so that consecutive threads store consecutive nodes.
+// Sums as fold_kernel forms them (set s: A = V0(bin j) + V2(bin j-1), B = dx (V1(bin j) +
+// V3(bin j-1)), V = vr - i vi; even rows A+ + A-, odd rows A+ - A-), stored as B/dx.
+template <typename PT>
+__global__ void __launch_bounds__(1024)
+fold_digits_kernel(int Nl, int Nx, int nbins, int Kp, const int* __restrict__ piece_first,
+                   const PT* __restrict__ partial, const int16_t* __restrict__ cexp, int map, int ncols,
+                   uint8_t* __restrict__ fdig) {
+  // stage[m][par][d][c][kh][j]: 32 x 2 x 4 x 4 x 2 x 32 bytes (dynamic: 64 KB)
+  extern __shared__ __align__(16) uint8_t stage[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int m0 = blockIdx.y * 32, j0 = blockIdx.x * 32;
+  const int m = m0 + lane, j = j0 + warp;
+  const int sh0 = 31 - cexp[0], sh1 = 31 - cexp[1];
+  double A[4][2], Bv[4][2];
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    double ar = 0.0, ai = 0.0, br = 0.0, bi = 0.0;
+    if (m < Nl && j < Nx) {
+      if (j < nbins) {
+        const int key = s * nbins + j;
+        for (int p = piece_first[key]; p < piece_first[key + 1]; ++p) {
+          const PT* v = partial + (size_t)p * 8 * Nl + m;
+          ar += v[0];
+          ai -= v[(size_t)Nl];
+          br += v[(size_t)2 * Nl];
+          bi -= v[(size_t)3 * Nl];
+        }
+      }
+      if (j >= 1) {
+        const int key = s * nbins + j - 1;
+        for (int p = piece_first[key]; p < piece_first[key + 1]; ++p) {
+          const PT* v = partial + (size_t)p * 8 * Nl + m;
+          ar += v[(size_t)4 * Nl];
+          ai -= v[(size_t)5 * Nl];
+          br += v[(size_t)6 * Nl];
+          bi -= v[(size_t)7 * Nl];
+        }
+      }
+    }
+    A[s][0] = ar;
+    A[s][1] = ai;
+    Bv[s][0] = br;
+    Bv[s][1] = bi;
+  }
+  // values[par][h][ri][kh]: kh = 0 the A entry, 1 the B/dx entry
+#pragma unroll
+  for (int par = 0; par < 2; ++par)
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+      for (int ri = 0; ri < 2; ++ri)
+#pragma unroll
+        for (int kh = 0; kh < 2; ++kh) {
+          const double (*X)[2] = kh ? Bv : A;
+          const double v = par ? X[2 * h][ri] - X[2 * h + 1][ri] : X[2 * h][ri] + X[2 * h + 1][ri];
+          const uint32_t w = digit_word(v, h ? sh1 : sh0);
+          const int c = 2 * h + ri;
+#pragma unroll
+          for (int d = 0; d < 4; ++d)
+            stage[((((lane * 2 + par) * 4 + d) * 4 + c) * 2 + kh) * 32 + warp] = (uint8_t)(w >> (8 * (3 - d)));
+        }
+  __syncthreads();
+  // 64 KB of digits = 16384 words; word w covers 4 nodes of one (m, par, d, c, kh) row.
+  const int nj = min(32, Nx - j0);
+  for (int w = threadIdx.x; w < 32 * 2 * 4 * 4 * 2 * 8; w += blockDim.x) {
+    const int q = w & 7;           // 4-node group
+    const int row = w >> 3;        // (((ml * 2 + par) * 4 + d) * 4 + c) * 2 + kh
+    const int kh = row & 1;
+    const int c = (row >> 1) & 3;
+    const int d = (row >> 3) & 3;
+    const int par = (row >> 5) & 1;
+    const int ml = row >> 6;
+    const int mm = m0 + ml;
+    if (mm >= Nl || 4 * q >= nj) continue;
+    const uint32_t word = *reinterpret_cast<const uint32_t*>(stage + row * 32 + 4 * q);
+    uint8_t* dst = fdig + ((((size_t)mm * 2 + par) * 4 + d) * ncols + 4 * map + c) * (size_t)Kp + (size_t)kh * Nx + j0 +
+                   4 * q;
+    if (4 * q + 4 <= nj && ((reinterpret_cast<uintptr_t>(dst) & 3) == 0)) {
+      *reinterpret_cast<uint32_t*>(dst) = word;
+    } else {
+      for (int e = 0; e < 4 && 4 * q + e < nj; ++e) dst[e] = (uint8_t)(word >> (8 * e));
+    }
+  }
+}
+
+}  // namespace
+
+int digit_kp(int Nx) { return (2 * Nx + 63) / 64 * 64; }
+
+void launch_table_rowexp(const Geometry& g, int64_t row0, int64_t nrows, const double* Yv, const double* Yd,
+                         int16_t* rexp, cudaStream_t s) {
+  int64_t blocks = (nrows + 7) / 8;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  if (blocks < 1) blocks = 1;
+  table_rowexp_kernel<<<(unsigned)blocks, 256, 0, s>>>(g.Nl, g.Nx, g.dx, row0, nrows, Yv, Yd, rexp);
+  count_launches(1);
+}
+
+void launch_table_digits(const Geometry& g, int64_t row0, int64_t nrows, const double* Yv, const double* Yd,
+                         const int16_t* rexp, uint8_t* dig, cudaStream_t s) {
+  const int Kp = digit_kp(g.Nx);
+  const int64_t total = nrows * (Kp / 4);
+  int64_t blocks = (total + 255) / 256;
+  if (blocks > 148 * 64) blocks = 148 * 64;
+  if (blocks < 1) blocks = 1;
+  table_digits_kernel<<<(unsigned)blocks, 256, 0, s>>>(g.Nl, g.Nx, Kp, g.dx, row0, nrows, Yv, Yd, rexp,
+                                                       (int64_t)g.Nlm * Kp, dig);
+  count_launches(1);
+}
+
+void launch_table_decode(const Geometry& g, int which, int64_t r0, int64_t n, const uint8_t* dig,
+                         const int16_t* rexp, double* out, cudaStream_t s) {
+  const int Kp = digit_kp(g.Nx);
+  int64_t blocks = (n * g.Nx + 255) / 256;
+  if (blocks > 148 * 64) blocks = 148 * 64;
+  if (blocks < 1) blocks = 1;
+  table_decode_kernel<<<(unsigned)blocks, 256, 0, s>>>(g.Nl, g.Nx, Kp, g.dx, which, r0, n, dig,
+                                                       (int64_t)g.Nlm * Kp, rexp, out);
+  count_launches(1);
+}
+
+void launch_fold_scale(const Geometry& g, const Workspace& ws, int16_t* cexp, cudaStream_t s) {
+  fold_scale_kernel<<<1, kScaleThreads, 0, s>>>(g.nbins, g.Nx, ws.piece_first, ws.wsum, cexp);
+  count_launches(1);
+}
+
+void launch_fold_digits(const Geometry& g, const Workspace& ws, const int16_t* cexp, int map, int ncols,
+                        uint8_t* fdig, cudaStream_t s) {
+  const int Kp = digit_kp(g.Nx);
+  dim3 grid((g.Nx + 31) / 32, (g.Nl + 31) / 32);
+  constexpr int kStageBytes = 32 * 2 * 4 * 4 * 2 * 32;
+  cudaFuncSetAttribute(fold_digits_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStageBytes);
+  cudaFuncSetAttribute(fold_digits_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStageBytes);
+  if (ws.partial_f32)
+    fold_digits_kernel<float><<<grid, 1024, kStageBytes, s>>>(g.Nl, g.Nx, g.nbins, Kp, ws.piece_first,
+                                                    reinterpret_cast<const float*>(ws.partial), cexp, map, ncols, fdig);
+  else
+    fold_digits_kernel<double><<<grid, 1024, kStageBytes, s>>>(g.Nl, g.Nx, g.nbins, Kp, ws.piece_first, ws.partial, cexp, map,
+                                                     ncols, fdig);
+  count_launches(1);
+}
+
+}  // namespace dsht

@@ -17,6 +17,8 @@
 #include <stdint.h>
 #include <stddef.h>
 
+#include <vector>
+
 #include "../../include/dsht.h"
 
 #define DSHT_KEY_DROP 0xffffffffu
@@ -50,6 +52,14 @@ struct MapOut {
   double* equ[kMaxPass];
   double* pol[kMaxPass];
   const int* heavy_n[kMaxPass];
+};
+
+// Output pointers of one tensor-core contraction pass (contract_tc.cu): map k's equatorial
+// alm to equ[k], its rotated-polar alm to pol[k] (2 Nlm doubles each).
+constexpr int kTcMaxMaps = 8;
+struct TcOut {
+  double* equ[kTcMaxMaps];
+  double* pol[kTcMaxMaps];
 };
 
 // Heavy nodes of the FP32-table contraction (heavy.cu): a (half, node) holding more than
@@ -94,7 +104,10 @@ struct Workspace {
   int* npieces;         // [1]
   unsigned* flags;      // [1]
   double* partial;      // [pmax][8][Nl]
-  double* fold;         // [fold_slots][Nl][4][Nx][4]
+  double* fold;         // [fold_slots][Nl][4][Nx][4]; the tensor-core route's fold digits
+                        // [Nl][2][4][4 tc_maps][Kp] (int8) share this region
+  int16_t* cexp;        // [tc_maps][2] fold column scale exponents (tensor-core route)
+  int tc_maps;          // maps one tensor-core contraction pass can hold
   uint8_t* tile_live;   // [2][ceil(Nx/128)] tiles of the fallback contraction
   uint8_t* tile_live2;  // [2][ceil(Nx/256)] tiles of the streaming contraction
   double* alm_equ;      // [Nlm][2]
@@ -114,13 +127,14 @@ struct Workspace {
 // fold_slots: folds held at once (one contraction pass); multi: add the records of
 // multi-transform calls (gather indices, rotation and flag slots).
 size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* base, Workspace* ws,
-                        int fold_slots = 1, bool multi = false);
+                        int fold_slots = 1, bool multi = false, int tc_maps = 1);
 int default_piece_max(const Geometry& g, int64_t N);
 int plan_piece_max(const dsht_plan_s* p, int64_t N);
 // How a transform of N points runs on a plan: tensor-core bin sums (tc), FP32 tables
 // (f32_tables), streamed contraction (streamed; otherwise the FP64 fallback kernel).
 struct Route {
   bool tc, f32_tables, streamed;
+  bool digits;  // tensor-core contraction of the digit tables (contract_tc.cu)
 };
 Route plan_route(const dsht_plan_s* p, int64_t N);
 int plan_maps_per_pass(const dsht_plan_s* p);
@@ -140,6 +154,25 @@ int tc_inner_factor(int Nl);
 // Fold of the current map into ws.fold; with an FP32 fold, `heavy` ([2][Nx] flags or null)
 // marks the (half, node) entries written as zeros.
 void launch_fold(const Geometry& g, const Workspace& ws, cudaStream_t s, const uint8_t* heavy = nullptr);
+// Digit tables and folds (digits.cu) and the tensor-core contraction (contract_tc.cu).
+int digit_kp(int Nx);                   // bytes per digit row: 2 Nx rounded up to 64
+constexpr int kTcMaxNx = 8192;          // S32 class sums stay below 2^31 for 2 Nx <= 16384
+void launch_tables_cols(const Geometry& g, int m0, int m1, double* Yv, double* Yd, cudaStream_t s);
+void launch_table_rowexp(const Geometry& g, int64_t row0, int64_t nrows, const double* Yv, const double* Yd,
+                         int16_t* rexp, cudaStream_t s);
+void launch_table_digits(const Geometry& g, int64_t row0, int64_t nrows, const double* Yv, const double* Yd,
+                         const int16_t* rexp, uint8_t* dig, cudaStream_t s);
+void launch_table_decode(const Geometry& g, int which, int64_t r0, int64_t n, const uint8_t* dig,
+                         const int16_t* rexp, double* out, cudaStream_t s);
+void launch_fold_scale(const Geometry& g, const Workspace& ws, int16_t* cexp, cudaStream_t s);
+void launch_fold_digits(const Geometry& g, const Workspace& ws, const int16_t* cexp, int map, int ncols,
+                        uint8_t* fdig, cudaStream_t s);
+int make_table_digit_tmap(CUtensorMap* tm, const uint8_t* dig, int Nx, int64_t Nlm);
+std::vector<uint32_t> tc_items(int Nl);
+int launch_contract_tc(const Geometry& g, const CUtensorMap& tmA, const uint32_t* items, int nitems,
+                       const int16_t* rexp, const uint8_t* fdig, int fdig_cols, const int16_t* cexp, int nmaps,
+                       const TcOut& out, unsigned* flags, cudaStream_t s);
+
 // Heavy nodes of fold slot `slot`: flags and list from the per-piece |w| sums (ws.wsum).
 void launch_heavy_select(const Geometry& g, const Workspace& ws, int slot, cudaStream_t s);
 // Their FP64 contribution for every (l, m) stored (not added) into alm_equ / alm_pol, from
@@ -164,9 +197,9 @@ void launch_contract_pass(const Geometry& g, bool mixed, const CUtensorMap& tmv,
 int make_table_tmap(CUtensorMap* tm, const void* base, size_t elem_bytes, int Nx, int64_t Nlm, int rows = 0);
 void launch_tables_to_f32(const Geometry& g, const double* Yv, const double* Yd, float* Yv32, float* Yd32,
                           cudaStream_t s);
-// A table in the JAX path's layout out[m][l - m][j] (Nl x Nl x Nx doubles, zeros where
-// l >= Nl) on the device, from the FP64 table t64 or, when it is null, the FP32 table t32.
-void launch_table_mlayout(const Geometry& g, const double* t64, const float* t32, double* out, cudaStream_t s);
+// An FP64 table in the JAX path's layout out[m][l - m][j] (Nl x Nl x Nx doubles, zeros
+// where l >= Nl) on the device.
+void launch_table_mlayout(const Geometry& g, const double* t64, double* out, cudaStream_t s);
 void launch_rotate_back(const Geometry& g, const double* alm_rot, const double* alm_add,
                         double* alm_out, const unsigned* flags, cudaStream_t s);
 // alm io[k] += R(rot[k]) for k < nmaps <= kMaxRot (a map without polar points is left as it is).
@@ -206,6 +239,14 @@ struct dsht_plan_s {
   alignas(64) CUtensorMap tmYv, tmYd, tmYv32, tmYd32;
   alignas(64) CUtensorMap tmYv32h, tmYd32h;  // FP32 tables, 16-row boxes (passes of 3-4 folds)
   bool tm64 = false, tm32 = false;
+  // Digit tables of the tensor-core contraction (digits.cu): 4 planes [Nlm][Kp] int8 in
+  // rows grouped by parity, row exponents, the work items and the TMA map of the planes.
+  uint8_t* dig = nullptr;
+  int16_t* rexp = nullptr;
+  uint32_t* tc_items = nullptr;
+  int tc_nitems = 0;
+  alignas(64) CUtensorMap tmDig;
+  bool tmdig = false;
   // Plan-owned buffers, grown on demand (used when the caller passes no workspace and by
   // the host-pointer entry points).
   void* ws = nullptr;

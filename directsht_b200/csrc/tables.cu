@@ -14,11 +14,12 @@ namespace {
 constexpr int kTableThreads = 256;
 
 // TO = double: the FP64 tables; TO = float: the same FP64 values rounded once to float.
+// Columns m = m0 + blockIdx.y; row r of the tables lands at (r - row_base) * Nx.
 template <typename TO>
 __global__ void __launch_bounds__(kTableThreads)
-table_kernel(int Nl, int Nx, double step, TO* __restrict__ Yv, TO* __restrict__ Yd) {
+table_kernel(int Nl, int Nx, double step, TO* __restrict__ Yv, TO* __restrict__ Yd, int m0, int64_t row_base) {
   extern __shared__ double smem_raw[];
-  const int m = blockIdx.y;
+  const int m = m0 + blockIdx.y;
   Coef* cf = reinterpret_cast<Coef*>(smem_raw);       // [Nl]
   double* smm = smem_raw + (size_t)Nl * 6;            // [m+1] sqrt(1 - 1/(2m'))
   for (int l = threadIdx.x; l < Nl; l += blockDim.x) cf[l] = make_coef(l, m);
@@ -31,7 +32,7 @@ table_kernel(int Nl, int Nx, double step, TO* __restrict__ Yv, TO* __restrict__ 
   node_x(j, step, &x, &omx2, &sx);               // numpy: arange(Nx) * (xmax/(Nx-1))
   const double ymm = diag_value(m, sx, smm);     // Y_mm (sht/legendre_py.py:28-30)
 
-  const int64_t row0 = hp_index(m, m, Nl);
+  const int64_t row0 = hp_index(m, m, Nl) - row_base;
   TO* yv = Yv + row0 * Nx + j;
   TO* yd = Yd + row0 * Nx + j;
   ColumnState st;
@@ -74,12 +75,9 @@ __global__ void table_mlayout_kernel(int Nl, int Nx, const TI* __restrict__ t, d
 
 }  // namespace
 
-void launch_table_mlayout(const Geometry& g, const double* t64, const float* t32, double* out, cudaStream_t s) {
+void launch_table_mlayout(const Geometry& g, const double* t64, double* out, cudaStream_t s) {
   dim3 grid((g.Nx + 255) / 256 < 8 ? (g.Nx + 255) / 256 : 8, g.Nl, g.Nl);
-  if (t64)
-    table_mlayout_kernel<double><<<grid, 256, 0, s>>>(g.Nl, g.Nx, t64, out);
-  else
-    table_mlayout_kernel<float><<<grid, 256, 0, s>>>(g.Nl, g.Nx, t32, out);
+  table_mlayout_kernel<double><<<grid, 256, 0, s>>>(g.Nl, g.Nx, t64, out);
   count_launches(1);
 }
 
@@ -91,16 +89,24 @@ void launch_tables_to_f32(const Geometry& g, const double* Yv, const double* Yd,
 }
 
 template <typename TO>
-static void tables_launch(const Geometry& g, TO* Yv, TO* Yd, cudaStream_t s) {
+static void tables_launch(const Geometry& g, TO* Yv, TO* Yd, int m0, int m1, cudaStream_t s) {
   const size_t smem = (size_t)g.Nl * sizeof(Coef) + (size_t)(g.Nl + 1) * sizeof(double);
   cudaFuncSetAttribute(table_kernel<TO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  dim3 grid((g.Nx + kTableThreads - 1) / kTableThreads, g.Nl);
-  table_kernel<TO><<<grid, kTableThreads, smem, s>>>(g.Nl, g.Nx, g.dx, Yv, Yd);
+  dim3 grid((g.Nx + kTableThreads - 1) / kTableThreads, m1 - m0);
+  table_kernel<TO><<<grid, kTableThreads, smem, s>>>(g.Nl, g.Nx, g.dx, Yv, Yd, m0, hp_index(m0, m0, g.Nl));
   count_launches(1);
 }
 
-void launch_tables(const Geometry& g, double* Yv, double* Yd, cudaStream_t s) { tables_launch(g, Yv, Yd, s); }
+void launch_tables(const Geometry& g, double* Yv, double* Yd, cudaStream_t s) {
+  tables_launch(g, Yv, Yd, 0, g.Nl, s);
+}
 
-void launch_tables_f32(const Geometry& g, float* Yv, float* Yd, cudaStream_t s) { tables_launch(g, Yv, Yd, s); }
+void launch_tables_f32(const Geometry& g, float* Yv, float* Yd, cudaStream_t s) {
+  tables_launch(g, Yv, Yd, 0, g.Nl, s);
+}
+
+void launch_tables_cols(const Geometry& g, int m0, int m1, double* Yv, double* Yd, cudaStream_t s) {
+  tables_launch(g, Yv, Yd, m0, m1, s);
+}
 
 }  // namespace dsht

@@ -29,7 +29,7 @@ class DirectSHT:
     """Brute-force spherical harmonic transforms on a B200 (``sht/sht.py:30``)."""
 
     def __init__(self, Nell, Nx, xmax=0.75, dflt_type="float64", null_unphysical=True, device=None,
-                 precision="fp64", f32_tables=False, table_layout="healpix"):
+                 precision="fp64", compact_tables=False, table_layout="healpix", f32_tables=None):
         """Build the FP64 Ylm/dYlm tables on the GPU (``sht/sht.py:32-56``).
 
         :param Nell: number of ells (and m's).
@@ -40,15 +40,19 @@ class DirectSHT:
             the JAX layout's unphysical entries (l >= Nell) always read as zero.
         :param device: CUDA device (default: the current one).
         :param precision: "fp64" (agrees with the reference to ~1e-15), "mixed" (tensor-core
-            per-bin sums and FP32 tables: fastest, <= 1e-7 x max|alm| for point sets spread over
-            many x bins) or "mixed_f64_tables" (tensor-core sums, FP64 tables: <= 1e-7 also when
-            the weight concentrates in one bin).
-        :param f32_tables: keep only FP32 copies of the tables (half the memory; the plan then
-            runs at precision "mixed" only).
+            per-bin sums and a tensor-core contraction of 4-byte fixed-point copies of the
+            tables: fastest, <= 1e-7 x max|alm|) or "mixed_f64_tables" (tensor-core sums, FP64
+            tables through the CUDA-core contraction).
+        :param compact_tables: keep only the 4-byte fixed-point tables (half the memory of the
+            FP64 pair; the plan then runs at precision "mixed" only, and get_Ylm/get_dYlm return
+            the stored values, within 2^-31 of each row's largest entry).
+        :param f32_tables: former name of ``compact_tables``.
         :param table_layout: layout of the host attributes ``Yv``/``Yd``: "healpix" (Nlm, Nx) rows
             in Healpy order, as the reference's numpy path stores them, or "jax" (Nell, Nell, Nx)
             indexed [m, ell - m, :], as its JAX path stores them (``sht/legendre_jax.py:14-25``).
         """
+        if f32_tables is not None:
+            compact_tables = f32_tables
         if table_layout not in ("healpix", "jax"):
             raise ValueError(f"table_layout must be 'healpix' or 'jax', not {table_layout!r}")
         self.table_layout = table_layout
@@ -64,11 +68,11 @@ class DirectSHT:
         self.x = xx
         self._plan = ct.c_void_p()
         with torch.cuda.device(self.device):
-            flags = L.DSHT_PLAN_F32_TABLES if f32_tables else L.DSHT_PLAN_DEFAULT
+            flags = L.DSHT_PLAN_F32_TABLES if compact_tables else L.DSHT_PLAN_DEFAULT
             L.check(self._lib.dsht_plan_create(self.Nell, self.Nx, self.xmax, flags, ct.byref(self._plan)))
         self.precision = None
-        self._f32_only = bool(f32_tables)
-        self.set_precision("mixed" if f32_tables else precision)
+        self._f32_only = bool(compact_tables)
+        self.set_precision("mixed" if compact_tables else precision)
         self._Yv = None
         self._Yd = None
         self.verbose_timing = None

@@ -131,19 +131,23 @@ def test_enqueue_batch_in_cuda_graph():
     assert all(d._lib.dsht_status(int(f), L.DSHT_MODE_CALL) == L.DSHT_OK for f in status.cpu().numpy())
 
 
-def test_f32_table_plan():
-    """A plan holding FP32 tables only: mixed results within 1e-7 of the oracle, small
-    transforms included (FP64 bin sums on FP32 tables); its rows are the FP64 rows rounded."""
+def test_compact_table_plan():
+    """A plan holding the compact (4-byte fixed-point digit) tables only: mixed results
+    within 1e-7 of the oracle, small transforms included (FP64 bin sums on the digit
+    tables); its rows are the FP64 rows to within 2^-31 of the row's scale."""
     Nl, Nx = 64, 128
-    d = DirectSHT(Nl, Nx, f32_tables=True)
+    d = DirectSHT(Nl, Nx, compact_tables=True)
     assert d.precision == "mixed"
     with pytest.raises(Exception):
         d.set_precision("fp64")
     tab = O.build_tables(Nl, Nx)
     d64 = DirectSHT(Nl, Nx)
-    for l, m in ((10, 3), (63, 0), (40, 40)):
-        np.testing.assert_array_equal(d.get_Ylm(l, m), d64.get_Ylm(l, m).astype(np.float32).astype(np.float64))
-        np.testing.assert_array_equal(d.get_dYlm(l, m), d64.get_dYlm(l, m).astype(np.float32).astype(np.float64))
+    dx = 0.75 / (Nx - 1)
+    for l, m in ((10, 3), (63, 0), (40, 40), (0, 0), (1, 0)):
+        yv, yd = d64.get_Ylm(l, m), d64.get_dYlm(l, m)
+        scale = max(np.abs(yv).max(), dx * np.abs(yd).max())
+        assert np.abs(d.get_Ylm(l, m) - yv).max() <= 2.0 ** -30 * scale, (l, m)
+        assert np.abs(d.get_dYlm(l, m) - yd).max() <= 2.0 ** -30 * scale / dx, (l, m)
     sets = _sets(6, [50000, 700, 20000])
     got = d.call_batch(sets)
     for i, (th, ph, w) in enumerate(sets):

@@ -117,29 +117,29 @@ def test_mixed_concentrated_weight_vs_oracle(case):
     th = np.arccos(cost)
     ph = rng.uniform(0, 2 * np.pi, N)
     ref = _oracle_basic(Nl, Nx, th, ph, w)
-    for kwargs in (dict(precision="mixed"), dict(f32_tables=True)):
+    for kwargs in (dict(precision="mixed"), dict(compact_tables=True)):
         d = DirectSHT(Nl, Nx, **kwargs)
         a = d.basic_sht(th, ph, w.copy(), verbose=False)
         assert _rel(a, ref) <= TOL_MIXED, (case, kwargs)
 
 
 @pytest.mark.parametrize("N,seed", [(1, 0), (700, 1), (5000, 2)])
-def test_f32_only_plan_few_points_call_vs_oracle(N, seed):
-    """An FP32-only plan (no FP64 tables at all) on a handful of points, polar ones
-    included: every node is heavy, so the result is FP64 throughout."""
+def test_compact_plan_few_points_call_vs_oracle(N, seed):
+    """A compact-table plan (no FP64 tables at all) on a handful of points, polar ones
+    included (FP64 bin sums, tensor-core contraction of the digit tables)."""
     rng = np.random.default_rng(seed)
     Nl, Nx = 96, 192
     th = np.arccos(rng.uniform(-1, 1, N))
     ph = rng.uniform(0, 2 * np.pi, N)
     w = rng.uniform(0.5, 1.5, N)
     ref = O.direct_sht(O.build_tables(Nl, Nx), th, ph, w)
-    d = DirectSHT(Nl, Nx, f32_tables=True)
+    d = DirectSHT(Nl, Nx, compact_tables=True)
     assert _rel(d(th, ph, w), ref) <= TOL_MIXED
 
 
 @pytest.mark.slow
-def test_f32_only_plan_nl2048_concentrated_columns_vs_oracle():
-    """Nl=2048, Nx=4096 with FP32 tables only (68.7 GB, the uneven-batch and serving plans at
+def test_compact_plan_nl2048_concentrated_columns_vs_oracle():
+    """Nl=2048, Nx=4096 with compact tables only (68.7 GB, the uneven-batch and serving plans at
     that size): 40 % of the weight in one bin, the rest spread; columns against the per-m
     oracle."""
     rng = np.random.default_rng(12)
@@ -148,7 +148,7 @@ def test_f32_only_plan_nl2048_concentrated_columns_vs_oracle():
     th = np.arccos(cost)
     ph = rng.uniform(0, 2 * np.pi, N)
     w = rng.uniform(0.5, 1.5, N)
-    d = DirectSHT(Nl, Nx, f32_tables=True)
+    d = DirectSHT(Nl, Nx, compact_tables=True)
     a = d.basic_sht(th, ph, w.copy(), verbose=False)
     cols = {m: O.basic_sht_column(Nl, Nx, 0.75, m, th, ph, w) for m in (0, 1, 2, 700, 1500, 2047)}
     scale = max(np.abs(c).max() for c in cols.values())

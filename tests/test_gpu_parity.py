@@ -47,18 +47,18 @@ def test_full_tables_match_oracle():
     assert _rel(d.Yd, tab.Yd) <= 1e-14
 
 
-@pytest.mark.parametrize("f32_tables", [False, True])
-def test_jax_layout_tables(f32_tables):
+@pytest.mark.parametrize("compact", [False, True])
+def test_jax_layout_tables(compact):
     """Yv/Yd in the JAX path's [m, l-m, :] layout with the unphysical entries nulled
     (sht/legendre_jax.py:14-25): the same rows as the Healpy-order tables, host and device."""
     Nl, Nx = 70, 132
-    d = DirectSHT(Nl, Nx, table_layout="jax", f32_tables=f32_tables)
+    d = DirectSHT(Nl, Nx, table_layout="jax", compact_tables=compact)
     tab = O.build_tables(Nl, Nx)
     for which, ref, host in (("Yv", tab.Yv, d.Yv), ("Yd", tab.Yd, d.Yd)):
         assert host.shape == (Nl, Nl, Nx)
         dev = d.table_on_device(which).cpu().numpy()
         assert np.array_equal(dev, host)
-        tol = 1e-7 if f32_tables else 1e-14
+        tol = 1e-7 if compact else 1e-14
         for m in range(Nl):
             r0 = O.healpy_index(m, m, Nl)
             assert _rel(host[m, :Nl - m], ref[r0:r0 + Nl - m]) <= tol, (which, m)

@@ -15,7 +15,7 @@ pytestmark = pytest.mark.gpu
 def test_served_results_equal_alone_results():
     rng = np.random.default_rng(3)
     timed = poisson_requests(rng, 24, 2000.0, Nls=(32, 64), n_range=(2e3, 1e5), maps=(1, 4))
-    cache = PlanCache(precision="mixed", f32_tables_min_nl=64)  # Nl=64 plans keep FP32 tables only
+    cache = PlanCache(precision="mixed", compact_min_nl=64)  # Nl=64 plans keep compact tables only
     for Nl in (32, 64):
         cache.get(Nl, 2 * Nl)
     srv = Server(GpuExecutor(cache), budget_bytes=2 << 30, slots=4).start()
@@ -49,7 +49,7 @@ def test_budget_smaller_than_mix_still_serves_everything():
 
 @pytest.mark.slow
 def test_served_caps_nl1024_vs_fp64_and_oracle():
-    """Serving-stream requests at Nl=1024, Nx=2048 on the FP32-table plan the server keeps
+    """Serving-stream requests at Nl=1024, Nx=2048 on the compact-table plan the server keeps
     resident, with points in caps of half-angle 0.2 rad (a few hundred x bins) and 0.5 rad:
     every served map within 1e-7 x max|alm| of the FP64 plan, and the transform of map 0's
     equatorial and rotated polar points against the per-m oracle."""
@@ -60,7 +60,7 @@ def test_served_caps_nl1024_vs_fp64_and_oracle():
         th, ph = cap_points(rng, N, alpha)
         w = rng.uniform(0.5, 1.5, (k, N)).astype(np.float32)
         reqs.append((0.0, Request(Nl, Nx, th, ph, w)))
-    cache = PlanCache(precision="mixed", f32_tables_min_nl=1024)
+    cache = PlanCache(precision="mixed", compact_min_nl=1024)
     plan = cache.get(Nl, Nx)
     srv = Server(GpuExecutor(cache), budget_bytes=16 << 30, slots=4).start()
     futs = replay(srv, reqs)
