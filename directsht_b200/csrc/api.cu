@@ -76,7 +76,6 @@ size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* ba
   const int ntile = (g.Nx + tile - 1) / tile;
   Workspace w{};
   w.key = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * n));
-  w.rec = reinterpret_cast<double*>(take(sizeof(double) * 3 * n));
   w.pay = reinterpret_cast<double*>(take(sizeof(double) * kRec * n));
   const bool maps = multi;
   if (maps) {

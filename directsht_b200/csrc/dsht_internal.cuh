@@ -3,7 +3,6 @@
 // Data layout in HBM (Nlm = Nl(Nl+1)/2, rows in Healpy order m(2Nl-1-m)/2 + l):
 //   tables   Yv, Yd      double [Nlm][Nx]          (sht/sht.py:50-56 layout, numpy path)
 //   points   key         uint32 [N]                set*(Nx-1) + bin, or DSHT_KEY_DROP
-//            record      double [N][3]             (cos phi, sin phi, t) in input order
 //            sorted      double [N][4]             (cos phi, sin phi, w, t) by key
 //   pieces   <= 1 bin each, <= piece_max points    (key, start, len)
 //   partial  double [piece][8][Nl]                 (k, re/im) bin sums for every m
@@ -85,7 +84,6 @@ struct StatusOut {
 // Workspace carve-up for one execute call.
 struct Workspace {
   uint32_t* key;        // [N]
-  double* rec;          // [N][3]
   double* pay;          // [N][4] sorted records (cos phi, sin phi, w, t)
   uint32_t* sidx;       // [N] input index of each sorted slot (multi-map transforms)
   uint32_t* piecemax;   // [pmax] largest |w h_k| of the piece's points (float bits)

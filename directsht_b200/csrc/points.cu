@@ -6,13 +6,14 @@
 // sht/sht.py:212) and t = (|x| - x_j)/dx (sht/sht.py:221); the payload is cos phi, sin phi
 // and w * {(2t+1)(1-t)^2, t(1-t)^2, t^2(3-2t), t^2(t-1)} (sht/sht.py:239-240).
 //
-// Sort: key = set*(Nx-1) + bin.  The count pass classifies every point once (key, cos phi,
-// sin phi, t in input order) and histograms the keys in shared memory (one global add per
-// live key and block); a one-block exclusive scan cuts every key into pieces of at most
-// piece_max points; the scatter pass reserves a contiguous range per key and block with
-// one global add and writes each point's 32-byte record (cos phi, sin phi, w, t) -- one
-// DRAM sector -- to its sorted slot; the bin-sum kernels form w h_k(t) themselves.  HBM
-// bound: about 16 B read + 28 B written (count), 36 B read + 32 B written (scatter) per point.
+// Sort: key = set*(Nx-1) + bin.  The count pass bins every point (its key, 4 bytes) and
+// histograms the keys in shared memory (one global add per live key and block); a one-block
+// exclusive scan cuts every key into pieces of at most piece_max points; the scatter pass
+// reserves a contiguous range per key and block with one global add, recomputes each
+// point's 32-byte record (cos phi, sin phi, w, t) -- one DRAM sector -- from its inputs and
+// writes it to its sorted slot; the bin-sum kernels form w h_k(t) themselves.  HBM bytes
+// per point: 12-16 read + 4 written (count), 28 read + 32 written (scatter), against the
+// algorithmic 24 read + 32 written.
 #include "dsht_internal.cuh"
 
 namespace dsht {
@@ -21,71 +22,49 @@ namespace {
 constexpr int kPointThreads = 256;
 constexpr int kScatterTile = 16384;  // points per block in the scatter pass
 
-struct PointOut {
+// The binning of one point: key = set * nbins + bin (DSHT_KEY_DROP when it is in no set)
+// and its flag bits.  x = cos(theta) for equatorial points; a polar point (|cos theta| >=
+// xmax in __call__) is rotated by +90 deg about y, n = (s cos p, s sin p, c) -> (c, s sin p,
+// -s cos p), and binned by its rotated x = -sin(theta) cos(phi) -- the cosine of the rotated
+// theta that the reference bins (sht/sht.py:190), without the acos/cos round trip.
+// st, c = sin, cos of theta; cp = cos phi (read for polar points only).  The scatter pass
+// computes x with the same operations, so the two passes agree on it bit for bit.
+struct KeyOut {
   uint32_t key;
-  double cphi, sphi;  // cos, sin of the (rotated) azimuth
-  double t;
   unsigned flag;
+  double x;  // the signed x that was binned
 };
 
-// sp, cp: sin and cos of the azimuth (both sets need them: computed once, before the
-// branch, so that a warp with polar points does not evaluate them twice); inv_dx = 1/dx
-// gives the bin guess that the exact comparisons below correct.
-__device__ __forceinline__ PointOut classify(const Geometry& g, double inv_dx, int mode, double th, double sp,
-                                             double cp) {
-  PointOut o;
-  o.flag = 0;
+__device__ __forceinline__ KeyOut point_key(const Geometry& g, double inv_dx, int mode, double th, double st, double c,
+                                            const double* phi_p) {
+  KeyOut o;
   o.key = DSHT_KEY_DROP;
-  o.cphi = 1.0;
-  o.sphi = 0.0;
-  o.t = 0.0;
-  const double c = cos(th);
-  double x;        // signed x used for binning
+  o.flag = 0;
+  o.x = 0.0;
+  double x;
   int set;
-  if (mode == DSHT_MODE_CALL) {
-    const double xv = fabs(c);
-    if (xv >= g.xmax) {
-      // Rotate n = (s cos p, s sin p, c) to (c, s sin p, -s cos p).
-      const double st = sin(th);
-      const double nx = st * cp, ny = st * sp;
-      const double xr = -nx;
-      // azimuth of the rotated point: atan2(ny, c), kept as its cosine and sine
-      const double rho = sqrt(ny * ny + c * c);
-      if (rho > 0.0) {
-        o.cphi = c / rho;
-        o.sphi = ny / rho;
-      }
-      const double tr = acos(fmin(fmax(xr, -1.0), 1.0));
-      if (!(tr > g.acos_xmax && tr < g.acos_mxmax)) {
-        o.flag = kFlagPolarRange;
-        return o;
-      }
-      x = cos(tr);  // the reference takes cos of the rotated theta (sht/sht.py:190)
-      set = 2;
-      o.flag = kFlagHasPolar;
-    } else if (xv < g.xmax) {
-      if (!(th >= 0.0 && th > g.acos_xmax && th < g.acos_mxmax)) {
-        o.flag = kFlagThetaRange;
-        return o;
-      }
-      x = c;
-      set = 0;
-      o.cphi = cp;
-      o.sphi = sp;
-    } else {
-      return o;  // NaN theta: in neither set (sht/sht.py:129-130)
+  const double xv = fabs(c);
+  if (mode == DSHT_MODE_CALL && xv >= g.xmax) {
+    double sp, cp;
+    sincos(*phi_p, &sp, &cp);
+    x = -__dmul_rn(st, cp);
+    if (!(x < g.xmax && x > -g.xmax)) {  // the rotated point is still polar
+      o.flag = kFlagPolarRange;
+      return o;
     }
+    set = 2;
+    o.flag = kFlagHasPolar;
+  } else if (mode == DSHT_MODE_CALL && !(xv < g.xmax)) {
+    return o;  // NaN theta: in neither set (sht/sht.py:129-130)
   } else {
-    if (!(th >= 0.0 && th > g.acos_xmax && th < g.acos_mxmax)) {
+    if (!(th >= 0.0 && th > g.acos_xmax && th < g.acos_mxmax)) {  // sht/sht.py:171-172
       o.flag = kFlagThetaRange;
       return o;
     }
     x = c;
     set = 0;
-    o.cphi = cp;
-    o.sphi = sp;
   }
-  if (!(x >= 0.0)) set += 1;          // x < 0 half (sht/sht.py:193)
+  if (!(x >= 0.0)) set += 1;  // x < 0 half (sht/sht.py:193)
   const double ax = fabs(x);
   // digitize: x_j <= ax < x_{j+1} with x_j = j * dx exactly as numpy builds the grid.
   int j = (int)(ax * inv_dx);
@@ -97,15 +76,16 @@ __device__ __forceinline__ PointOut classify(const Geometry& g, double inv_dx, i
     o.flag = (set >= 2) ? kFlagPolarRange : kFlagThetaRange;
     return o;
   }
-  o.t = __ddiv_rn(__dadd_rn(ax, -(double)j * g.dx), g.dx);
   o.key = (uint32_t)(set * g.nbins + j);
+  o.x = x;
   return o;
 }
 
+// Count pass: the key of every point (4 bytes written) and a shared-memory histogram of the
+// keys (one global add per live key and block).  Reads theta, and phi of polar points only.
 __global__ void __launch_bounds__(kPointThreads)
 count_kernel(Geometry g, int mode, const double* __restrict__ theta, const double* __restrict__ phi,
-             int64_t N, uint32_t* __restrict__ keys, double* __restrict__ rec, uint32_t* __restrict__ count,
-             unsigned* __restrict__ flags) {
+             int64_t N, uint32_t* __restrict__ keys, uint32_t* __restrict__ count, unsigned* __restrict__ flags) {
   extern __shared__ uint32_t hist[];
   for (int k = threadIdx.x; k < g.nkeys; k += blockDim.x) hist[k] = 0;
   __syncthreads();
@@ -113,13 +93,11 @@ count_kernel(Geometry g, int mode, const double* __restrict__ theta, const doubl
   const double inv_dx = 1.0 / g.dx;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
-    double sp, cp;
-    sincos(phi[i], &sp, &cp);
-    PointOut o = classify(g, inv_dx, mode, theta[i], sp, cp);
+    const double th = theta[i];
+    double st, c;
+    sincos(th, &st, &c);
+    const KeyOut o = point_key(g, inv_dx, mode, th, st, c, phi + i);
     keys[i] = o.key;
-    rec[3 * i] = o.cphi;
-    rec[3 * i + 1] = o.sphi;
-    rec[3 * i + 2] = o.t;
     fl |= o.flag;
     if (o.key != DSHT_KEY_DROP) atomicAdd(&hist[o.key], 1u);
   }
@@ -209,19 +187,21 @@ __device__ __forceinline__ uint32_t gmax_bits(const double* h) {
   return __float_as_uint((float)fmax(fmax(fabs(h[0]), fabs(h[1])), fmax(fabs(h[2]), fabs(h[3]))));
 }
 
+// Scatter pass: every point's 32-byte record (cos phi, sin phi, w, t) -- one DRAM sector --
+// to its sorted slot.  The record is recomputed from theta, phi, w and the key of the count
+// pass: for a rotated polar point the azimuth of (c, s sin p, -s cos p), kept as its cosine
+// and sine (c / rho, s sin p / rho), and t = (|x| - x_j) / dx (sht/sht.py:221).
 template <typename WT>
 __global__ void __launch_bounds__(kPointThreads)
-scatter_kernel(Geometry g, const WT* __restrict__ w, int64_t N, const uint32_t* __restrict__ keys,
-               const double* __restrict__ rec, uint32_t* __restrict__ cursor, double* __restrict__ pay,
-               uint32_t* __restrict__ sidx) {
+scatter_kernel(Geometry g, const double* __restrict__ theta, const double* __restrict__ phi,
+               const WT* __restrict__ w, int64_t N, const uint32_t* __restrict__ keys, uint32_t* __restrict__ cursor,
+               double* __restrict__ pay, uint32_t* __restrict__ sidx) {
   extern __shared__ uint32_t loc[];  // [nkeys] local counts, then local bases
   const int64_t lo = (int64_t)blockIdx.x * kScatterTile;
   const int64_t hi = min(lo + (int64_t)kScatterTile, N);
   for (int k = threadIdx.x; k < g.nkeys; k += blockDim.x) loc[k] = 0;
   __syncthreads();
-  // kUnroll points per thread and step: their loads are issued together, so each thread
-  // keeps several DRAM reads in flight (one point at a time leaves the pass latency bound).
-  constexpr int kUnroll = 8;
+  constexpr int kUnroll = 4;
   const int64_t step = (int64_t)kUnroll * blockDim.x;
   for (int64_t b = lo + threadIdx.x; b < hi; b += step) {
     uint32_t k[kUnroll];
@@ -240,28 +220,46 @@ scatter_kernel(Geometry g, const WT* __restrict__ w, int64_t N, const uint32_t* 
     if (c) loc[k] = atomicAdd(&cursor[k], c);
   }
   __syncthreads();
+  const int polar_key0 = 2 * g.nbins;
   for (int64_t b = lo + threadIdx.x; b < hi; b += step) {
     uint32_t k[kUnroll];
-    double c[kUnroll], sn[kUnroll], t[kUnroll], wi[kUnroll];
+    double th[kUnroll], ph[kUnroll], wi[kUnroll];
 #pragma unroll
     for (int u = 0; u < kUnroll; ++u) {
       const int64_t i = b + (int64_t)u * blockDim.x;
       k[u] = DSHT_KEY_DROP;
       if (i < hi) {
         k[u] = keys[i];
-        c[u] = rec[3 * i];
-        sn[u] = rec[3 * i + 1];
-        t[u] = rec[3 * i + 2];
+        th[u] = theta[i];
+        ph[u] = phi[i];
         wi[u] = (double)w[i];
       }
     }
 #pragma unroll
     for (int u = 0; u < kUnroll; ++u) {
       if (k[u] == DSHT_KEY_DROP) continue;
+      double st, c, sp, cp;
+      sincos(th[u], &st, &c);
+      sincos(ph[u], &sp, &cp);
+      double cphi = cp, sphi = sp, x = c;
+      if ((int)k[u] >= polar_key0) {
+        x = -__dmul_rn(st, cp);
+        const double ny = st * sp;
+        const double rho = sqrt(ny * ny + c * c);
+        cphi = 1.0;
+        sphi = 0.0;
+        if (rho > 0.0) {
+          const double ir = 1.0 / rho;
+          cphi = c * ir;
+          sphi = ny * ir;
+        }
+      }
+      const int j = (int)(k[u] % (uint32_t)g.nbins);
+      const double t = __ddiv_rn(__dadd_rn(fabs(x), -(double)j * g.dx), g.dx);
       const uint32_t pos = atomicAdd(&loc[k[u]], 1u);
       double2* out = reinterpret_cast<double2*>(pay + (size_t)kRec * pos);  // one 32-byte sector
-      out[0] = make_double2(c[u], sn[u]);
-      out[1] = make_double2(wi[u], t[u]);
+      out[0] = make_double2(cphi, sphi);
+      out[1] = make_double2(wi[u], t);
       if (sidx) sidx[pos] = (uint32_t)(b + (int64_t)u * blockDim.x);
     }
   }
@@ -346,8 +344,8 @@ void launch_points(const Geometry& g, const double* theta, const double* phi, co
   if (N > 0) {
     int64_t blocks = (N + kPointThreads * 8 - 1) / (kPointThreads * 8);
     if (blocks > 148 * 8) blocks = 148 * 8;
-    count_kernel<<<(unsigned)blocks, kPointThreads, hsmem, s>>>(g, mode, theta, phi, N, ws.key, ws.rec,
-                                                               ws.count, ws.flags);
+    count_kernel<<<(unsigned)blocks, kPointThreads, hsmem, s>>>(g, mode, theta, phi, N, ws.key, ws.count,
+                                                               ws.flags);
     count_launches(1);
   }
   scan_kernel<<<1, kScanThreads, 0, s>>>(g.nkeys, g.nbins, ws.piece_max, ws.pmax, ws.count, ws.offset,
@@ -358,7 +356,8 @@ void launch_points(const Geometry& g, const double* theta, const double* phi, co
     const int64_t blocks = (N + kScatterTile - 1) / kScatterTile;
     auto go = [&](auto kern, const auto* wp) {
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem);
-      kern<<<(unsigned)blocks, kPointThreads, hsmem, s>>>(g, wp, N, ws.key, ws.rec, ws.cursor, ws.pay, ws.sidx);
+      kern<<<(unsigned)blocks, kPointThreads, hsmem, s>>>(g, theta, phi, wp, N, ws.key, ws.cursor, ws.pay,
+                                                          ws.sidx);
     };
     if (w_f32) go(scatter_kernel<float>, reinterpret_cast<const float*>(w));
     else go(scatter_kernel<double>, reinterpret_cast<const double*>(w));
