@@ -259,18 +259,19 @@ int run_after_sort(dsht_plan_s* p, int64_t N, int mode, double* alm, const Works
                                     ws.flags, s))
       return rc;
   } else {
-  w2.fold_f32 = f32_tables ? 1 : 0;
-  mark(DSHT_STAGE_FOLD);
-  if (f32_tables) launch_heavy_select(g, w2, 0, s);
-  launch_fold(g, w2, s, f32_tables ? w2.heavy_flag : nullptr);
-  mark(DSHT_STAGE_CONTRACT);
-  if (f32_tables) {
-    launch_heavy_otf(g, w2, 0, ws.alm_equ, ws.alm_pol, s);
-    launch_contract_stream(g, true, p->tmYv32, p->tmYd32, ws, s, ws.heavy_n);
-  } else if (p->tm64)
-    launch_contract_stream(g, false, p->tmYv, p->tmYd, ws, s);
-  else
-    launch_contract_fp64(g, p->Yv, p->Yd, ws, s);
+    w2.fold_f32 = f32_tables ? 1 : 0;
+    mark(DSHT_STAGE_FOLD);
+    if (f32_tables) launch_heavy_select(g, w2, 0, s);
+    launch_fold(g, w2, s, f32_tables ? w2.heavy_flag : nullptr);
+    mark(DSHT_STAGE_CONTRACT);
+    if (f32_tables) {
+      launch_heavy_otf(g, w2, 0, ws.alm_equ, ws.alm_pol, s);
+      launch_contract_stream(g, true, p->tmYv32, p->tmYd32, ws, s, ws.heavy_n);
+    } else if (p->tm64) {
+      launch_contract_stream(g, false, p->tmYv, p->tmYd, ws, s);
+    } else {
+      launch_contract_fp64(g, p->Yv, p->Yd, ws, s);
+    }
   }
   mark(DSHT_STAGE_ROTATE);
   if (mode == DSHT_MODE_CALL) {

@@ -30,6 +30,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <atomic>
 
 #include "dsht_internal.cuh"
 #include "tc_ptx.cuh"
@@ -67,7 +68,8 @@ template <int NC>
 __global__ void __launch_bounds__(kTcThreads, 1)
 contract_tc_kernel(int Nl, int nchunks, const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                    const uint32_t* __restrict__ items, int nitems, const int16_t* __restrict__ rexp,
-                   const int16_t* __restrict__ cexp, int ncols, const TcOut out, unsigned* __restrict__ err) {
+                   const int16_t* __restrict__ cexp, int ncols, const TcOut out, unsigned* __restrict__ err,
+                   int stall) {
   using L = TcLayout<NC>;
   constexpr int S = L::kStages;
   extern __shared__ uint8_t smem_raw[];
@@ -188,7 +190,9 @@ contract_tc_kernel(int Nl, int nchunks, const __grid_constant__ CUtensorMap tmA,
           }
           tc::mma_commit(&empty[s]);
         }
-        if (ok) tc::mma_commit(&tfull[b]);
+        // stall != 0 (test hook): block 0 never signals its first tile, so the epilogue's
+        // bounded wait runs out and the launch reports kFlagTimeout
+        if (ok && !(stall && blockIdx.x == 0 && iter == 0)) tc::mma_commit(&tfull[b]);
       }
       // every MMA issued has completed before TMEM is released
       tc::mma_commit(drain);
@@ -253,6 +257,9 @@ contract_tc_kernel(int Nl, int nchunks, const __grid_constant__ CUtensorMap tmA,
   if (warp == 1) tc::tmem_dealloc(tmem, L::kTmemCols);
 }
 
+// Test hook (dsht_test_stall_next_contraction): the next launch leaves one wait unsatisfied.
+std::atomic<int> g_stall_next{0};
+
 PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
   if (!encode) {
@@ -298,7 +305,9 @@ int tc_launch(const Geometry& g, const CUtensorMap& tmA, const uint8_t* fdig, in
   const int grid = nitems < sms ? nitems : sms;
   auto kern = contract_tc_kernel<NC>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kBytes);
-  kern<<<grid, kTcThreads, L::kBytes, s>>>(g.Nl, kp / kChunk, tmA, tmB, items, nitems, rexp, cexp, ncols, out, flags);
+  const int stall = g_stall_next.exchange(0);
+  kern<<<grid, kTcThreads, L::kBytes, s>>>(g.Nl, kp / kChunk, tmA, tmB, items, nitems, rexp, cexp, ncols, out, flags,
+                                           stall);
   count_launches(1);
   return DSHT_OK;
 }
@@ -334,3 +343,8 @@ int launch_contract_tc(const Geometry& g, const CUtensorMap& tmA, const uint32_t
 }
 
 }  // namespace dsht
+
+extern "C" int dsht_test_stall_next_contraction(void) {
+  dsht::g_stall_next.store(1);
+  return DSHT_OK;
+}

@@ -252,6 +252,13 @@ int dsht_profile_enable(dsht_plan_t plan, int enable);
 /* Accumulated milliseconds per stage and number of profiled executes; reset=1 clears. */
 int dsht_profile_read(dsht_plan_t plan, double* ms, int64_t* calls, int reset);
 
+/* Test hook, no counterpart in the reference: the next tensor-core contraction launch (any
+ * plan, any thread) withholds one of its internal signals, so a bounded wait inside it runs
+ * out after about one second; the kernel then stops cleanly, the device stays usable, and the
+ * call returns DSHT_ERR_CUDA ("timed out").  Lets a test check that a stalled tensor-core
+ * pipeline is reported instead of hanging. */
+int dsht_test_stall_next_contraction(void);
+
 /* Kernels this library has launched in this process (all devices). */
 int64_t dsht_launch_count(void);
 
