@@ -762,6 +762,28 @@ def main(argv=None):
                        "neighbouring steps' kernels; wall clock over the steps",
                "sync_one_at_a_time": e2e_sync}
         del pipe
+        # The host link alone: the same host->device bytes from the same pinned buffers, timed
+        # with CUDA events on a copy stream with nothing else running.  Each end-to-end step
+        # has to move them, so h2d_bytes / this rate bounds its time from below.
+        cps = torch.cuda.Stream(device=dev)
+        dsts = [torch.empty_like(a, device=dev) for a in hp[:2]] + [torch.empty_like(wmat, device=dev)]
+        srcs = [hp[0], hp[1], wmat]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(cps):
+            for _ in range(2):
+                for d_, s_ in zip(dsts, srcs):
+                    d_.copy_(s_, non_blocking=True)
+            e0.record(cps)
+            for _ in range(3):
+                for d_, s_ in zip(dsts, srcs):
+                    d_.copy_(s_, non_blocking=True)
+            e1.record(cps)
+        cps.synchronize()
+        h2d_ms = e0.elapsed_time(e1) / 3
+        e2e["h2d_link"] = {"gb_per_s": h2d / (h2d_ms * 1e-3) / 1e9, "ms_per_step": h2d_ms,
+                           "what": "pinned host -> device copy of one step's inputs alone (CUDA events, copy "
+                                   "stream, nothing else running): the floor of an end-to-end step"}
+        del dsts
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -70,6 +70,7 @@ SIGNATURES = {
     "dsht_get_table_mlayout": (ct.c_int, [_vp, ct.c_int, _vp, ct.c_int, _vp]),
     "dsht_alm2cl": (ct.c_int, [ct.c_int, _dp, _dp]),
     "dsht_alm2cl_device": (ct.c_int, [ct.c_int, ct.c_int, _vp, ct.c_int64, _vp, _vp]),
+    "dsht_mode_coupling": (ct.c_int, [ct.c_int, _vp, ct.c_int, _vp, _vp]),
     "dsht_make_table": (ct.c_int, [ct.c_int, ct.c_int, ct.c_double, _dp, _dp]),
     "dsht_do_transform": (ct.c_int, [ct.c_int, ct.c_int, ct.c_double, _dp, _dp, ct.c_int, _dp, _dp, _dp, _dp,
                                      _dp]),

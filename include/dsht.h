@@ -16,6 +16,7 @@
  *   dsht_get_row          DirectSHT.get_Ylm / get_dYlm  sht/sht.py:69-93
  *   dsht_alm2cl           DirectSHT.alm2cl              sht/sht.py:95-109
  *   dsht_index            DirectSHT.indx                sht/sht.py:58-67
+ *   dsht_mode_coupling    MaskDeconvolution.get_M       sht/mask_deconvolution.py:171-192
  *   dsht_make_table       make_table   (ctypes)         csht/sht_helper.c:18, csht/sht.py:39-42
  *   dsht_do_transform     do_transform (ctypes)         csht/sht_helper.c:176, csht/sht.py:111-115
  *
@@ -54,11 +55,13 @@ enum {
   DSHT_MODE_BASIC = 1   /* DirectSHT.basic_sht: every point must be equatorial     */
 };
 
-/* Plan flags.  DSHT_PLAN_F32_TABLES: keep only FP32 copies of the tables (the FP64 values
- * rounded once; half the memory: 68.7 GB instead of 137 GB at Nl=2048, Nx=4096).  Such a
- * plan runs at DSHT_PREC_MIXED only; transforms below DSHT_MIXED_MIN_POINTS points use FP64
- * bin sums with the FP32 tables; dsht_get_row / dsht_get_table return the FP32 values
- * widened to double.  Needs Nx % 4 == 0 and Nl <= 2048. */
+/* Plan flags.  DSHT_PLAN_F32_TABLES: keep only the compact 4-byte fixed-point tables (each
+ * row of Yv and dx*Yd as 31-bit integers of one power-of-two row scale, stored as four int8
+ * digit planes; built from the FP64 recurrences a few columns at a time; half the memory of
+ * the FP64 pair: 68.7 GB instead of 137 GB at Nl=2048, Nx=4096).  Such a plan runs at
+ * DSHT_PREC_MIXED only (transforms below DSHT_MIXED_MIN_POINTS points use FP64 bin sums with
+ * the compact tables); dsht_get_row / dsht_get_table return the stored values, within
+ * 2^-31 of their row's largest entry.  Needs Nx <= 8192 and Nl <= 2048. */
 enum {
   DSHT_PLAN_DEFAULT = 0,
   DSHT_PLAN_F32_TABLES = 1
@@ -69,15 +72,18 @@ enum {
  *                     reference's numpy path to about 1e-15 (tested at <= 1e-12 x max|alm|).
  *   DSHT_PREC_MIXED : tcgen05 tensor-core per-bin sums (operands quantised to 22-bit fixed
  *                     point, split into int8 slices, slice products accumulated exactly in
- *                     S32 and combined in FP64; unbiased, about 5.6e-8 rms per product) and
- *                     an FP32 copy of the tables streamed by the contraction (half the HBM
- *                     bytes, FP64 sums).  Within 1e-7 x max|alm| of FP64 for point sets
- *                     spread over many nodes (4.5e-8 measured on 1e7 points, Nl=1024); the
- *                     FP32 table rounding can reach a few 1e-7 when most of the weight sits
- *                     in one x bin.  Also the fixed-point scale of a bin piece is its
- *                     largest |weight|: weights spanning many decades lose accuracy.
- *   DSHT_PREC_MIXED_F64_TABLES : the same tensor-core sums with the FP64 tables
- *                     (within 1e-7 x max|alm| also for concentrated point sets).
+ *                     S32 and combined in FP64; unbiased, about 5.6e-8 rms per product) and a
+ *                     tcgen05 tensor-core contraction of 4-byte fixed-point copies of the
+ *                     tables (31-bit digits per row and per fold column, five exact S32
+ *                     digit-pair classes; contraction error about 1e-9 x max|alm|), built on
+ *                     first use; every table tile is read once for up to eight maps or point
+ *                     sets of a multi-transform call.  Within 1e-7 x max|alm| of FP64,
+ *                     concentrated point sets included.  The fixed-point scale of a bin
+ *                     piece is its largest |weight|: weights spanning many decades lose
+ *                     accuracy (lognormal sigma <= 1.5 stays within 1e-7).  Plans with
+ *                     Nx > 8192 use an FP32 copy of the tables instead.
+ *   DSHT_PREC_MIXED_F64_TABLES : the same tensor-core sums with the FP64 tables streamed
+ *                     by the CUDA-core contraction.
  * Mixed levels need Nl <= 2048; transforms of fewer than DSHT_MIXED_MIN_POINTS points run
  * the FP64 stages (they cost little, and the quantisation error of a handful of points
  * does not average down).  The rotation stays FP64 in all levels. */
@@ -93,9 +99,10 @@ int dsht_get_precision(dsht_plan_t plan, int* precision);
 
 /* Launch-shape tuning of a plan (no counterpart in the reference; results do not depend on
  * it beyond rounding).  DSHT_TUNE_PIECE_MAX: points per bin piece of the per-bin sums, a
- * multiple of 32 in [256, 2048], 0 = chosen from N.  DSHT_TUNE_MAPS_PER_PASS: maps that
- * share one read of the tables in the multi-map contraction, 1..4, 0 = 2.  Workspace sizes
- * depend on both: query them after tuning. */
+ * multiple of 32 in [256, 2048], 0 = chosen from N.  DSHT_TUNE_MAPS_PER_PASS: maps or point
+ * sets that share one read of the tables in a multi-transform call, 1..8, 0 = the most
+ * (8 for the tensor-core contraction, 2 for the FP32 one).  Workspace sizes depend on both:
+ * query them after tuning. */
 enum { DSHT_TUNE_PIECE_MAX = 1, DSHT_TUNE_MAPS_PER_PASS = 2 };
 int dsht_plan_tune(dsht_plan_t plan, int param, int value);
 int dsht_plan_get_tune(dsht_plan_t plan, int param, int* value);
@@ -155,9 +162,9 @@ int dsht_status(unsigned flags, int mode);
  * users call DirectSHT.__call__ once per point set).  Transform i: N[i] points at the
  * DEVICE pointers theta[i], phi[i], w[i] (float64), alm to the DEVICE pointer alm[i]
  * (2*Nlm doubles); the pointer arrays themselves are HOST arrays read during the call.
- * Each point set is sorted on its own; the contraction serves up to 4 transforms per read
- * of the tables (DSHT_TUNE_MAPS_PER_PASS) and the rotation up to 8.  Results equal those of
- * one dsht_execute per transform.  The workspace (dsht_workspace_size_batch with the
+ * Each point set is sorted on its own; the contraction serves up to 8 transforms per read
+ * of the tables (DSHT_TUNE_MAPS_PER_PASS; 4 with FP32 tables, 1 with FP64 tables) and the
+ * rotation up to 8.  Results equal those of one dsht_execute per transform.  The workspace (dsht_workspace_size_batch with the
  * largest N of the batch) is used in turn by every transform.  dsht_execute_batch
  * synchronises and returns the first error of any transform; dsht_enqueue_batch does not
  * synchronise, allocates nothing, and writes the flags of transform i to the DEVICE word
@@ -226,6 +233,14 @@ int dsht_alm2cl(int Nl, const double* alm, double* cl);
  * spectrum at cl + k * Nl.  Stream-ordered on `stream` (NULL = default), no synchronisation.
  * Replaces DirectSHT.alm2cl (sht/sht.py:95-109) for device-resident alm. */
 int dsht_alm2cl_device(int Nl, int nmaps, const double* alm, int64_t alm_stride, double* cl, void* stream);
+
+/* Mode-coupling matrix of pseudo-Cl for a window W: M[l1 * Nl + l2] =
+ * (2 l2 + 1)/(4 pi) sum_{l3} (2 l3 + 1) W[l3] (l1 l2 l3; 0 0 0)^2 for l1, l2 < Nl, with
+ * W[l3] = 0 for l3 >= nW.  W: DEVICE pointer to nW doubles; M: DEVICE pointer to Nl*Nl
+ * doubles.  Stream-ordered on `stream`, no synchronisation.  Replaces
+ * MaskDeconvolution.get_M (sht/mask_deconvolution.py:171-192) and the Wigner 3j table it
+ * reads (sht/threej000.py:9-41, 76-117): the symbols are formed on the fly. */
+int dsht_mode_coupling(int Nl, const double* W, int nW, double* M, void* stream);
 
 /* Drop-ins for the reference's ctypes library csht/sht_helper.so (HOST arrays).
  * dsht_make_table fills Yv, Yd (Nlm*Nx doubles each) like make_table

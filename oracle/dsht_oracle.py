@@ -462,3 +462,63 @@ def brute_force_alm(theta, phi, w, Nl: int) -> np.ndarray:
         for ell in range(m, Nl):
             alm[healpy_index(ell, m, Nl)] = np.sum(w * np.conj(sph_harm_y(ell, m, theta, phi)))
     return alm
+
+
+# ----------------------------------------------------------------------------
+# Mode coupling of pseudo-Cl (next to the transform: MaskDeconvolution)
+# ----------------------------------------------------------------------------
+def threej000(l1: int, l2: int, l3: int, _cache={}) -> float:
+    """Wigner 3j (l1 l2 l3; 0 0 0) by the reference's recursion (``sht/threej000.py:9-41``):
+    sort j1 >= j2 >= j3; zero for odd J; (-1)^j1/sqrt(2 j1 + 1) at j3 = 0, j1 = j2; else
+    sqrt((J-2j2-1)(J-2j3+2) / ((J-2j2)(J-2j3+1))) times the value at (j1, j2+1, j3-1)."""
+    J = l1 + l2 + l3
+    j1 = max(l1, l2, l3)
+    j3 = min(l1, l2, l3)
+    j2 = J - j1 - j3
+    key = (j1, j2, j3)
+    if key in _cache:
+        return _cache[key]
+    if J % 2:
+        res = 0.0
+    elif j3 == 0:
+        res = (-1.0) ** j1 / np.sqrt(2 * j1 + 1.0) if j1 == j2 else 0.0
+    else:
+        num = (J - 2 * j2 - 1) * (J - 2 * j3 + 2)
+        den = (J - 2 * j2) * (J - 2 * j3 + 1)
+        res = np.sqrt(float(num) / float(den)) * threej000(j1, j2 + 1, j3 - 1)
+    _cache[key] = res
+    return res
+
+
+def mode_coupling(Nl: int, W_l: np.ndarray) -> np.ndarray:
+    """M[l1, l2] = (2 l2 + 1)/(4 pi) sum_l3 (2 l3 + 1) W[l3] (l1 l2 l3; 000)^2 for l1, l2 < Nl,
+    W right-padded with zeros to 2 Nl - 1 (``sht/mask_deconvolution.py:28-32, 171-192``).
+    Pure Python loops: small Nl only."""
+    W = np.pad(np.asarray(W_l, "float64"), (0, max(0, 2 * Nl - 1 - len(W_l))))
+    M = np.zeros((Nl, Nl))
+    for l1 in range(Nl):
+        for l2 in range(Nl):
+            s = 0.0
+            for l3 in range(abs(l1 - l2), l1 + l2 + 1):
+                if (l1 + l2 + l3) % 2 == 0:
+                    s += (2 * l3 + 1) * W[l3] * threej000(l1, l2, l3) ** 2
+            M[l1, l2] = s * (2 * l2 + 1)
+    return M / (4 * np.pi)
+
+
+def mode_coupling_closed_form(Nl: int, W_l: np.ndarray) -> np.ndarray:
+    """The same matrix from the closed form of (l1 l2 l3; 000)^2 with log-gamma (vectorised
+    over l3): an independent check for sizes where the recursion above is too slow."""
+    from scipy.special import gammaln
+    W = np.pad(np.asarray(W_l, "float64"), (0, max(0, 2 * Nl - 1 - len(W_l))))
+    M = np.zeros((Nl, Nl))
+    for l1 in range(Nl):
+        for l2 in range(Nl):
+            l3 = np.arange(abs(l1 - l2), l1 + l2 + 1, 2)
+            J = l1 + l2 + l3
+            g = J // 2
+            lw = (gammaln(J - 2 * l1 + 1) + gammaln(J - 2 * l2 + 1) + gammaln(J - 2 * l3 + 1) - gammaln(J + 2)
+                  + 2 * (gammaln(g + 1) - gammaln(g - l1 + 1) - gammaln(g - l2 + 1) - gammaln(g - l3 + 1)))
+            Wl3 = np.where(l3 < len(W), W[np.minimum(l3, len(W) - 1)], 0.0)
+            M[l1, l2] = np.sum((2 * l3 + 1) * Wl3 * np.exp(lw)) * (2 * l2 + 1)
+    return M / (4 * np.pi)
