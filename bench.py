@@ -447,7 +447,7 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--cpu-sample", type=int, default=1_000_000,
                     help="points of the cpu_baseline step (the reference's C transform on the host cores)")
     ap.add_argument("--ref-sample", type=int, default=1_000_000,
@@ -733,9 +733,12 @@ def main(argv=None):
         # step still copies its host arrays in and its alm out, but the copies of one step
         # overlap the kernels of the neighbouring steps (two slots in flight).
         from directsht_b200.pipeline import Pipeline
-        pipe = Pipeline(d, max_N=N, nmaps=maps, w_dtype=w.dtype, depth=2)
+        # three slots: the host collects a result two steps behind, so a slot's next copy-in
+        # never waits for the host (with two slots the host's result handling sits in the
+        # critical path between one step's kernels and the copy-in of the step after next)
+        pipe = Pipeline(d, max_N=N, nmaps=maps, w_dtype=w.dtype, depth=3)
         wmat = torch.from_numpy(np.ascontiguousarray(w if w.ndim == 2 else w[None, :])).pin_memory()
-        for _ in range(2):
+        for _ in range(3):
             pipe.submit(hp[0], hp[1], wmat)
         pipe.drain()
         if world > 1:
@@ -745,7 +748,7 @@ def main(argv=None):
         tickets = []
         for k in range(args.e2e_steps):
             tickets.append(pipe.submit(hp[0], hp[1], wmat))
-            if len(tickets) > 1:
+            if len(tickets) > 2:
                 pipe.result(tickets.pop(0))
         for tk in tickets:
             pipe.result(tk)
@@ -759,7 +762,7 @@ def main(argv=None):
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 16 * d.Nlm * maps,
                "path": "directsht_b200.pipeline.Pipeline: pinned host inputs -> device (copy stream), "
                        "dsht_enqueue_maps (C ABI), alm -> pinned host; copies of a step overlap the "
-                       "neighbouring steps' kernels; wall clock over the steps",
+                       "neighbouring steps' kernels (three slots); wall clock over the steps",
                "sync_one_at_a_time": e2e_sync}
         del pipe
         # The host link alone: the same host->device bytes from the same pinned buffers, timed

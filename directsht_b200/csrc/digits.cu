@@ -24,6 +24,7 @@
 namespace dsht {
 namespace {
 
+constexpr int kStageRow = 36;  // bytes per staging row of fold_digits_kernel (32 used)
 constexpr double kScaleMargin = 1.01;  // scale > 1.01 x bound: |X| < 2^31 / 1.01 < 2^31 - 2^24
 
 // Smallest e with kScaleMargin * v <= 2^e (v >= 0; 0 for v = 0).
@@ -174,6 +175,8 @@ fold_scale_kernel(int nbins, int Nx, const int* __restrict__ piece_first, const 
 // Fold of one map straight into digits.  A block covers 32 m x 32 nodes: warp = node,
 // lane = m while the per-piece sums are read (consecutive m: coalesced), then the digit
 // bytes go through shared memory so that consecutive threads store consecutive nodes.
+// Staging rows (one per (parity, digit, column, K half, m), 32 node bytes each) are 36
+// bytes apart with m fastest, so the 32 lanes of a warp store into 32 different banks.
 // Sums as fold_kernel forms them (set s: A = V0(bin j) + V2(bin j-1), B = dx (V1(bin j) +
 // V3(bin j-1)), V = vr - i vi; even rows A+ + A-, odd rows A+ - A-), stored as B/dx.
 template <typename PT>
@@ -181,7 +184,8 @@ __global__ void __launch_bounds__(1024)
 fold_digits_kernel(int Nl, int Nx, int nbins, int Kp, const int* __restrict__ piece_first,
                    const PT* __restrict__ partial, const int16_t* __restrict__ cexp, int map, int ncols,
                    uint8_t* __restrict__ fdig) {
-  // stage[m][par][d][c][kh][j]: 32 x 2 x 4 x 4 x 2 x 32 bytes (dynamic: 64 KB)
+  // stage[row][36], row = (((par * 4 + d) * 4 + c) * 2 + kh) * 32 + m, byte j of the row
+  // = node j0 + j (dynamic: 72 KB)
   extern __shared__ __align__(16) uint8_t stage[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int m0 = blockIdx.y * 32, j0 = blockIdx.x * 32;
@@ -233,22 +237,23 @@ fold_digits_kernel(int Nl, int Nx, int nbins, int Kp, const int* __restrict__ pi
           const int c = 2 * h + ri;
 #pragma unroll
           for (int d = 0; d < 4; ++d)
-            stage[((((lane * 2 + par) * 4 + d) * 4 + c) * 2 + kh) * 32 + warp] = (uint8_t)(w >> (8 * (3 - d)));
+            stage[(((((par * 4 + d) * 4 + c) * 2 + kh) * 32) + lane) * kStageRow + warp] =
+                (uint8_t)(w >> (8 * (3 - d)));
         }
   __syncthreads();
-  // 64 KB of digits = 16384 words; word w covers 4 nodes of one (m, par, d, c, kh) row.
+  // 2048 rows x 8 words; word w covers 4 nodes of one (par, d, c, kh, m) row.
   const int nj = min(32, Nx - j0);
   for (int w = threadIdx.x; w < 32 * 2 * 4 * 4 * 2 * 8; w += blockDim.x) {
     const int q = w & 7;           // 4-node group
-    const int row = w >> 3;        // (((ml * 2 + par) * 4 + d) * 4 + c) * 2 + kh
-    const int kh = row & 1;
-    const int c = (row >> 1) & 3;
-    const int d = (row >> 3) & 3;
-    const int par = (row >> 5) & 1;
-    const int ml = row >> 6;
+    const int row = w >> 3;        // (((par * 4 + d) * 4 + c) * 2 + kh) * 32 + ml
+    const int ml = row & 31;
+    const int kh = (row >> 5) & 1;
+    const int c = (row >> 6) & 3;
+    const int d = (row >> 8) & 3;
+    const int par = (row >> 10) & 1;
     const int mm = m0 + ml;
     if (mm >= Nl || 4 * q >= nj) continue;
-    const uint32_t word = *reinterpret_cast<const uint32_t*>(stage + row * 32 + 4 * q);
+    const uint32_t word = *reinterpret_cast<const uint32_t*>(stage + row * kStageRow + 4 * q);
     uint8_t* dst = fdig + ((((size_t)mm * 2 + par) * 4 + d) * ncols + 4 * map + c) * (size_t)Kp + (size_t)kh * Nx + j0 +
                    4 * q;
     if (4 * q + 4 <= nj && ((reinterpret_cast<uintptr_t>(dst) & 3) == 0)) {
@@ -304,7 +309,7 @@ void launch_fold_digits(const Geometry& g, const Workspace& ws, const int16_t* c
                         uint8_t* fdig, cudaStream_t s) {
   const int Kp = digit_kp(g.Nx);
   dim3 grid((g.Nx + 31) / 32, (g.Nl + 31) / 32);
-  constexpr int kStageBytes = 32 * 2 * 4 * 4 * 2 * 32;
+  constexpr int kStageBytes = 32 * 2 * 4 * 4 * 2 * kStageRow;
   cudaFuncSetAttribute(fold_digits_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStageBytes);
   cudaFuncSetAttribute(fold_digits_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStageBytes);
   if (ws.partial_f32)

@@ -80,7 +80,8 @@ enum {
  *                     sets of a multi-transform call.  Within 1e-7 x max|alm| of FP64,
  *                     concentrated point sets included.  The fixed-point scale of a bin
  *                     piece is its largest |weight|: weights spanning many decades lose
- *                     accuracy (lognormal sigma <= 1.5 stays within 1e-7).  Plans with
+ *                     accuracy (lognormal sigma <= 1.5 stays within 1e-7), and so do weights
+ *                     of both signs whose sums cancel (zero-mean normal weights: ~3e-7).  Plans with
  *                     Nx > 8192 use an FP32 copy of the tables instead.
  *   DSHT_PREC_MIXED_F64_TABLES : the same tensor-core sums with the FP64 tables streamed
  *                     by the CUDA-core contraction.
