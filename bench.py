@@ -359,7 +359,7 @@ def run_batch(args, spec):
         line = {"metric": "points*ell/s", "value": world * pe / (ms_step / 1e3), "unit": "points*ell/s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "i8 tensor sums + f32 tables + f64", "data": "synthetic",
+                "dtype": "i8 tensor sums + i8 digit-table contraction + f64", "data": "synthetic",
                 "config": {"workload": spec["name"], "transforms": len(ts), "points": int(sum(b.Ns)),
                            "points_ell": pe, "precision": "mixed (compact digit tables only for Nl >= 1024)",
                            "l2": "inputs (GBs) and tables (79 GB) exceed L2", "parallelism": f"replicas x{world}",
@@ -423,7 +423,7 @@ def run_serve(args, spec):
         line = {"metric": "points*ell/s", "value": value, "unit": "points*ell/s", "n_gpus": world,
                 "steps": spec["nreq"], "warmup": len(warm), "ms_per_step": st["mean_ms"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "i8 tensor sums + f32 tables + f64", "data": "synthetic",
+                "dtype": "i8 tensor sums + i8 digit-table contraction + f64", "data": "synthetic",
                 "config": {"workload": spec["name"], "requests": spec["nreq"], "rate_hz": spec["rate"],
                            "points_ell": st["points_ell"], "budget_GB": budget / 1e9, "slots": 8,
                            "plans_resident_GB": cache.resident_bytes() / 1e9, "parallelism": f"replicas x{world}",
@@ -803,7 +803,7 @@ def main(argv=None):
             "metric": "points*ell/s", "value": value, "unit": "points*ell/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": "i8 tensor sums + f64" if args.precision == "mixed" else "f64", "data": "synthetic",
+            "dtype": "i8 tensor sums + i8 digit-table contraction + f64" if args.precision == "mixed" else "f64", "data": "synthetic",
             "config": {"workload": spec["name"], "Nl": Nl, "Nx": Nx, "N": N, "maps": maps,
                        "point_sets_per_step": batch, "precision": args.precision,
                        "l2": f"inputs ({(th.nbytes + ph.nbytes + w.nbytes) / 1e6:.0f} MB) and tables "

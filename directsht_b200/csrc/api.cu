@@ -62,8 +62,8 @@ int default_piece_max(const Geometry& g, int64_t N) {
   return (int)p;
 }
 
-size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* base, Workspace* ws, int fold_slots,
-                        bool multi, int tc_maps) {
+size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* base, Workspace* ws, bool multi,
+                        int tc_maps) {
   size_t off = 0;
   auto take = [&](size_t bytes) -> uint8_t* {
     uint8_t* p = base ? base + off : nullptr;
@@ -90,7 +90,6 @@ size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* ba
   w.piece_len = reinterpret_cast<int*>(take(sizeof(int) * pmax));
   w.piecemax = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * pmax));
   w.wsum = reinterpret_cast<double*>(take(sizeof(double) * pmax));
-  w.nodew = reinterpret_cast<double*>(take(sizeof(double) * 2 * (size_t)g.Nx));
   w.npieces = reinterpret_cast<int*>(take(sizeof(int)));
   w.flags = reinterpret_cast<unsigned*>(take(sizeof(unsigned)));
   if (maps) {
@@ -98,14 +97,10 @@ size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* ba
     w.all_flags = reinterpret_cast<unsigned*>(take(sizeof(unsigned)));
   }
   w.partial = reinterpret_cast<double*>(take(sizeof(double) * 8 * (size_t)g.Nl * pmax));
-  // One fold per map of a contraction pass (multi-map transforms).
-  w.fold_slots = std::max(1, std::min(fold_slots, kMaxPass));
-  w.heavy_flag = reinterpret_cast<uint8_t*>(take(2 * (size_t)g.Nx * w.fold_slots));
-  w.heavy_list = reinterpret_cast<int*>(take(sizeof(int) * (size_t)kHeavyMax * w.fold_slots));
-  w.heavy_n = reinterpret_cast<int*>(take(sizeof(int) * w.fold_slots));
-  // The tensor-core route's fold digits ([Nl][2][4][4 tc_maps][Kp] int8) use the same region.
+  // The FP64 fold of one map, or the tensor-core route's fold digits ([Nl][2][4][4 tc_maps]
+  // [Kp] int8), whichever is larger: a call's route uses one of them.
   w.tc_maps = std::max(1, std::min(tc_maps, kTcMaxMaps));
-  const size_t fold_bytes = sizeof(double) * 16 * (size_t)g.Nl * g.Nx * w.fold_slots;
+  const size_t fold_bytes = sizeof(double) * 16 * (size_t)g.Nl * g.Nx;
   const size_t fdig_bytes = (size_t)g.Nl * 8 * 4 * w.tc_maps * (size_t)digit_kp(g.Nx);
   w.fold = reinterpret_cast<double*>(take(std::max(fold_bytes, fdig_bytes)));
   w.cexp = reinterpret_cast<int16_t*>(take(sizeof(int16_t) * 2 * w.tc_maps));
@@ -125,23 +120,13 @@ int plan_piece_max(const dsht_plan_s* p, int64_t N) {
   return p->tune_piece_max > 0 ? p->tune_piece_max : default_piece_max(p->g, N);
 }
 
-// Two folds per contraction pass unless tuned: the 32-row kernel keeps two maps' FP64
-// sums in registers; passes of three or four maps use 16-row items, whose extra fold
-// reloads cost more than the table reads they save (measured at Nl=1024, Nx=2048).
-int plan_maps_per_pass(const dsht_plan_s* p) {
-  const int mx = contract_stream_max_maps(true);
-  return p->tune_maps_per_pass > 0 ? std::min(p->tune_maps_per_pass, mx) : std::min(2, mx);
-}
-
 Route plan_route(const dsht_plan_s* p, int64_t N) {
   Route r{};
   r.tc = p->precision != DSHT_PREC_FP64 && N >= DSHT_MIXED_MIN_POINTS;
-  // The compact tables (digits, else FP32) serve tensor-core transforms at the MIXED level
-  // and every transform of a plan that holds no FP64 tables.
-  const bool compact = (r.tc && p->precision == DSHT_PREC_MIXED) || !p->Yv;
-  r.digits = p->tmdig && compact;
-  r.f32_tables = !r.digits && p->tm32 && compact;
-  r.streamed = r.digits || r.f32_tables || p->tm64;
+  // The digit tables serve tensor-core transforms at the MIXED level and every transform
+  // of a plan that holds no FP64 tables; everything else contracts the FP64 tables.
+  r.digits = p->tmdig && ((r.tc && p->precision == DSHT_PREC_MIXED) || !p->Yv);
+  r.streamed = r.digits || p->tm64;
   return r;
 }
 
@@ -236,13 +221,12 @@ int run_after_sort(dsht_plan_s* p, int64_t N, int mode, double* alm, const Works
   Workspace w2 = ws;
   // Small transforms run the FP64 stages even on a mixed-precision plan.
   const Route rt = plan_route(p, N);
-  const bool f32_tables = rt.f32_tables;
   if (rt.tc) {
     int rc = launch_bin_sums_tc(g, ws, s);  // piece maxima and |w| sums first
     if (rc) return rc;
     w2.partial_f32 = 1;
   } else {
-    if (f32_tables || rt.digits) launch_piece_maxima(ws, s);  // the |w| sums (node weights)
+    if (rt.digits) launch_piece_maxima(ws, s);  // the |w| sums (fold digit scales)
     launch_bin_sums_fp64(g, ws, s);
     w2.partial_f32 = 0;
   }
@@ -259,19 +243,13 @@ int run_after_sort(dsht_plan_s* p, int64_t N, int mode, double* alm, const Works
                                     ws.flags, s))
       return rc;
   } else {
-    w2.fold_f32 = f32_tables ? 1 : 0;
     mark(DSHT_STAGE_FOLD);
-    if (f32_tables) launch_heavy_select(g, w2, 0, s);
-    launch_fold(g, w2, s, f32_tables ? w2.heavy_flag : nullptr);
+    launch_fold(g, w2, s);
     mark(DSHT_STAGE_CONTRACT);
-    if (f32_tables) {
-      launch_heavy_otf(g, w2, 0, ws.alm_equ, ws.alm_pol, s);
-      launch_contract_stream(g, true, p->tmYv32, p->tmYd32, ws, s, ws.heavy_n);
-    } else if (p->tm64) {
-      launch_contract_stream(g, false, p->tmYv, p->tmYd, ws, s);
-    } else {
+    if (p->tm64)
+      launch_contract_stream(g, p->tmYv, p->tmYd, ws.fold, ws.tile_live2, ws.alm_equ, ws.alm_pol, ws.flags, s);
+    else
       launch_contract_fp64(g, p->Yv, p->Yd, ws, s);
-    }
   }
   mark(DSHT_STAGE_ROTATE);
   if (mode == DSHT_MODE_CALL) {
@@ -366,16 +344,15 @@ static int run_class_digits(dsht_plan_s* p, const Item* items, const std::vector
 // Several transforms in one call: multi-map transforms (one point set, the later maps marked
 // same_points) and batches of independent transforms on one plan.  Each point set is
 // classified and sorted once; a same_points item only gathers its weights into the sorted
-// payload.  Bin sums and the fold run per item; the contraction runs in passes of up to
-// contract_stream_max_maps items whose folds share one read of the tables; equatorial alm
-// go straight to item.alm, polar alm to a rotation slot, and every kMaxRot slots one
-// batched rotation adds them back.  Items with N < DSHT_MIXED_MIN_POINTS on a mixed plan
-// run the FP64 stages, in their own passes.
+// payload.  Bin sums and the fold run per item.  On the digit tables the contraction runs
+// in passes of up to ws.tc_maps items that share one read of the tables
+// (run_class_digits); on the FP64 tables once per item.  Equatorial alm go straight to
+// item.alm, polar alm to a rotation slot, and one batched rotation per kMaxRot slots adds
+// them back.  Items with N < DSHT_MIXED_MIN_POINTS on a mixed plan run the FP64 bin sums,
+// in their own class.
 int run_items(dsht_plan_s* p, const Item* items, int n, int mode, const Workspace& ws, cudaStream_t s) {
   const Geometry& g = p->g;
   const int64_t nlm2 = 2 * g.Nlm;
-  const int64_t fold_stride = 4 * (int64_t)g.Nl * g.Nx;  // F4 elements per fold
-  const int ntile2 = (g.Nx + 255) / 256;
   p->ev_n = 0;
   DSHT_CUDA_OK(cudaMemsetAsync(ws.all_flags, 0, sizeof(unsigned), s));
   // Items in two classes by the precision their size selects; same_points chains stay whole
@@ -392,12 +369,9 @@ int run_items(dsht_plan_s* p, const Item* items, int n, int mode, const Workspac
       if (rc) return rc;
       continue;
     }
+    // FP64 tables: one contraction per item, rotations batched up to kMaxRot items.
     const bool mixed = rt.tc;
-    const bool f32_tables = rt.f32_tables;
-    const bool streamed = rt.streamed;
-    const int G = f32_tables ? ws.fold_slots : 1;
-    const size_t f4 = f32_tables ? sizeof(float4) : sizeof(double4);
-    std::vector<int> pass, pend;          // item indices; slot of pass[k] = pend.size() + k
+    std::vector<int> pend;                // items awaiting rotation; item pend[k] in slot k
     auto flush_rotation = [&]() -> int {  // rotate and publish every pending item
       if (pend.empty()) return DSHT_OK;
       RotMaps rm{};
@@ -415,30 +389,10 @@ int run_items(dsht_plan_s* p, const Item* items, int n, int mode, const Workspac
       pend.clear();
       return DSHT_OK;
     };
-    auto run_pass = [&]() -> int {
-      if (pass.empty()) return DSHT_OK;
-      const int base = (int)pend.size();
-      if (streamed) {
-        MapOut out{};
-        for (size_t k = 0; k < pass.size(); ++k) {
-          out.equ[k] = items[pass[k]].alm;
-          out.pol[k] = ws.alm_pol + nlm2 * (base + k);
-          out.heavy_n[k] = f32_tables ? ws.heavy_n + k : nullptr;  // fold slot k
-        }
-        prof_mark(p, DSHT_STAGE_CONTRACT, s);
-        launch_contract_pass(g, f32_tables, f32_tables ? p->tmYv32 : p->tmYv, f32_tables ? p->tmYd32 : p->tmYd,
-                             p->tmYv32h, p->tmYd32h,
-                             ws.fold, fold_stride, (int)pass.size(), ws.tile_live2, out, ws.slot_flags + base, s);
-      }
-      for (int it : pass) pend.push_back(it);
-      pass.clear();
-      if (pend.size() + G > (size_t)kMaxRot) return flush_rotation();
-      return DSHT_OK;
-    };
     for (size_t li = 0; li < list.size(); ++li) {
       const int i = list[li];
       const Item& item = items[i];
-      const int slot = (int)(pend.size() + pass.size());
+      const int slot = (int)pend.size();
       Workspace w2 = ws;
       w2.flags = ws.slot_flags + slot;
       if (item.same_points && sorted_item >= 0) {
@@ -446,12 +400,9 @@ int run_items(dsht_plan_s* p, const Item* items, int n, int mode, const Workspac
         launch_gather(g, item.w, item.w_f32, item.N, ws, s);
       } else {
         prof_mark(p, DSHT_STAGE_POINTS, s);
-        // The sort keeps the input index and t of every slot when later items share it.
+        // The sort keeps the input index of every slot when later items share it.
         Workspace wp = ws;
-        const bool shared = li + 1 < list.size() && items[list[li + 1]].same_points;
-        if (!shared) {
-          wp.sidx = nullptr;
-        }
+        if (!(li + 1 < list.size() && items[list[li + 1]].same_points)) wp.sidx = nullptr;
         launch_points(g, item.theta, item.phi, item.w, item.w_f32, item.N, mode, wp, s);
         sorted_item = i;
       }
@@ -466,36 +417,18 @@ int run_items(dsht_plan_s* p, const Item* items, int n, int mode, const Workspac
         w2.partial_f32 = 0;
       }
       prof_mark(p, DSHT_STAGE_FOLD, s);
-      if (streamed) {
-        if (pass.empty()) DSHT_CUDA_OK(cudaMemsetAsync(ws.tile_live2, 0, 2 * (size_t)ntile2, s));
-        w2.fold_f32 = f32_tables ? 1 : 0;
-        w2.fold = reinterpret_cast<double*>(reinterpret_cast<uint8_t*>(ws.fold) + f4 * fold_stride * pass.size());
-        w2.live_or = 1;
-        const int fslot = (int)pass.size();
-        if (f32_tables) {
-          if (!mixed) launch_piece_maxima(w2, s);  // the |w| sums of the heavy-node test
-          launch_heavy_select(g, w2, fslot, s);
-        }
-        launch_fold(g, w2, s, f32_tables ? w2.heavy_flag + (size_t)fslot * 2 * g.Nx : nullptr);
-        // heavy nodes in FP64 now, while this map's bin sums are in ws.partial; the pass adds
-        if (f32_tables) launch_heavy_otf(g, w2, fslot, item.alm, ws.alm_pol + nlm2 * slot, s);
-        pass.push_back(i);
-        if ((int)pass.size() == G || li + 1 == list.size()) {
-          int rc = run_pass();
-          if (rc) return rc;
-        }
-      } else {  // tables without the streaming layout: the single-transform stages
-        w2.fold_f32 = 0;
-        w2.alm_pol = ws.alm_pol + nlm2 * slot;
-        w2.alm_equ = item.alm;
-        launch_fold(g, w2, s);
-        prof_mark(p, DSHT_STAGE_CONTRACT, s);
+      w2.alm_pol = ws.alm_pol + nlm2 * slot;
+      w2.alm_equ = item.alm;
+      launch_fold(g, w2, s);
+      prof_mark(p, DSHT_STAGE_CONTRACT, s);
+      if (rt.streamed)
+        launch_contract_stream(g, p->tmYv, p->tmYd, ws.fold, ws.tile_live2, w2.alm_equ, w2.alm_pol, w2.flags, s);
+      else
         launch_contract_fp64(g, p->Yv, p->Yd, w2, s);
-        pend.push_back(i);
-        if (pend.size() + 1 > (size_t)kMaxRot) {
-          int rc = flush_rotation();
-          if (rc) return rc;
-        }
+      pend.push_back(i);
+      if (pend.size() >= (size_t)kMaxRot) {
+        int rc = flush_rotation();
+        if (rc) return rc;
       }
     }
     int rc = flush_rotation();
@@ -581,8 +514,6 @@ int dsht_plan_create(int Nl, int Nx, double xmax, int flags, dsht_plan_t* plan) 
   auto fail = [&](cudaError_t e, const char* what) {
     cudaFree(p->Yv);
     cudaFree(p->Yd);
-    cudaFree(p->Yv32);
-    cudaFree(p->Yd32);
     cudaFreeHost(p->h_flags);
     delete p;
     cudaGetLastError();
@@ -609,9 +540,8 @@ int dsht_plan_create(int Nl, int Nx, double xmax, int flags, dsht_plan_t* plan) 
   e = cudaDeviceSynchronize();
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) return fail(e, "table build");
-  if (contract_stream_ok(p->g, sizeof(double)) &&
-             make_table_tmap(&p->tmYv, p->Yv, sizeof(double), Nx, p->g.Nlm) == DSHT_OK &&
-             make_table_tmap(&p->tmYd, p->Yd, sizeof(double), Nx, p->g.Nlm) == DSHT_OK) {
+  if (contract_stream_ok(p->g) && make_table_tmap(&p->tmYv, p->Yv, Nx, p->g.Nlm) == DSHT_OK &&
+      make_table_tmap(&p->tmYd, p->Yd, Nx, p->g.Nlm) == DSHT_OK) {
     p->tm64 = true;
   }
   *plan = p;
@@ -627,8 +557,6 @@ int dsht_plan_destroy(dsht_plan_t p) {
   }
   cudaFree(p->Yv);
   cudaFree(p->Yd);
-  cudaFree(p->Yv32);
-  cudaFree(p->Yd32);
   cudaFree(p->dig);
   cudaFree(p->rexp);
   cudaFree(p->tc_items);
@@ -650,36 +578,10 @@ int dsht_set_precision(dsht_plan_t p, int precision) {
     return set_error(DSHT_ERR_INVALID, "this plan holds compact tables only (DSHT_PLAN_F32_TABLES): precision MIXED");
   std::lock_guard<std::mutex> lock(p->mu);
   // MIXED streams the digit tables through the tensor-core contraction (built on first use);
-  // where they do not fit, an FP32 copy streamed by the CUDA-core contraction, else FP64.
-  if (precision == DSHT_PREC_MIXED && !p->tmdig && !p->Yv32 && p->g.Nx <= kTcMaxNx) {
-    if (build_digits(p) == DSHT_OK) {
-      p->precision = precision;
-      return DSHT_OK;
-    }
+  // where they cannot be built (Nx > kTcMaxNx, or no room beside the FP64 tables) its
+  // transforms contract the FP64 tables instead, as DSHT_PREC_MIXED_F64_TABLES does.
+  if (precision == DSHT_PREC_MIXED && !p->tmdig && p->g.Nx <= kTcMaxNx && build_digits(p) != DSHT_OK)
     cudaGetLastError();
-  }
-  if (precision == DSHT_PREC_MIXED && !p->tmdig && !p->Yv32) {
-    const size_t tb = sizeof(float) * (size_t)p->g.Nlm * p->g.Nx;
-    cudaError_t e = cudaMalloc(&p->Yv32, tb);
-    if (e == cudaSuccess) e = cudaMalloc(&p->Yd32, tb);
-    if (e != cudaSuccess) {  // no room for the FP32 copies: stream the FP64 tables instead
-      cudaFree(p->Yv32);
-      cudaFree(p->Yd32);
-      p->Yv32 = nullptr;
-      p->Yd32 = nullptr;
-      cudaGetLastError();
-      p->precision = precision;
-      return DSHT_OK;
-    }
-    launch_tables_to_f32(p->g, p->Yv, p->Yd, p->Yv32, p->Yd32, 0);
-    DSHT_CUDA_OK(cudaDeviceSynchronize());
-    if (contract_stream_ok(p->g, sizeof(float)) &&
-        make_table_tmap(&p->tmYv32, p->Yv32, sizeof(float), p->g.Nx, p->g.Nlm) == DSHT_OK &&
-        make_table_tmap(&p->tmYd32, p->Yd32, sizeof(float), p->g.Nx, p->g.Nlm) == DSHT_OK &&
-        make_table_tmap(&p->tmYv32h, p->Yv32, sizeof(float), p->g.Nx, p->g.Nlm, 16) == DSHT_OK &&
-        make_table_tmap(&p->tmYd32h, p->Yd32, sizeof(float), p->g.Nx, p->g.Nlm, 16) == DSHT_OK)
-      p->tm32 = true;
-  }
   p->precision = precision;
   return DSHT_OK;
 }
@@ -761,13 +663,12 @@ int dsht_workspace_size(dsht_plan_t p, int64_t N, size_t* bytes) {
 }
 
 // Workspace of a call: single transforms use the lean layout; multi-transform calls add
-// the gather records, fold slots, rotation slots and flag slots.
+// the gather records, fold digit columns of a contraction pass, rotation and flag slots.
 static size_t call_layout(dsht_plan_s* p, int64_t N, int ntrans, bool multi, uint8_t* base, Workspace* ws) {
-  const int slots = multi ? std::min(std::max(ntrans, 1), plan_maps_per_pass(p)) : 1;
   // maps per tensor-core contraction pass (digit tables): up to kTcMaxMaps unless tuned
   const int tc = multi ? std::min(std::max(ntrans, 1), p->tune_maps_per_pass > 0 ? p->tune_maps_per_pass
                                                                                   : kTcMaxMaps) : 1;
-  return workspace_layout(p->g, N, plan_piece_max(p, N), base, ws, slots, multi, tc);
+  return workspace_layout(p->g, N, plan_piece_max(p, N), base, ws, multi, tc);
 }
 
 // Resolves the workspace (caller's or the plan's, grown on demand) for a call.

@@ -1,21 +1,18 @@
-// Streaming contraction of the stored tables with the folded node sums, fed by TMA bulk
-// copies (cp.async.bulk) through a two-stage shared-memory ring.
+// Streaming contraction of the FP64 tables with the folded node sums (the FP64 and
+// DSHT_PREC_MIXED_F64_TABLES levels), fed by TMA through a two-stage shared-memory ring.
 //
 //   alm_equ[lm] = sum_j Yv[lm,j] A_q[m,j] + Yd[lm,j] B_q[m,j],  q = equ even/odd by (l-m)%2
 //   alm_pol[lm] = same with the polar q                     (sht/sht.py:266-279)
 //
-// Persistent CTAs walk work items (m, R consecutive rows l).  Warp 0 (one thread) is the
+// Persistent CTAs walk work items (m, 16 consecutive rows l).  Warp 0 (one thread) is the
 // producer: for every live tile of 256 nodes it issues one 2D tensor-map TMA load per table
-// (an R-row x 256-node box of Yv and of Yd) and one bulk copy per fold row (4 q), all
-// completing on the stage's mbarrier.  Warps 1-8 consume: each owns R/8 rows of equal
+// (a 16-row x 256-node box of Yv and of Yd) and one bulk copy per fold row (4 q), all
+// completing on the stage's mbarrier.  Warps 1-8 consume: each owns two rows of equal
 // parity and the 256 nodes of the tile (8 per lane); the FP64 fold values in shared memory
-// feed all its rows.  FP64 tables: double tables and fold, R = 16, FP64 FMAs.  FP32
-// tables: float tables and fold, R = 32, FP32 FMAs within a tile, FP64 sums across tiles.
-// HBM bound: 2 sizeof(T) bytes of table per (l, m, node).
+// feed both rows.  HBM bound: 16 bytes of table per (l, m, node).
 #include <cudaTypedefs.h>
 
 #include <algorithm>
-#include <type_traits>
 
 #include "dsht_internal.cuh"
 #include "tc_ptx.cuh"
@@ -74,41 +71,22 @@ __device__ __forceinline__ void item_of(int64_t item, int Nl, int* m_out, int* g
   *g_out = (int)(item - G(lo));
 }
 
-// FP64 tables: double tables and fold, 16 rows per item, FP64 FMAs.  FP32 tables (the
-// DSHT_PREC_MIXED level): float tables and fold, 32 rows per item, FP32 FMAs within a
-// tile and FP64 sums across tiles -- half the HBM traffic.
-template <bool kMixed, int kG = 1, int kRowsSet = 0>
-struct StageLayout {
-  using T = typename std::conditional<kMixed, float, double>::type;
-  using F4 = typename std::conditional<kMixed, float4, double4>::type;
-  static constexpr int kRows = kRowsSet ? kRowsSet : kMixed ? 32 : 16;
-  static constexpr int kRowsPerWarp = kRows / 8;               // same parity, stride 2
-  static constexpr int kTab = kRows * kTJ * sizeof(T);         // one of Yv, Yd
-  static constexpr int kFold = 4 * kTJ * sizeof(F4);           // 4 q x kTJ, one map
-  static constexpr int kStage = 2 * kTab + kG * kFold;
-  static constexpr int kBytes = kStagesC * kStage + 128 + 128;
-};
+constexpr int kRows = 16;                 // rows per work item
+constexpr int kRowsPerWarp = kRows / 8;   // same parity, stride 2
+constexpr int kTab = kRows * kTJ * sizeof(double);   // one of Yv, Yd
+constexpr int kFold = 4 * kTJ * sizeof(double4);     // 4 q x kTJ
+constexpr int kStage = 2 * kTab + kFold;
+constexpr int kStreamBytes = kStagesC * kStage + 128 + 128;
 
-// kG maps per pass (multi-map transforms): map g's fold at fold_v + g * fold_stride (F4
-// elements) and its alm at out.equ[g], out.pol[g] (2 Nlm doubles each).  The
-// table tile in shared memory serves all kG maps, so a pass reads the tables once.  Passes
-// of three or four maps take 16-row items (two rows per warp), which keeps the FP64
-// accumulators of all maps in registers.
-template <bool kMixed, int kG, int kRowsSet = 0>
 __global__ void __launch_bounds__(kThreads, 1)
 contract_stream_kernel(int Nl, int Nx, int64_t nitems, const __grid_constant__ CUtensorMap tmv,
-                       const __grid_constant__ CUtensorMap tmd, const void* __restrict__ fold_v,
-                       int64_t fold_stride, const uint8_t* __restrict__ live, int ntile,
-                       const MapOut out, unsigned* __restrict__ err) {
-  using L = StageLayout<kMixed, kG, kRowsSet>;
-  using T = typename L::T;
-  using F4 = typename L::F4;
-  constexpr int kRows = L::kRows;
-  constexpr int RW = L::kRowsPerWarp;
-  const F4* fold = reinterpret_cast<const F4*>(fold_v);
+                       const __grid_constant__ CUtensorMap tmd, const double4* __restrict__ fold,
+                       const uint8_t* __restrict__ live, int ntile, double* __restrict__ alm_equ,
+                       double* __restrict__ alm_pol, unsigned* __restrict__ err) {
+  constexpr int RW = kRowsPerWarp;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStagesC * L::kStage);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStagesC * kStage);
   uint64_t* empty = full + kStagesC;
   volatile int* abort_flag = reinterpret_cast<volatile int*>(empty + kStagesC);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -142,17 +120,15 @@ contract_stream_kernel(int Nl, int Nx, int64_t nitems, const __grid_constant__ C
           }
           const int j0 = t * kTJ;
           const int nj = min(kTJ, Nx - j0);
-          uint8_t* st = smem + s * L::kStage;
-          const uint32_t fold_bytes = nj * sizeof(F4);
+          uint8_t* st = smem + s * kStage;
+          const uint32_t fold_bytes = nj * sizeof(double4);
           // The table boxes always transfer kRows x kTJ elements (zero fill out of range).
-          mbar_arrive_tx(&full[s], 2u * L::kTab + 4u * kG * fold_bytes);
+          mbar_arrive_tx(&full[s], 2u * kTab + 4u * fold_bytes);
           tma_load_2d(st, &tmv, j0, (int)row0, &full[s]);
-          tma_load_2d(st + L::kTab, &tmd, j0, (int)row0, &full[s]);
-#pragma unroll
-          for (int gm = 0; gm < kG; ++gm)
-            for (int q = 0; q < 4; ++q)
-              bulk_g2s(st + 2 * L::kTab + gm * L::kFold + q * kTJ * sizeof(F4),
-                       fold + gm * fold_stride + ((size_t)m * 4 + q) * Nx + j0, fold_bytes, &full[s]);
+          tma_load_2d(st + kTab, &tmd, j0, (int)row0, &full[s]);
+          for (int q = 0; q < 4; ++q)
+            bulk_g2s(st + 2 * kTab + q * kTJ * sizeof(double4), fold + ((size_t)m * 4 + q) * Nx + j0, fold_bytes,
+                     &full[s]);
           ++n;
         }
       }
@@ -168,13 +144,11 @@ contract_stream_kernel(int Nl, int Nx, int64_t nitems, const __grid_constant__ C
       int m, g;
       item_of<kRows>(item, Nl, &m, &g);
       const int l0 = m + g * kRows;
-      double acc[kG][RW][4];
+      double acc[RW][4];
 #pragma unroll
-      for (int gm = 0; gm < kG; ++gm)
+      for (int i = 0; i < RW; ++i)
 #pragma unroll
-        for (int i = 0; i < RW; ++i)
-#pragma unroll
-          for (int c = 0; c < 4; ++c) acc[gm][i][c] = 0.0;
+        for (int c = 0; c < 4; ++c) acc[i][c] = 0.0;
       for (int t = 0; t < ntile; ++t) {
         if (!live[t] && !live[ntile + t]) continue;
         const int s = n % kStagesC;
@@ -186,82 +160,45 @@ contract_stream_kernel(int Nl, int Nx, int64_t nitems, const __grid_constant__ C
           ok = false;
         }
         if (ok) {
-          const uint8_t* st = smem + s * L::kStage;
-          const T* Tv = reinterpret_cast<const T*>(st);
-          const T* Td = reinterpret_cast<const T*>(st + L::kTab);
+          const uint8_t* st = smem + s * kStage;
+          const double* Tv = reinterpret_cast<const double*>(st);
+          const double* Td = reinterpret_cast<const double*>(st + kTab);
+          const double4* Fe = reinterpret_cast<const double4*>(st + 2 * kTab) + par * kTJ;
           const int nj = min(kTJ, Nx - t * kTJ);
-          T part[kG][RW][4];
-#pragma unroll
-          for (int gm = 0; gm < kG; ++gm)
-#pragma unroll
-            for (int i = 0; i < RW; ++i)
-#pragma unroll
-              for (int c = 0; c < 4; ++c) part[gm][i][c] = (T)0;
-#pragma unroll(kG == 1 ? 4 : 2)
+#pragma unroll 4
           for (int jj = lane; jj < nj; jj += 32) {
-            T v[RW], d[RW];
+            const double4 fe = Fe[jj], fp = Fe[2 * kTJ + jj];
 #pragma unroll
             for (int i = 0; i < RW; ++i) {
               const int r = rbase + 2 * i;
-              v[i] = Tv[r * kTJ + jj];
-              d[i] = Td[r * kTJ + jj];
-            }
-#pragma unroll
-            for (int gm = 0; gm < kG; ++gm) {
-              const F4* Fe = reinterpret_cast<const F4*>(st + 2 * L::kTab + gm * L::kFold) + par * kTJ;
-              const F4 fe = Fe[jj], fp = Fe[2 * kTJ + jj];
-#pragma unroll
-              for (int i = 0; i < RW; ++i) {
-                part[gm][i][0] = fma(v[i], fe.x, fma(d[i], fe.z, part[gm][i][0]));
-                part[gm][i][1] = fma(v[i], fe.y, fma(d[i], fe.w, part[gm][i][1]));
-                part[gm][i][2] = fma(v[i], fp.x, fma(d[i], fp.z, part[gm][i][2]));
-                part[gm][i][3] = fma(v[i], fp.y, fma(d[i], fp.w, part[gm][i][3]));
-              }
+              const double v = Tv[r * kTJ + jj], d = Td[r * kTJ + jj];
+              acc[i][0] = fma(v, fe.x, fma(d, fe.z, acc[i][0]));
+              acc[i][1] = fma(v, fe.y, fma(d, fe.w, acc[i][1]));
+              acc[i][2] = fma(v, fp.x, fma(d, fp.z, acc[i][2]));
+              acc[i][3] = fma(v, fp.y, fma(d, fp.w, acc[i][3]));
             }
           }
-#pragma unroll
-          for (int gm = 0; gm < kG; ++gm)
-#pragma unroll
-            for (int i = 0; i < RW; ++i)
-#pragma unroll
-              for (int c = 0; c < 4; ++c) acc[gm][i][c] += (double)part[gm][i][c];
         }
         __syncwarp();
         if (lane == 0) tc::mbar_arrive(&empty[s]);
         ++n;
       }
 #pragma unroll
-      for (int gm = 0; gm < kG; ++gm)
+      for (int i = 0; i < RW; ++i)
 #pragma unroll
-        for (int i = 0; i < RW; ++i)
+        for (int c = 0; c < 4; ++c)
 #pragma unroll
-          for (int c = 0; c < 4; ++c)
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) acc[gm][i][c] += __shfl_xor_sync(0xffffffffu, acc[gm][i][c], o);
+          for (int o = 16; o > 0; o >>= 1) acc[i][c] += __shfl_xor_sync(0xffffffffu, acc[i][c], o);
       if (lane == 0) {
 #pragma unroll
-        for (int gm = 0; gm < kG; ++gm) {
-          // outputs that already hold heavy-node FP64 sums (heavy.cu) are added to
-          const bool add = out.heavy_n[gm] != nullptr && *out.heavy_n[gm] > 0;
-#pragma unroll
-          for (int i = 0; i < RW; ++i) {
-            const int l = l0 + rbase + 2 * i;
-            if (l < Nl) {
-              const int64_t idx = hp_index(l, m, Nl);
-              double* ae = out.equ[gm];
-              double* ap = out.pol[gm];
-              if (add) {
-                ae[2 * idx] += acc[gm][i][0];
-                ae[2 * idx + 1] += acc[gm][i][1];
-                ap[2 * idx] += acc[gm][i][2];
-                ap[2 * idx + 1] += acc[gm][i][3];
-              } else {
-                ae[2 * idx] = acc[gm][i][0];
-                ae[2 * idx + 1] = acc[gm][i][1];
-                ap[2 * idx] = acc[gm][i][2];
-                ap[2 * idx + 1] = acc[gm][i][3];
-              }
-            }
+        for (int i = 0; i < RW; ++i) {
+          const int l = l0 + rbase + 2 * i;
+          if (l < Nl) {
+            const int64_t idx = hp_index(l, m, Nl);
+            alm_equ[2 * idx] = acc[i][0];
+            alm_equ[2 * idx + 1] = acc[i][1];
+            alm_pol[2 * idx] = acc[i][2];
+            alm_pol[2 * idx + 1] = acc[i][3];
           }
         }
       }
@@ -273,13 +210,12 @@ contract_stream_kernel(int Nl, int Nx, int64_t nitems, const __grid_constant__ C
 
 }  // namespace
 
-bool contract_stream_ok(const Geometry& g, size_t elem_bytes) {
+bool contract_stream_ok(const Geometry& g) {
   // Bulk copies need 16-byte aligned row segments.
-  return ((size_t)g.Nx * elem_bytes) % 16 == 0;
+  return ((size_t)g.Nx * sizeof(double)) % 16 == 0;
 }
 
-int make_table_tmap(CUtensorMap* tm, const void* base, size_t elem_bytes, int Nx, int64_t Nlm, int rows) {
-  const int kRows = rows > 0 ? rows : elem_bytes == 8 ? StageLayout<false, 1>::kRows : StageLayout<true, 1>::kRows;
+int make_table_tmap(CUtensorMap* tm, const void* base, int Nx, int64_t Nlm) {
   static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
   if (!encode) {
     void* fn = nullptr;
@@ -290,70 +226,29 @@ int make_table_tmap(CUtensorMap* tm, const void* base, size_t elem_bytes, int Nx
     encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
   }
   const cuuint64_t dims[2] = {(cuuint64_t)Nx, (cuuint64_t)Nlm};
-  const cuuint64_t strides[1] = {(cuuint64_t)Nx * elem_bytes};
+  const cuuint64_t strides[1] = {(cuuint64_t)Nx * sizeof(double)};
   const cuuint32_t box[2] = {(cuuint32_t)kTJ, (cuuint32_t)kRows};
   const cuuint32_t estr[2] = {1, 1};
-  CUresult r = encode(tm, elem_bytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
-                      const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+  CUresult r = encode(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<void*>(base), dims, strides, box, estr,
+                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return set_error(DSHT_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
   return DSHT_OK;
 }
 
-template <bool kMixed, int kG, int kRowsSet = 0>
-static void stream_launch(const Geometry& g, const CUtensorMap& tmv, const CUtensorMap& tmd, const void* fold,
-                          int64_t fold_stride, const uint8_t* live, const MapOut& out, unsigned* flags,
-                          cudaStream_t s) {
-  using L = StageLayout<kMixed, kG, kRowsSet>;
+void launch_contract_stream(const Geometry& g, const CUtensorMap& tmv, const CUtensorMap& tmd, const double* fold,
+                            const uint8_t* live, double* alm_equ, double* alm_pol, unsigned* flags, cudaStream_t s) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int ntile = (g.Nx + kTJ - 1) / kTJ;
   int64_t nitems = 0;
-  for (int m = 0; m < g.Nl; ++m) nitems += (g.Nl - m + L::kRows - 1) / L::kRows;
+  for (int m = 0; m < g.Nl; ++m) nitems += (g.Nl - m + kRows - 1) / kRows;
   const int64_t grid = nitems < sms ? nitems : sms;
-  auto kern = contract_stream_kernel<kMixed, kG, kRowsSet>;
-  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kBytes);
-  kern<<<(unsigned)grid, kThreads, L::kBytes, s>>>(g.Nl, g.Nx, nitems, tmv, tmd, fold, fold_stride, live, ntile,
-                                                   out, flags);
+  cudaFuncSetAttribute(contract_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kStreamBytes);
+  contract_stream_kernel<<<(unsigned)grid, kThreads, kStreamBytes, s>>>(
+      g.Nl, g.Nx, nitems, tmv, tmd, reinterpret_cast<const double4*>(fold), live, ntile, alm_equ, alm_pol, flags);
   count_launches(1);
-}
-
-void launch_contract_stream(const Geometry& g, bool mixed, const CUtensorMap& tmv, const CUtensorMap& tmd,
-                            const Workspace& ws, cudaStream_t s, const int* heavy_n) {
-  MapOut out{};
-  out.equ[0] = ws.alm_equ;
-  out.pol[0] = ws.alm_pol;
-  out.heavy_n[0] = heavy_n;
-  if (mixed)
-    stream_launch<true, 1>(g, tmv, tmd, ws.fold, 0, ws.tile_live2, out, ws.flags, s);
-  else
-    stream_launch<false, 1>(g, tmv, tmd, ws.fold, 0, ws.tile_live2, out, ws.flags, s);
-}
-
-int contract_stream_max_maps(bool mixed) { return mixed ? kMaxPass : 1; }
-
-void launch_contract_pass(const Geometry& g, bool mixed, const CUtensorMap& tmv, const CUtensorMap& tmd,
-                          const CUtensorMap& tmv16, const CUtensorMap& tmd16, const void* fold, int64_t fold_stride,
-                          int nmaps, const uint8_t* live, const MapOut& out, unsigned* flags, cudaStream_t s) {
-  if (mixed && nmaps == 4)
-    stream_launch<true, 4, 16>(g, tmv16, tmd16, fold, fold_stride, live, out, flags, s);
-  else if (mixed && nmaps == 3)
-    stream_launch<true, 3, 16>(g, tmv16, tmd16, fold, fold_stride, live, out, flags, s);
-  else if (mixed && nmaps == 2)
-    stream_launch<true, 2>(g, tmv, tmd, fold, fold_stride, live, out, flags, s);
-  else if (mixed)
-    stream_launch<true, 1>(g, tmv, tmd, fold, fold_stride, live, out, flags, s);
-  else  // FP64 tables: one map per pass (two stages of two maps' FP64 folds do not fit)
-    for (int k = 0; k < nmaps; ++k) {
-      MapOut o1{};
-      o1.equ[0] = out.equ[k];
-      o1.pol[0] = out.pol[k];
-      o1.heavy_n[0] = out.heavy_n[k];
-      stream_launch<false, 1>(g, tmv, tmd, static_cast<const double4*>(fold) + fold_stride * k, 0, live, o1, flags,
-                              s);
-    }
 }
 
 }  // namespace dsht

@@ -25,7 +25,7 @@
 // next tile accumulates into the other TMEM buffer.  Every wait is bounded and records
 // kFlagTimeout instead of hanging.  No cluster multicast anywhere.
 //
-// Bound: HBM (the table digits, 8 B per (l, m, node) as with FP32 tables) while N is
+// Bound: HBM (the table digits, 8 B per (l, m, node), half the FP64 pair) while N is
 // small; each table byte is read once per pass however many maps the pass holds.
 #include <cudaTypedefs.h>
 

@@ -43,16 +43,6 @@ struct Geometry {
   int nkeys;          // kSets * nbins
 };
 
-// Output pointers of one contraction pass (kernel parameter, passed by value).  When
-// heavy_n[k] is set and *heavy_n[k] > 0, map k's outputs already hold its heavy nodes' FP64
-// contribution (heavy.cu) and the pass adds to them instead of storing.
-constexpr int kMaxPass = 4;
-struct MapOut {
-  double* equ[kMaxPass];
-  double* pol[kMaxPass];
-  const int* heavy_n[kMaxPass];
-};
-
 // Output pointers of one tensor-core contraction pass (contract_tc.cu): map k's equatorial
 // alm to equ[k], its rotated-polar alm to pol[k] (2 Nlm doubles each).
 constexpr int kTcMaxMaps = 8;
@@ -61,11 +51,6 @@ struct TcOut {
   double* pol[kTcMaxMaps];
 };
 
-// Heavy nodes of the FP32-table contraction (heavy.cu): a (half, node) holding more than
-// 1/kHeavyDiv of a transform's total |w| is contracted in FP64 instead; at most kHeavyMax
-// of them (every point feeds two nodes, so fewer than 2 kHeavyDiv can exceed the share).
-constexpr int kHeavyDiv = 256;
-constexpr int kHeavyMax = 2 * kHeavyDiv;
 
 // Maps of one batched rotation: io[k] += R(rot[k]) when *flags[k] has polar points.
 constexpr int kMaxRot = 8;
@@ -87,11 +72,7 @@ struct Workspace {
   double* pay;          // [N][4] sorted records (cos phi, sin phi, w, t)
   uint32_t* sidx;       // [N] input index of each sorted slot (multi-map transforms)
   uint32_t* piecemax;   // [pmax] largest |w h_k| of the piece's points (float bits)
-  double* wsum;         // [pmax] sum of |w| of the piece's points
-  double* nodew;        // [2][Nx] sum of |w| feeding each (half, node)
-  uint8_t* heavy_flag;  // [fold_slots][2][Nx] node contracted in FP64 (FP32-table route)
-  int* heavy_list;      // [fold_slots][kHeavyMax] heavy entries h * Nx + j in order
-  int* heavy_n;         // [fold_slots] number of heavy entries
+  double* wsum;         // [pmax] sum of |w| of the piece's points (fold digit scales)
   uint32_t* count;      // [nkeys + 1]
   uint32_t* offset;     // [nkeys + 1]
   uint32_t* cursor;     // [nkeys]
@@ -102,7 +83,7 @@ struct Workspace {
   int* npieces;         // [1]
   unsigned* flags;      // [1]
   double* partial;      // [pmax][8][Nl]
-  double* fold;         // [fold_slots][Nl][4][Nx][4]; the tensor-core route's fold digits
+  double* fold;         // [Nl][4][Nx][4] FP64 fold; the tensor-core route's fold digits
                         // [Nl][2][4][4 tc_maps][Kp] (int8) share this region
   int16_t* cexp;        // [tc_maps][2] fold column scale exponents (tensor-core route)
   int tc_maps;          // maps one tensor-core contraction pass can hold
@@ -112,34 +93,29 @@ struct Workspace {
   double* alm_pol;      // [Nlm][2] (x nmaps for multi-map transforms)
   int64_t npts;         // N, the stride of pay
   int partial_f32;      // partial sums stored as float (tensor-core path) instead of double
-  int fold_f32;         // fold written as float4 (mixed contraction) instead of double4
   int64_t pmax;
   int piece_max;
-  int fold_slots;       // folds held at once (maps of one contraction pass)
-  int live_or;          // tile_live2 accumulates (OR) over the folds of a pass
   unsigned* slot_flags; // [kMaxRot] flags of the transforms awaiting rotation (multi-transform calls)
   unsigned* all_flags;  // [1] OR of every finished transform's flags
   size_t bytes;
 };
 
-// fold_slots: folds held at once (one contraction pass); multi: add the records of
-// multi-transform calls (gather indices, rotation and flag slots).
+// multi: add the records of multi-transform calls (gather indices, rotation and flag slots);
+// tc_maps: maps one tensor-core contraction pass holds (fold digit columns).
 size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* base, Workspace* ws,
-                        int fold_slots = 1, bool multi = false, int tc_maps = 1);
+                        bool multi = false, int tc_maps = 1);
 int default_piece_max(const Geometry& g, int64_t N);
 int plan_piece_max(const dsht_plan_s* p, int64_t N);
-// How a transform of N points runs on a plan: tensor-core bin sums (tc), FP32 tables
-// (f32_tables), streamed contraction (streamed; otherwise the FP64 fallback kernel).
+// How a transform of N points runs on a plan: tensor-core bin sums (tc), tensor-core
+// contraction of the digit tables (digits), else the FP64 tables streamed by TMA (streamed)
+// or, for Nx whose rows are not 16-byte multiples, the FP64 fallback kernel.
 struct Route {
-  bool tc, f32_tables, streamed;
-  bool digits;  // tensor-core contraction of the digit tables (contract_tc.cu)
+  bool tc, digits, streamed;
 };
 Route plan_route(const dsht_plan_s* p, int64_t N);
-int plan_maps_per_pass(const dsht_plan_s* p);
 
 // Kernels launched by api.cu (each file owns its launch helpers).
 void launch_tables(const Geometry& g, double* Yv, double* Yd, cudaStream_t s);
-void launch_tables_f32(const Geometry& g, float* Yv, float* Yd, cudaStream_t s);
 void launch_points(const Geometry& g, const double* theta, const double* phi, const void* w, int w_f32,
                    int64_t N, int mode, const Workspace& ws, cudaStream_t s);
 void launch_gather(const Geometry& g, const void* w, int w_f32, int64_t N, const Workspace& ws, cudaStream_t s);
@@ -149,9 +125,8 @@ void launch_publish_flags(const StatusOut& st, int n, unsigned* all, cudaStream_
 void launch_bin_sums_fp64(const Geometry& g, const Workspace& ws, cudaStream_t s);
 int launch_bin_sums_tc(const Geometry& g, const Workspace& ws, cudaStream_t s);
 int tc_inner_factor(int Nl);
-// Fold of the current map into ws.fold; with an FP32 fold, `heavy` ([2][Nx] flags or null)
-// marks the (half, node) entries written as zeros.
-void launch_fold(const Geometry& g, const Workspace& ws, cudaStream_t s, const uint8_t* heavy = nullptr);
+// FP64 fold of the current map into ws.fold, and the live-tile flags of the contractions.
+void launch_fold(const Geometry& g, const Workspace& ws, cudaStream_t s);
 // Digit tables and folds (digits.cu) and the tensor-core contraction (contract_tc.cu).
 int digit_kp(int Nx);                   // bytes per digit row: 2 Nx rounded up to 64
 constexpr int kTcMaxNx = 8192;          // S32 class sums stay below 2^31 for 2 Nx <= 16384
@@ -171,30 +146,14 @@ int launch_contract_tc(const Geometry& g, const CUtensorMap& tmA, const uint32_t
                        const int16_t* rexp, const uint8_t* fdig, int fdig_cols, const int16_t* cexp, int nmaps,
                        const TcOut& out, unsigned* flags, cudaStream_t s);
 
-// Heavy nodes of fold slot `slot`: flags and list from the per-piece |w| sums (ws.wsum).
-void launch_heavy_select(const Geometry& g, const Workspace& ws, int slot, cudaStream_t s);
-// Their FP64 contribution for every (l, m) stored (not added) into alm_equ / alm_pol, from
-// the per-piece bin sums ws.partial; does nothing when the slot has no heavy node.
-void launch_heavy_otf(const Geometry& g, const Workspace& ws, int slot, double* alm_equ, double* alm_pol,
-                      cudaStream_t s);
 void launch_contract_fp64(const Geometry& g, const double* Yv, const double* Yd,
                           const Workspace& ws, cudaStream_t s);
-bool contract_stream_ok(const Geometry& g, size_t elem_bytes);
-void launch_contract_stream(const Geometry& g, bool mixed, const CUtensorMap& tmv, const CUtensorMap& tmd,
-                            const Workspace& ws, cudaStream_t s, const int* heavy_n = nullptr);
-// One contraction pass over up to contract_stream_max_maps(mixed) folds (fold k at fold +
-// k * fold_stride F4 elements) that share one read of the tables; alm of fold k to
-// out.equ[k], out.pol[k].  FP64 tables take one fold per launch.
-int contract_stream_max_maps(bool mixed);
-void launch_contract_pass(const Geometry& g, bool mixed, const CUtensorMap& tmv, const CUtensorMap& tmd,
-                          const CUtensorMap& tmv16, const CUtensorMap& tmd16, const void* fold, int64_t fold_stride,
-                          int nmaps, const uint8_t* live, const MapOut& out, unsigned* flags, cudaStream_t s);
-// 2D tensor map over a (Nlm x Nx) table for the streaming contraction's TMA loads.
-// 2D tensor map of a table (node x row) with boxes of 256 nodes x `rows` rows (0: the
-// single-map row count for the element size).
-int make_table_tmap(CUtensorMap* tm, const void* base, size_t elem_bytes, int Nx, int64_t Nlm, int rows = 0);
-void launch_tables_to_f32(const Geometry& g, const double* Yv, const double* Yd, float* Yv32, float* Yd32,
-                          cudaStream_t s);
+bool contract_stream_ok(const Geometry& g);
+// FP64 tables through TMA (contract_stream.cu): alm of the fold to alm_equ / alm_pol.
+void launch_contract_stream(const Geometry& g, const CUtensorMap& tmv, const CUtensorMap& tmd, const double* fold,
+                            const uint8_t* live, double* alm_equ, double* alm_pol, unsigned* flags, cudaStream_t s);
+// 2D tensor map of an FP64 table (node x row), boxes of 256 nodes x 16 rows.
+int make_table_tmap(CUtensorMap* tm, const void* base, int Nx, int64_t Nlm);
 // An FP64 table in the JAX path's layout out[m][l - m][j] (Nl x Nl x Nx doubles, zeros
 // where l >= Nl) on the device.
 void launch_table_mlayout(const Geometry& g, const double* t64, double* out, cudaStream_t s);
@@ -230,13 +189,10 @@ __host__ __device__ inline int64_t hp_index(int l, int m, int Nl) {
 struct dsht_plan_s {
   dsht::Geometry g;
   int device = 0;
-  double* Yv = nullptr;
+  double* Yv = nullptr;  // FP64 tables (null in a compact plan)
   double* Yd = nullptr;
-  float* Yv32 = nullptr;  // FP32 copies streamed by mixed-precision executes (made on first use)
-  float* Yd32 = nullptr;
-  alignas(64) CUtensorMap tmYv, tmYd, tmYv32, tmYd32;
-  alignas(64) CUtensorMap tmYv32h, tmYd32h;  // FP32 tables, 16-row boxes (passes of 3-4 folds)
-  bool tm64 = false, tm32 = false;
+  alignas(64) CUtensorMap tmYv, tmYd;
+  bool tm64 = false;
   // Digit tables of the tensor-core contraction (digits.cu): 4 planes [Nlm][Kp] int8 in
   // rows grouped by parity, row exponents, the work items and the TMA map of the planes.
   uint8_t* dig = nullptr;

@@ -6,8 +6,10 @@
 //   A[m,j] = V0[m,j] + V2[m,j-1],   B[m,j] = dx (V1[m,j] + V3[m,j-1]).
 // The x < 0 half enters with (-1)^(l-m) (sht/sht.py:279); rows with l-m even use
 // A+ + A-, odd rows A+ - A-, for the equatorial and the rotated polar sets.
-// Output fold[m][q][j] = (A re, A im, B re, B im), q = {equ even, equ odd, pol even, pol odd}.
-// Partial sums are FP64 (plain path) or FP32 (tensor-core path); they are added in FP64.
+// Output fold[m][q][j] = (A re, A im, B re, B im), q = {equ even, equ odd, pol even, pol odd},
+// FP64, for the FP64-table contraction (the tensor-core contraction takes its fold straight
+// as digits, digits.cu).  Partial sums are FP64 (plain path) or FP32 (tensor-core bin sums);
+// they are added in FP64.
 #include "dsht_internal.cuh"
 
 namespace dsht {
@@ -15,10 +17,10 @@ namespace {
 
 constexpr int kFoldThreads = 128;
 
-template <typename T, typename F4>
+template <typename T>
 __global__ void __launch_bounds__(kFoldThreads)
 fold_kernel(int Nl, int Nx, int nbins, double dx, const int* __restrict__ piece_first,
-            const T* __restrict__ partial, F4* __restrict__ fold, const uint8_t* __restrict__ heavy) {
+            const T* __restrict__ partial, double4* __restrict__ fold) {
   const int j = blockIdx.x;
   const int m = blockIdx.y * blockDim.x + threadIdx.x;
   if (m >= Nl) return;
@@ -51,22 +53,11 @@ fold_kernel(int Nl, int Nx, int nbins, double dx, const int* __restrict__ piece_
     B[s][0] = dx * br;
     B[s][1] = dx * bi;
   }
-  using E = decltype(F4::x);
-  // Heavy (half, node) entries are contracted in FP64 elsewhere (heavy.cu): zero here.
-  if (heavy) {
-#pragma unroll
-    for (int h = 0; h < 2; ++h)
-      if (heavy[h * Nx + j])
-#pragma unroll
-        for (int s = 2 * h; s < 2 * h + 2; ++s) A[s][0] = A[s][1] = B[s][0] = B[s][1] = 0.0;
-  }
-  F4* out = fold + ((size_t)m * 4) * Nx + j;
-  out[0] = F4{(E)(A[0][0] + A[1][0]), (E)(A[0][1] + A[1][1]), (E)(B[0][0] + B[1][0]), (E)(B[0][1] + B[1][1])};
-  out[(size_t)Nx] = F4{(E)(A[0][0] - A[1][0]), (E)(A[0][1] - A[1][1]), (E)(B[0][0] - B[1][0]), (E)(B[0][1] - B[1][1])};
-  out[(size_t)2 * Nx] =
-      F4{(E)(A[2][0] + A[3][0]), (E)(A[2][1] + A[3][1]), (E)(B[2][0] + B[3][0]), (E)(B[2][1] + B[3][1])};
-  out[(size_t)3 * Nx] =
-      F4{(E)(A[2][0] - A[3][0]), (E)(A[2][1] - A[3][1]), (E)(B[2][0] - B[3][0]), (E)(B[2][1] - B[3][1])};
+  double4* out = fold + ((size_t)m * 4) * Nx + j;
+  out[0] = make_double4(A[0][0] + A[1][0], A[0][1] + A[1][1], B[0][0] + B[1][0], B[0][1] + B[1][1]);
+  out[(size_t)Nx] = make_double4(A[0][0] - A[1][0], A[0][1] - A[1][1], B[0][0] - B[1][0], B[0][1] - B[1][1]);
+  out[(size_t)2 * Nx] = make_double4(A[2][0] + A[3][0], A[2][1] + A[3][1], B[2][0] + B[3][0], B[2][1] + B[3][1]);
+  out[(size_t)3 * Nx] = make_double4(A[2][0] - A[3][0], A[2][1] - A[3][1], B[2][0] - B[3][0], B[2][1] - B[3][1]);
 }
 
 // tile_live[h][t] = 1 when any point of the equatorial (h = 0) or polar (h = 1) sets
@@ -89,29 +80,21 @@ __global__ void tile_live_kernel(int nbins, int ntile, int tile, const uint32_t*
 
 int contract_tile();
 
-void launch_fold(const Geometry& g, const Workspace& ws, cudaStream_t s, const uint8_t* heavy) {
+void launch_fold(const Geometry& g, const Workspace& ws, cudaStream_t s) {
   dim3 grid(g.Nx, (g.Nl + kFoldThreads - 1) / kFoldThreads);
-  const float* pf = reinterpret_cast<const float*>(ws.partial);
-  float4* f32 = reinterpret_cast<float4*>(ws.fold);
   double4* f64 = reinterpret_cast<double4*>(ws.fold);
-  if (ws.partial_f32 && ws.fold_f32)
-    fold_kernel<float, float4><<<grid, kFoldThreads, 0, s>>>(g.Nl, g.Nx, g.nbins, g.dx, ws.piece_first, pf, f32, heavy);
-  else if (ws.fold_f32)
-    fold_kernel<double, float4><<<grid, kFoldThreads, 0, s>>>(g.Nl, g.Nx, g.nbins, g.dx, ws.piece_first,
-                                                             ws.partial, f32, heavy);
-  else if (ws.partial_f32)
-    fold_kernel<float, double4><<<grid, kFoldThreads, 0, s>>>(g.Nl, g.Nx, g.nbins, g.dx, ws.piece_first, pf, f64, nullptr);
+  if (ws.partial_f32)
+    fold_kernel<float><<<grid, kFoldThreads, 0, s>>>(g.Nl, g.Nx, g.nbins, g.dx, ws.piece_first,
+                                                     reinterpret_cast<const float*>(ws.partial), f64);
   else
-    fold_kernel<double, double4><<<grid, kFoldThreads, 0, s>>>(g.Nl, g.Nx, g.nbins, g.dx, ws.piece_first,
-                                                              ws.partial, f64, nullptr);
+    fold_kernel<double><<<grid, kFoldThreads, 0, s>>>(g.Nl, g.Nx, g.nbins, g.dx, ws.piece_first, ws.partial, f64);
   count_launches(1);
   const int tile = contract_tile();
   const int ntile = (g.Nx + tile - 1) / tile;
   tile_live_kernel<<<(ntile + 127) / 128, 128, 0, s>>>(g.nbins, ntile, tile, ws.count, ws.tile_live, 0);
   count_launches(1);
   const int ntile2 = (g.Nx + 255) / 256;
-  tile_live_kernel<<<(ntile2 + 127) / 128, 128, 0, s>>>(g.nbins, ntile2, 256, ws.count, ws.tile_live2,
-                                                             ws.live_or);
+  tile_live_kernel<<<(ntile2 + 127) / 128, 128, 0, s>>>(g.nbins, ntile2, 256, ws.count, ws.tile_live2, 0);
   count_launches(1);
 }
 

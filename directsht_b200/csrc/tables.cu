@@ -13,7 +13,7 @@ namespace {
 
 constexpr int kTableThreads = 256;
 
-// TO = double: the FP64 tables; TO = float: the same FP64 values rounded once to float.
+// TO = double: the FP64 tables (the template keeps the store type explicit).
 // Columns m = m0 + blockIdx.y; row r of the tables lands at (r - row_base) * Nx.
 template <typename TO>
 __global__ void __launch_bounds__(kTableThreads)
@@ -53,14 +53,6 @@ table_kernel(int Nl, int Nx, double step, TO* __restrict__ Yv, TO* __restrict__ 
   }
 }
 
-__global__ void to_f32_kernel(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
-                              float* __restrict__ a32, float* __restrict__ b32) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    a32[i] = (float)a[i];
-    b32[i] = (float)b[i];
-  }
-}
-
 // out[m][k][j] = table row (l = m + k, m) at node j for k < Nl - m, else 0 (the JAX path's
 // Yv[m, l-m, :] layout with its unphysical entries nulled, sht/legendre_jax.py:14-25).
 // Grid: x over node chunks, y = k, z = m; consecutive threads take consecutive nodes.
@@ -81,13 +73,6 @@ void launch_table_mlayout(const Geometry& g, const double* t64, double* out, cud
   count_launches(1);
 }
 
-void launch_tables_to_f32(const Geometry& g, const double* Yv, const double* Yd, float* Yv32, float* Yd32,
-                          cudaStream_t s) {
-  const int64_t n = g.Nlm * (int64_t)g.Nx;
-  to_f32_kernel<<<148 * 16, 256, 0, s>>>(n, Yv, Yd, Yv32, Yd32);
-  count_launches(1);
-}
-
 template <typename TO>
 static void tables_launch(const Geometry& g, TO* Yv, TO* Yd, int m0, int m1, cudaStream_t s) {
   const size_t smem = (size_t)g.Nl * sizeof(Coef) + (size_t)(g.Nl + 1) * sizeof(double);
@@ -98,10 +83,6 @@ static void tables_launch(const Geometry& g, TO* Yv, TO* Yd, int m0, int m1, cud
 }
 
 void launch_tables(const Geometry& g, double* Yv, double* Yd, cudaStream_t s) {
-  tables_launch(g, Yv, Yd, 0, g.Nl, s);
-}
-
-void launch_tables_f32(const Geometry& g, float* Yv, float* Yd, cudaStream_t s) {
   tables_launch(g, Yv, Yd, 0, g.Nl, s);
 }
 

@@ -81,8 +81,9 @@ enum {
  *                     concentrated point sets included.  The fixed-point scale of a bin
  *                     piece is its largest |weight|: weights spanning many decades lose
  *                     accuracy (lognormal sigma <= 1.5 stays within 1e-7), and so do weights
- *                     of both signs whose sums cancel (zero-mean normal weights: ~3e-7).  Plans with
- *                     Nx > 8192 use an FP32 copy of the tables instead.
+ *                     of both signs whose sums cancel (zero-mean normal weights: ~3e-7).
+ *                     Plans with Nx > 8192 (or without room for the digit tables beside the
+ *                     FP64 pair) contract the FP64 tables instead.
  *   DSHT_PREC_MIXED_F64_TABLES : the same tensor-core sums with the FP64 tables streamed
  *                     by the CUDA-core contraction.
  * Mixed levels need Nl <= 2048; transforms of fewer than DSHT_MIXED_MIN_POINTS points run
@@ -102,7 +103,7 @@ int dsht_get_precision(dsht_plan_t plan, int* precision);
  * it beyond rounding).  DSHT_TUNE_PIECE_MAX: points per bin piece of the per-bin sums, a
  * multiple of 32 in [256, 2048], 0 = chosen from N.  DSHT_TUNE_MAPS_PER_PASS: maps or point
  * sets that share one read of the tables in a multi-transform call, 1..8, 0 = the most
- * (8 for the tensor-core contraction, 2 for the FP32 one).  Workspace sizes depend on both:
+ * (8; the tensor-core contraction only: the FP64 one reads the tables once per map).  Workspace sizes depend on both:
  * query them after tuning. */
 enum { DSHT_TUNE_PIECE_MAX = 1, DSHT_TUNE_MAPS_PER_PASS = 2 };
 int dsht_plan_tune(dsht_plan_t plan, int param, int value);
@@ -164,7 +165,7 @@ int dsht_status(unsigned flags, int mode);
  * DEVICE pointers theta[i], phi[i], w[i] (float64), alm to the DEVICE pointer alm[i]
  * (2*Nlm doubles); the pointer arrays themselves are HOST arrays read during the call.
  * Each point set is sorted on its own; the contraction serves up to 8 transforms per read
- * of the tables (DSHT_TUNE_MAPS_PER_PASS; 4 with FP32 tables, 1 with FP64 tables) and the
+ * of the digit tables (DSHT_TUNE_MAPS_PER_PASS; one per read of FP64 tables) and the
  * rotation up to 8.  Results equal those of one dsht_execute per transform.  The workspace (dsht_workspace_size_batch with the
  * largest N of the batch) is used in turn by every transform.  dsht_execute_batch
  * synchronises and returns the first error of any transform; dsht_enqueue_batch does not

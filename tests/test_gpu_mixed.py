@@ -80,8 +80,8 @@ def test_mixed_heavy_bin_and_wide_weights():
     w = rng.lognormal(0.0, 1.0, N)
     d = DirectSHT(256, 512)
     ref = d.basic_sht(th, ph, w.copy(), verbose=False)
-    # Half of the weight sits in one bin: the FP32-table level contracts that bin's two
-    # nodes in FP64 (heavy nodes), so both levels hold 1e-7.
+    # Half of the weight sits in one bin: the digit tables' fixed point is relative to each
+    # row's and fold column's scale, so both levels hold 1e-7.
     for level in ("mixed_f64_tables", "mixed"):
         d.set_precision(level)
         a = d.basic_sht(th, ph, w.copy(), verbose=False)
@@ -94,8 +94,8 @@ def _oracle_basic(Nl, Nx, th, ph, w):
 
 @pytest.mark.parametrize("case", ["one_bin", "dominant_bin", "two_bins_signed", "few_points"])
 def test_mixed_concentrated_weight_vs_oracle(case):
-    """Weight concentrated at a few nodes, against the oracle: the FP32-table level holds
-    1e-7 because the heavy nodes are contracted in FP64 with regenerated table values."""
+    """Weight concentrated at a few nodes, against the oracle: the mixed level (tensor-core
+    contraction of the 31-bit digit tables) and a compact plan hold 1e-7."""
     rng = np.random.default_rng(11)
     Nl, Nx = 200, 400
     if case == "one_bin":          # every point in one x bin
