@@ -80,6 +80,7 @@ SIGNATURES = {
     "dsht_profile_read": (ct.c_int, [_vp, _dp, ct.POINTER(ct.c_int64), ct.c_int]),
     "dsht_launch_count": (ct.c_int64, []),
     "dsht_test_stall_next_contraction": (ct.c_int, []),
+    "dsht_test_point_keys": (ct.c_int, [_vp, _vp, _vp, ct.c_int64, ct.c_int, _vp, _vp, _vp]),
     "dsht_mixed_min_points": (ct.c_int64, []),
     "dsht_last_error": (ct.c_char_p, []),
     "dsht_version": (ct.c_char_p, []),

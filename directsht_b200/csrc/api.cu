@@ -501,7 +501,8 @@ int64_t dsht_index(int Nl, int ell, int m) { return hp_index(ell, m, Nl); }
 int dsht_plan_create(int Nl, int Nx, double xmax, int flags, dsht_plan_t* plan) {
   if (!plan) return set_error(DSHT_ERR_INVALID, "plan pointer is NULL");
   *plan = nullptr;
-  if (Nl < 1 || Nx < 2 || !(xmax > 0.0 && xmax < 1.0) || Nl > 16384 || Nx > 65536)
+  // Nx <= 12288: the sort histograms 4 (Nx - 1) keys in shared memory
+  if (Nl < 1 || Nx < 2 || !(xmax > 0.0 && xmax < 1.0) || Nl > 16384 || Nx > 12288)
     return set_error(DSHT_ERR_INVALID, "invalid sizes Nl=%d Nx=%d xmax=%g", Nl, Nx, xmax);
   if (flags & ~DSHT_PLAN_F32_TABLES) return set_error(DSHT_ERR_INVALID, "unknown plan flags %d", flags);
   const bool f32_only = (flags & DSHT_PLAN_F32_TABLES) != 0;
@@ -793,6 +794,28 @@ static int batch_device(dsht_plan_t p, int ntrans, const double* const* theta, c
   DSHT_CUDA_OK(cudaStreamSynchronize(s));
   collect_profile(p);
   return flags_to_status(hf, mode);
+}
+
+int dsht_test_point_keys(dsht_plan_t p, const double* theta, const double* phi, int64_t N, int mode, uint32_t* keys,
+                         unsigned* flags, void* stream) {
+  if (!p || N < 1 || N > (int64_t)0xfffffff0LL || !theta || !phi || !keys || !flags)
+    return set_error(DSHT_ERR_INVALID, "invalid arguments");
+  if (mode != DSHT_MODE_CALL && mode != DSHT_MODE_BASIC) return set_error(DSHT_ERR_INVALID, "bad mode %d", mode);
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  std::unique_lock<std::mutex> lock(p->mu, std::defer_lock);
+  const size_t need = call_layout(p, N, 1, false, nullptr, nullptr);
+  uint8_t* base = nullptr;
+  int rc = call_workspace(p, need, nullptr, 0, lock, &base);
+  if (rc) return rc;
+  Workspace ws;
+  call_layout(p, N, 1, false, base, &ws);
+  // the sort also moves weights; the keys do not depend on them, so theta stands in
+  launch_points(p->g, theta, phi, theta, 0, N, mode, ws, s);
+  DSHT_CUDA_OK(cudaMemcpyAsync(keys, ws.key, sizeof(uint32_t) * N, cudaMemcpyDeviceToDevice, s));
+  DSHT_CUDA_OK(cudaMemcpyAsync(flags, ws.flags, sizeof(unsigned), cudaMemcpyDeviceToDevice, s));
+  DSHT_CUDA_OK(cudaStreamSynchronize(s));
+  DSHT_CUDA_OK(cudaGetLastError());
+  return DSHT_OK;
 }
 
 int dsht_execute(dsht_plan_t p, const double* theta, const double* phi, const double* w, int64_t N, int mode,

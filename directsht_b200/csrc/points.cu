@@ -81,25 +81,111 @@ __device__ __forceinline__ KeyOut point_key(const Geometry& g, double inv_dx, in
   return o;
 }
 
+// FP32 screen of point_key: the same decisions (polar or not, rotated range, sign of x, bin)
+// from FP32 sines and cosines, accepted only when no decision lies within the screen of its
+// boundary; otherwise (and for every point that raises a flag or is NaN) false, and the
+// FP64 path decides.  Bound on the FP32 x: theta, phi rounded to float move cos, sin by at
+// most 1.2e-7 and 2.4e-7 (theta in [0, 3.2], |phi| <= 8; other angles go to FP64); sincosf errs by at most 2 ulp (2.4e-7 here); the product rounds
+// once: |x32 - x| < 9e-7, and the screen is 3e-6.  The bin coordinate u = |x| / dx errs by
+// at most screen / dx plus its own rounding (nbins 2^-24 per operation): bin_guard bounds
+// both.  So an accepted key is the FP64 key.
+constexpr float kScreenX = 3e-6f;
+
+__device__ __forceinline__ bool screen_key(const Geometry& g, float inv_dx_f, float bin_guard, float xmax_f, int mode,
+                                           double th, const double* phi_p, uint32_t* key, unsigned* flag) {
+  // the bounds below hold for theta in [0, 3.2] and |phi| <= 8 (float rounding of the angles)
+  if (!(th >= 0.0 && th <= 3.2)) return false;
+  float sf, cf;
+  sincosf((float)th, &sf, &cf);
+  float x;
+  int set;
+  *flag = 0;
+  if (mode == DSHT_MODE_CALL) {
+    const float xv = fabsf(cf);
+    if (!(fabsf(xv - xmax_f) >= kScreenX)) return false;  // near the polar boundary, or NaN
+    if (xv > xmax_f) {
+      const double ph = *phi_p;
+      if (!(fabs(ph) <= 8.0)) return false;
+      float sp, cp;
+      sincosf((float)ph, &sp, &cp);
+      x = -sf * cp;
+      if (!(fabsf(x) <= xmax_f - kScreenX)) return false;  // near or beyond the rotated range
+      set = 2;
+      *flag = kFlagHasPolar;
+    } else {
+      if (!(th >= 0.0 && th > g.acos_xmax && th < g.acos_mxmax)) return false;
+      x = cf;
+      set = 0;
+    }
+  } else {
+    if (!(th >= 0.0 && th > g.acos_xmax && th < g.acos_mxmax)) return false;
+    x = cf;
+    set = 0;
+  }
+  if (!(fabsf(x) >= kScreenX)) return false;  // the sign of x near 0
+  if (x < 0.0f) set += 1;
+  const float u = fabsf(x) * inv_dx_f;
+  const int j = (int)u;
+  const float fr = u - (float)j;
+  if (!(fr >= bin_guard && fr <= 1.0f - bin_guard) || j >= g.nbins) return false;
+  *key = (uint32_t)(set * g.nbins + j);
+  return true;
+}
+
 // Count pass: the key of every point (4 bytes written) and a shared-memory histogram of the
 // keys (one global add per live key and block).  Reads theta, and phi of polar points only.
+// Keys come from the FP32 screen; the points it leaves undecided (~2 % at Nx = 2048) are
+// queued in shared memory and decided by the FP64 path a few rounds later by whole warps,
+// so the FP64 sines and cosines run for those points only.
+constexpr int kQueueRounds = 8;  // rounds of blockDim points between queue flushes
+
 __global__ void __launch_bounds__(kPointThreads)
 count_kernel(Geometry g, int mode, const double* __restrict__ theta, const double* __restrict__ phi,
-             int64_t N, uint32_t* __restrict__ keys, uint32_t* __restrict__ count, unsigned* __restrict__ flags) {
-  extern __shared__ uint32_t hist[];
+             int64_t N, uint32_t* __restrict__ keys, uint32_t* __restrict__ count, unsigned* __restrict__ flags,
+             float bin_guard) {
+  extern __shared__ uint32_t hist[];  // [nkeys], then the queue [kQueueRounds * blockDim]
+  uint32_t* queue = hist + g.nkeys;
+  __shared__ int qn;
   for (int k = threadIdx.x; k < g.nkeys; k += blockDim.x) hist[k] = 0;
+  if (threadIdx.x == 0) qn = 0;
   __syncthreads();
   unsigned fl = 0;
   const double inv_dx = 1.0 / g.dx;
+  const float inv_dx_f = (float)inv_dx, xmax_f = (float)g.xmax;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
-    const double th = theta[i];
-    double st, c;
-    sincos(th, &st, &c);
-    const KeyOut o = point_key(g, inv_dx, mode, th, st, c, phi + i);
-    keys[i] = o.key;
-    fl |= o.flag;
-    if (o.key != DSHT_KEY_DROP) atomicAdd(&hist[o.key], 1u);
+  int round = 0;
+  // block-uniform trip count: every thread reaches every flush
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < N; base += stride) {
+    const int64_t i = base + threadIdx.x;
+    if (i < N) {
+      uint32_t key;
+      unsigned f;
+      if (screen_key(g, inv_dx_f, bin_guard, xmax_f, mode, theta[i], phi + i, &key, &f)) {
+        keys[i] = key;
+        fl |= f;
+        atomicAdd(&hist[key], 1u);
+      } else {
+        queue[atomicAdd(&qn, 1)] = (uint32_t)i;
+      }
+    }
+    if (++round == kQueueRounds || base + stride >= N) {
+      round = 0;
+      __syncthreads();
+      const int nq = qn;
+      for (int q = threadIdx.x; q < nq; q += blockDim.x) {
+        const int64_t k = queue[q];
+        const double th = theta[k];
+        double st, c;
+        sincos(th, &st, &c);
+        const KeyOut o = point_key(g, inv_dx, mode, th, st, c, phi + k);
+        keys[k] = o.key;
+        fl |= o.flag;
+        if (o.key != DSHT_KEY_DROP) atomicAdd(&hist[o.key], 1u);
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) qn = 0;
+      __syncthreads();
+    }
   }
   if (fl) atomicOr(flags, fl);
   __syncthreads();
@@ -340,12 +426,16 @@ void launch_points(const Geometry& g, const double* theta, const double* phi, co
   cudaMemsetAsync(ws.count, 0, sizeof(uint32_t) * (g.nkeys + 1), s);
   cudaMemsetAsync(ws.flags, 0, sizeof(unsigned), s);
   const size_t hsmem = sizeof(uint32_t) * g.nkeys;
-  cudaFuncSetAttribute(count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem);
+  const size_t csmem = hsmem + sizeof(uint32_t) * kQueueRounds * kPointThreads;
+  cudaFuncSetAttribute(count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csmem);
   if (N > 0) {
     int64_t blocks = (N + kPointThreads * 8 - 1) / (kPointThreads * 8);
     if (blocks > 148 * 8) blocks = 148 * 8;
-    count_kernel<<<(unsigned)blocks, kPointThreads, hsmem, s>>>(g, mode, theta, phi, N, ws.key, ws.count,
-                                                               ws.flags);
+    // fraction-of-bin guard of the FP32 screen: the x bound over dx, plus the rounding of
+    // u = |x| / dx (four roundings of a value below nbins)
+    const float guard = (float)(kScreenX / g.dx + 4.0 * g.nbins * 5.960464477539063e-08 + 1e-6);
+    count_kernel<<<(unsigned)blocks, kPointThreads, csmem, s>>>(g, mode, theta, phi, N, ws.key, ws.count,
+                                                                ws.flags, guard);
     count_launches(1);
   }
   scan_kernel<<<1, kScanThreads, 0, s>>>(g.nkeys, g.nbins, ws.piece_max, ws.pmax, ws.count, ws.offset,

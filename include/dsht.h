@@ -110,7 +110,8 @@ int dsht_plan_tune(dsht_plan_t plan, int param, int value);
 int dsht_plan_get_tune(dsht_plan_t plan, int param, int* value);
 
 /* Build the x grid and the FP64 Ylm/dYlm tables on the current CUDA device.
- * Replaces DirectSHT.__init__ (sht/sht.py:32-56). Nl >= 1, Nx >= 2, 0 < xmax < 1. */
+ * Replaces DirectSHT.__init__ (sht/sht.py:32-56). 1 <= Nl <= 16384, 2 <= Nx <= 12288 (the sort histograms
+ * 4 (Nx - 1) bin keys in shared memory), 0 < xmax < 1. */
 int dsht_plan_create(int Nl, int Nx, double xmax, int flags, dsht_plan_t* plan);
 int dsht_plan_destroy(dsht_plan_t plan);
 
@@ -275,6 +276,15 @@ int dsht_profile_read(dsht_plan_t plan, double* ms, int64_t* calls, int reset);
  * call returns DSHT_ERR_CUDA ("timed out").  Lets a test check that a stalled tensor-core
  * pipeline is reported instead of hanging. */
 int dsht_test_stall_next_contraction(void);
+
+/* Test hook, no counterpart in the reference: the sort key of every point as the transform
+ * computes it (DEVICE pointers; keys[N] uint32, flags one unsigned), so tests can check the
+ * binning index for index.  key = set * (Nx - 1) + bin with set 0/1 for equatorial points
+ * of cos(theta) >= 0 / < 0 and 2/3 for rotated polar points of rotated x >= 0 / < 0, bin =
+ * numpy.digitize(|x|, x_grid) - 1 (sht/sht.py:212); 0xffffffff for a point in no set.
+ * flags holds the DSHT flag bits the call would raise. */
+int dsht_test_point_keys(dsht_plan_t plan, const double* theta, const double* phi, int64_t N, int mode,
+                         uint32_t* keys, unsigned* flags, void* stream);
 
 /* Kernels this library has launched in this process (all devices). */
 int64_t dsht_launch_count(void);
