@@ -138,6 +138,24 @@ def dram_traffic(stage, precision, N, Nlm, Nx):
     return e["bytes_per_point"] * N + e.get("bytes_per_table_entry", 0.0) * Nlm * Nx
 
 
+def nufft_logn(Nl):
+    """log2 of the NUFFT grid: 4 x 2^ceil(log2 Nl) cells, at least 64 (nufft.cu)."""
+    lg = max(int(np.ceil(np.log2(max(Nl, 1)))), 0) + 2
+    return max(lg, 6)
+
+
+def nufft_pieces(th, ph, Nx, xmax, piece):
+    """Bin pieces of a point set as the sort forms them: per (set, bin) key ceil(count/piece)."""
+    c = np.cos(th)
+    pol = np.abs(c) >= xmax
+    x = np.where(pol, -np.sin(th) * np.cos(ph), c)
+    nb = Nx - 1
+    j = np.minimum((np.abs(x) * (nb / xmax)).astype(np.int64), nb - 1)
+    key = (np.where(pol, 2, 0) + (x < 0)) * nb + j
+    counts = np.bincount(key, minlength=4 * nb)
+    return int(((counts + piece - 1) // piece).sum())
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -460,6 +478,8 @@ def main(argv=None):
                          "~/.cache/directsht_b200/autotune.json)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-fp64-compare", action="store_true")
+    ap.add_argument("--bin-sums", default="nufft", choices=["nufft", "tc"],
+                    help="bin sums of the mixed level: type-1 NUFFT (default) or direct tensor-core sums")
     ap.add_argument("--maps-per-pass", type=int, default=0, help="DSHT_TUNE_MAPS_PER_PASS (0: automatic)")
     ap.add_argument("--batch", type=int, default=None,
                     help="point sets per step for the headline (dsht_enqueue_batch); default 4 for c2, else 1")
@@ -553,6 +573,7 @@ def main(argv=None):
 
     if args.maps_per_pass:
         d.tune(maps_per_pass=args.maps_per_pass)
+    d.tune(bin_sums=args.bin_sums)
     batch = args.batch if args.batch is not None else (4 if args.workload == "c2" else 1)
     if maps > 1 or w_dtype != L.DSHT_W_F64:
         batch = 1
@@ -654,6 +675,21 @@ def main(argv=None):
             return {"kernel": "count/scan/scatter (counting sort by bin)", "bound": "hbm", "achieved": a,
                     "peak": hbm_peak, "unit": "GB/s", "frac": a / hbm_peak, "peak_source": peak_src,
                     "algorithmic": "24 B of inputs read + 32 B of sorted record written per point"}
+        if name == "bin_sums" and args.precision != "fp64" and args.bin_sums == "nufft":
+            # the NUFFT kernel's own FP64 work: per point 132 DFMA of kernel values, 48
+            # products and fixed-point conversions of the spread, ~50 for atan2 and the
+            # Hermite weights; per piece two complex FFTs of n cells (5 n log2 n each)
+            logn = nufft_logn(Nl)
+            pieces = nufft_pieces(th, ph, Nx, 0.75, 8192)
+            alg = (400.0 * N + pieces * 2 * 5.0 * (1 << logn) * logn * (2 if logn > 12 else 1)) * maps
+            a = alg / (ms * 1e-3) / 1e12
+            return {"kernel": "nufft_sums_kernel (FP64 spread, shared-memory FFT)", "bound": "fp64",
+                    "achieved": a, "peak": 40.0, "unit": "TFLOP/s", "frac": a / 40.0,
+                    "peak_source": "nominal (no measured FP64 figure)",
+                    "algorithmic": f"400 flop per point + 10 n log2 n per piece ({pieces} pieces, n = {1 << logn})",
+                    "equivalent_direct": {"value": 24.0 * N * Nl * maps / (ms * 1e-3) / 1e12, "unit": "TFLOP/s",
+                                          "what": "24 flop per (point, m, map) of the direct sums over the "
+                                                  "stage time: the rate the direct method would need"}}
         if name == "bin_sums" and args.precision != "fp64":
             alg = 24.0 * N * Nl * maps
             a = alg / (ms * 1e-3) / 1e12
@@ -803,9 +839,11 @@ def main(argv=None):
             "metric": "points*ell/s", "value": value, "unit": "points*ell/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": "i8 tensor sums + i8 digit-table contraction + f64" if args.precision == "mixed" else "f64", "data": "synthetic",
+            "dtype": ("f64" if args.precision != "mixed" else
+                      "f64 NUFFT sums + i8 digit-table contraction + f64" if args.bin_sums == "nufft" else
+                      "i8 tensor sums + i8 digit-table contraction + f64"), "data": "synthetic",
             "config": {"workload": spec["name"], "Nl": Nl, "Nx": Nx, "N": N, "maps": maps,
-                       "point_sets_per_step": batch, "precision": args.precision,
+                       "point_sets_per_step": batch, "precision": args.precision, "bin_sums": args.bin_sums,
                        "l2": f"inputs ({(th.nbytes + ph.nbytes + w.nbytes) / 1e6:.0f} MB) and tables "
                              f"({16 * d.Nlm * Nx / 1e9:.1f} GB FP64) exceed L2 every step",
                        "parallelism": f"replicas x{world}"},

@@ -31,6 +31,11 @@ DSHT_PLAN_F32_TABLES = 1
 
 DSHT_TUNE_PIECE_MAX = 1
 DSHT_TUNE_MAPS_PER_PASS = 2
+DSHT_TUNE_BIN_SUMS = 3
+
+DSHT_BIN_SUMS_AUTO = 0
+DSHT_BIN_SUMS_NUFFT = 1
+DSHT_BIN_SUMS_TC = 2
 
 DSHT_PREC_FP64 = 0
 DSHT_PREC_MIXED = 1

@@ -243,14 +243,15 @@ def autotune(batch: TransformBatch, path: str | None = None, reps: int = 2, verb
     config = {}
     main = torch.cuda.current_stream(batch.device)
     for key in batch.groups:
-        pk = f"{dev_name}|{batch.cache.precision}|{_profile_key(batch, key)}"
+        pk = f"{dev_name}|{batch.cache.precision}|nufft|{_profile_key(batch, key)}"
         if pk in store:
             config[key] = store[pk]["config"]
             continue
         plan = batch.cache.get(*key)
         f32 = plan.precision == "mixed"
         n = len(batch.groups[key])
-        pieces = [0, 512, 1024, 2048]
+        # the NUFFT bin sums of mixed plans pay one FFT per piece: larger pieces
+        pieces = [0, 4096, 16384] if f32 else [0, 512, 1024, 2048]
         per_pass = [0, 4] if f32 else [0]  # mixed plans: 8 (0) or 4 transforms per table read
         streams = [s for s in (1, 2, 4) if s <= n]
         best = None

@@ -116,8 +116,24 @@ size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* ba
   return off;
 }
 
+bool plan_uses_nufft(const dsht_plan_s* p) { return p->nu_dinv && p->tune_bin_sums != DSHT_BIN_SUMS_TC; }
+
+// Pieces of the direct sums stay at or below 2048 points (the tensor path's S32 sums stay
+// exact); the NUFFT sums pay one FFT per piece, so theirs are larger.
 int plan_piece_max(const dsht_plan_s* p, int64_t N) {
-  return p->tune_piece_max > 0 ? p->tune_piece_max : default_piece_max(p->g, N);
+  const bool nufft = plan_route(p, N).tc && plan_uses_nufft(p);
+  int pm = p->tune_piece_max > 0 ? p->tune_piece_max : nufft ? kNufftPiece : default_piece_max(p->g, N);
+  if (!nufft && pm > 2048) pm = 2048;
+  return pm;
+}
+
+int launch_bin_sums_mixed(const dsht_plan_s* p, Workspace& w2, cudaStream_t s) {
+  if (plan_uses_nufft(p)) {
+    w2.partial_f32 = 0;
+    return launch_bin_sums_nufft(p->g, w2, p->nu_logn, p->nu_dinv, p->nu_tw, s);
+  }
+  w2.partial_f32 = 1;
+  return launch_bin_sums_tc(p->g, w2, s);  // piece maxima and |w| sums first
 }
 
 Route plan_route(const dsht_plan_s* p, int64_t N) {
@@ -222,9 +238,7 @@ int run_after_sort(dsht_plan_s* p, int64_t N, int mode, double* alm, const Works
   // Small transforms run the FP64 stages even on a mixed-precision plan.
   const Route rt = plan_route(p, N);
   if (rt.tc) {
-    int rc = launch_bin_sums_tc(g, ws, s);  // piece maxima and |w| sums first
-    if (rc) return rc;
-    w2.partial_f32 = 1;
+    if (int rc = launch_bin_sums_mixed(p, w2, s)) return rc;
   } else {
     if (rt.digits) launch_piece_maxima(ws, s);  // the |w| sums (fold digit scales)
     launch_bin_sums_fp64(g, ws, s);
@@ -304,9 +318,7 @@ static int run_class_digits(dsht_plan_s* p, const Item* items, const std::vector
     prof_mark(p, DSHT_STAGE_BIN_SUMS, s);
     DSHT_CUDA_OK(cudaMemcpyAsync(w2.flags, ws.flags, sizeof(unsigned), cudaMemcpyDeviceToDevice, s));
     if (rt.tc) {
-      int rc = launch_bin_sums_tc(g, w2, s);
-      if (rc) return rc;
-      w2.partial_f32 = 1;
+      if (int rc = launch_bin_sums_mixed(p, w2, s)) return rc;
     } else {
       launch_piece_maxima(w2, s);
       launch_bin_sums_fp64(g, w2, s);
@@ -409,9 +421,7 @@ int run_items(dsht_plan_s* p, const Item* items, int n, int mode, const Workspac
       prof_mark(p, DSHT_STAGE_BIN_SUMS, s);
       DSHT_CUDA_OK(cudaMemcpyAsync(w2.flags, ws.flags, sizeof(unsigned), cudaMemcpyDeviceToDevice, s));
       if (mixed) {
-        int rc = launch_bin_sums_tc(g, w2, s);
-        if (rc) return rc;
-        w2.partial_f32 = 1;
+        if (int rc = launch_bin_sums_mixed(p, w2, s)) return rc;
       } else {
         launch_bin_sums_fp64(g, w2, s);
         w2.partial_f32 = 0;
@@ -515,6 +525,8 @@ int dsht_plan_create(int Nl, int Nx, double xmax, int flags, dsht_plan_t* plan) 
   auto fail = [&](cudaError_t e, const char* what) {
     cudaFree(p->Yv);
     cudaFree(p->Yd);
+    cudaFree(p->nu_dinv);
+    cudaFree(p->nu_tw);
     cudaFreeHost(p->h_flags);
     delete p;
     cudaGetLastError();
@@ -522,6 +534,16 @@ int dsht_plan_create(int Nl, int Nx, double xmax, int flags, dsht_plan_t* plan) 
   };
   cudaError_t e = cudaMallocHost(&p->h_flags, sizeof(unsigned));
   if (e != cudaSuccess) return fail(e, "plan allocation");
+  if (Nl <= 2048) {  // the NUFFT bin sums of the mixed levels: 1/Psi(m) and the twiddles
+    std::vector<double> dinv, tw;
+    p->nu_logn = nufft_logn(Nl);
+    nufft_host_tables(Nl, p->nu_logn, dinv, tw);
+    e = cudaMalloc(&p->nu_dinv, sizeof(double) * dinv.size());
+    if (e == cudaSuccess) e = cudaMalloc(&p->nu_tw, sizeof(double) * tw.size());
+    if (e == cudaSuccess) e = cudaMemcpy(p->nu_dinv, dinv.data(), sizeof(double) * dinv.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(p->nu_tw, tw.data(), sizeof(double) * tw.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return fail(e, "plan allocation");
+  }
   if (f32_only) {
     // compact plan: the digit tables alone, built from FP64 columns a few m at a time
     if (int rc = build_digits(p)) {
@@ -561,6 +583,8 @@ int dsht_plan_destroy(dsht_plan_t p) {
   cudaFree(p->dig);
   cudaFree(p->rexp);
   cudaFree(p->tc_items);
+  cudaFree(p->nu_dinv);
+  cudaFree(p->nu_tw);
   cudaFree(p->ws);
   cudaFree(p->in);
   cudaFree(p->alm);
@@ -592,9 +616,14 @@ int dsht_plan_tune(dsht_plan_t p, int param, int value) {
   std::lock_guard<std::mutex> lock(p->mu);
   switch (param) {
     case DSHT_TUNE_PIECE_MAX:
-      if (value != 0 && (value < 256 || value > 2048 || value % 32))
-        return set_error(DSHT_ERR_INVALID, "piece size %d: 0 or a multiple of 32 in [256, 2048]", value);
+      if (value != 0 && (value < 256 || value > 65536 || value % 32))
+        return set_error(DSHT_ERR_INVALID, "piece size %d: 0 or a multiple of 32 in [256, 65536]", value);
       p->tune_piece_max = value;
+      return DSHT_OK;
+    case DSHT_TUNE_BIN_SUMS:
+      if (value != DSHT_BIN_SUMS_AUTO && value != DSHT_BIN_SUMS_NUFFT && value != DSHT_BIN_SUMS_TC)
+        return set_error(DSHT_ERR_INVALID, "bin-sum method %d: AUTO (0), NUFFT (1) or TC (2)", value);
+      p->tune_bin_sums = value;
       return DSHT_OK;
     case DSHT_TUNE_MAPS_PER_PASS:
       if (value < 0 || value > kTcMaxMaps)
@@ -609,6 +638,7 @@ int dsht_plan_get_tune(dsht_plan_t p, int param, int* value) {
   if (!p || !value) return set_error(DSHT_ERR_INVALID, "invalid arguments");
   if (param == DSHT_TUNE_PIECE_MAX) *value = p->tune_piece_max;
   else if (param == DSHT_TUNE_MAPS_PER_PASS) *value = p->tune_maps_per_pass;
+  else if (param == DSHT_TUNE_BIN_SUMS) *value = p->tune_bin_sums;
   else return set_error(DSHT_ERR_INVALID, "unknown tuning parameter %d", param);
   return DSHT_OK;
 }

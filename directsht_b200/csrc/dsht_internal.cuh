@@ -124,6 +124,12 @@ void launch_piece_maxima(const Workspace& ws, cudaStream_t s);
 void launch_publish_flags(const StatusOut& st, int n, unsigned* all, cudaStream_t s);
 void launch_bin_sums_fp64(const Geometry& g, const Workspace& ws, cudaStream_t s);
 int launch_bin_sums_tc(const Geometry& g, const Workspace& ws, cudaStream_t s);
+// NUFFT bin sums (nufft.cu): FP64 partial sums [piece][8][Nl] and the pieces' |w| sums.
+int nufft_logn(int Nl);
+void nufft_host_tables(int Nl, int logn, std::vector<double>& dinv, std::vector<double>& tw);
+int launch_bin_sums_nufft(const Geometry& g, const Workspace& ws, int logn, const double* dinv, const double* tw,
+                          cudaStream_t s);
+constexpr int kNufftPiece = 8192;  // default points per piece of the NUFFT sums
 int tc_inner_factor(int Nl);
 // FP64 fold of the current map into ws.fold, and the live-tile flags of the contractions.
 void launch_fold(const Geometry& g, const Workspace& ws, cudaStream_t s);
@@ -210,7 +216,13 @@ struct dsht_plan_s {
   double* alm = nullptr;  // [2 Nlm]
   unsigned* h_flags = nullptr;  // pinned
   int precision = DSHT_PREC_FP64;
-  int tune_piece_max = 0;      // points per bin piece (0: chosen from N)
+  // Type-1 NUFFT bin sums (nufft.cu): grid of 2^nu_logn cells, 1/Psi(m) [Nl] and the
+  // twiddles e^{2 pi i i/n} [n] (complex), built at plan creation for Nl <= 2048.
+  int nu_logn = 0;
+  double* nu_dinv = nullptr;
+  double* nu_tw = nullptr;
+  int tune_bin_sums = DSHT_BIN_SUMS_AUTO;
+  int tune_piece_max = 0;      // points per bin piece (0: chosen from N and the method)
   int tune_maps_per_pass = 0;  // maps per multi-map contraction pass (0: the most that fit)
   // Stage timers: one event per stage boundary of a call, in stream order; the interval
   // from mark k to mark k+1 belongs to stage ev_stage[k] (-1: no stage).  Summed per stage
@@ -245,6 +257,10 @@ struct Item {
   bool same_points;
   unsigned* status;  // device word that receives the item's flags, or null
 };
+// Bin sums of a tensor-core-route transform: the NUFFT (default) or the tensor-core direct
+// sums; sets w2.partial_f32 to the layout written.
+int launch_bin_sums_mixed(const dsht_plan_s* p, Workspace& w2, cudaStream_t s);
+bool plan_uses_nufft(const dsht_plan_s* p);
 // Runs the items in order; every finished item's flags are OR-ed into ws.all_flags.
 int run_items(dsht_plan_s* p, const Item* items, int n, int mode, const Workspace& ws, cudaStream_t s);
 // After the stream has been synchronised: fold the stage events into the plan's totals.

@@ -1,0 +1,440 @@
+// Per-bin sums by a type-1 non-uniform FFT (the MIXED level's default bin-sum method).
+//
+// For one piece (points of one (set, bin) key) the sums of sht/shared_interp_funcs.py:88-105,
+//   v_k[m] = sum_p g_k(p) e^{i m phi_p},  g_k = w h_k(t) (sht/sht.py:239-240),  0 <= m < Nl,
+// are the Fourier coefficients of four real point distributions on the circle.  Each point
+// is spread onto a periodic real grid of n = 4 * 2^ceil(log2 Nl) cells (oversampling 2 of
+// the 2 Nl frequencies -Nl < m < Nl) with the "exponential of semicircle" kernel
+//   psi(x) = exp(beta (sqrt(1 - (2x/W)^2) - 1)),  |x| < W/2 cells,  W = 12, beta = 2.30 W
+// (Barnett, Magland & af Klinteberg, SIAM J. Sci. Comput. 41 (2019) C479), then
+//   v_k[m] = (sum_j G_k[j] e^{2 pi i m j / n}) / Psi(m),  Psi(m) = int psi(x) e^{-2 pi i m x/n} dx
+// up to a relative error of about 5e-12 of sum_p |g_k(p)| (aliasing of the truncated
+// kernel).  The two real grids of a pair (k, k+1) form one complex sequence, so four
+// grids take two complex FFTs; v_k and v_(k+1) come apart by the conjugate symmetry of a
+// real sequence's transform.
+//
+// Kernel values: psi at the W cells next to a point is a polynomial of degree 11 in the
+// point's fractional cell offset, one polynomial per cell (Chebyshev interpolants,
+// converted to monomials on the host; max error 1e-13 of psi(0)).  They are passed as a
+// kernel parameter, so every Horner step is one DFMA with a uniform operand.
+//
+// One CTA per piece (persistent over pieces): zero the padded grids in shared memory,
+// spread every point of the piece (64-bit fixed point of step 2^-50 of the piece's sum |w|,
+// shared-memory integer atomics: 4 x W per point, so the sums are exact and do not depend
+// on the order of the adds), convert to FP64, an in-place decimation-in-frequency FFT (radix-16 passes and one radix-2/4/8 pass, the
+// 16-point DFTs in registers), then each thread reads the outputs of its m from their
+// digit-reversed positions, divides by Psi(m) and writes the piece's partial sums
+// [8][Nl] (FP64, k-major, re | im).  The grid index i is stored at i + i/16 (one 16-byte
+// pad per 16 entries) so that the last pass's unit-stride butterflies hit distinct banks.
+// FP64 throughout; no tensor cores: per point about 130 DFMA for the kernel values and 96
+// for the spread, per piece 2 x 5 n log2 n for the FFTs -- against 24 x Nl flop per point
+// for the direct sums.
+#include <cmath>
+#include <mutex>
+#include <vector>
+
+#include "dsht_internal.cuh"
+
+namespace dsht {
+
+constexpr int kEsW = 12;     // kernel width in cells
+constexpr int kEsDeg = 11;   // polynomial degree per cell
+constexpr double kEsBeta = 2.30 * kEsW;
+
+// Kernel-parameter copy of the per-cell polynomials: c[i][d], cell i = 0..W-1 of a point
+// whose cell is c0 is (c0 - W/2 + 1 + i) and its offset x = f + W/2 - 1 - i, f = u - c0.
+struct EsPoly {
+  double c[kEsW][kEsDeg + 1];
+};
+
+namespace {
+
+constexpr int kNuThreads = 512;
+
+__device__ __forceinline__ int padi(int i) { return i + (i >> 4); }
+
+// rint(x) as a two's-complement integer for |x| < 2^51: one DFMA puts x into the binade of
+// 1.5 2^52, whose low bits are then the rounded integer (no conversion instruction).
+__device__ __forceinline__ unsigned long long fixed_point(double x) {
+  return (unsigned long long)(__double_as_longlong(x + 6755399441055744.0) - 0x4338000000000000ll);
+}
+__device__ __forceinline__ double from_fixed(long long v) {
+  return __longlong_as_double(v + 0x4338000000000000ll) - 6755399441055744.0;
+}
+
+__device__ __forceinline__ double2 cmul2(double2 a, double2 b) {
+  return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+
+// cos, sin of 2 pi e / 16 for a compile-time e (after unrolling).
+__device__ __forceinline__ double cos16(int e) {
+  constexpr double C1 = 0.92387953251128675613, C2 = 0.70710678118654752440, C3 = 0.38268343236508977173;
+  switch (e & 15) {
+    case 0: return 1.0;
+    case 1: return C1;
+    case 2: return C2;
+    case 3: return C3;
+    case 4: return 0.0;
+    case 5: return -C3;
+    case 6: return -C2;
+    case 7: return -C1;
+    case 8: return -1.0;
+    case 9: return -C1;
+    case 10: return -C2;
+    case 11: return -C3;
+    case 12: return 0.0;
+    case 13: return C3;
+    case 14: return C2;
+    default: return C1;
+  }
+}
+__device__ __forceinline__ double sin16(int e) { return cos16(e - 4); }
+
+// v * e^{2 pi i e / R}; the quarter turns are exact swaps and sign changes.
+template <int R>
+__device__ __forceinline__ double2 rot(double2 v, int e) {
+  const int e16 = (e * (16 / R)) & 15;
+  if (e16 == 0) return v;
+  if (e16 == 4) return make_double2(-v.y, v.x);
+  if (e16 == 8) return make_double2(-v.x, -v.y);
+  if (e16 == 12) return make_double2(v.y, -v.x);
+  const double c = cos16(e16), s = sin16(e16);
+  return make_double2(fma(v.x, c, -v.y * s), fma(v.x, s, v.y * c));
+}
+
+// In-register R-point DFT with the + sign, y_S = sum_r x_r e^{2 pi i r S / R}.  R = 8, 16
+// split as 4 x (R/4): radix-4 over r = 4-blocks, twiddle, R/4-point DFTs; output S lands
+// in register dreg<R>(S).
+template <int R>
+__device__ __forceinline__ constexpr int dreg(int S) {
+  return R <= 4 ? S : (R / 4) * (S % 4) + S / 4;
+}
+
+__device__ __forceinline__ void dft4(double2& x0, double2& x1, double2& x2, double2& x3) {
+  const double2 a0 = make_double2(x0.x + x2.x, x0.y + x2.y), a1 = make_double2(x0.x - x2.x, x0.y - x2.y);
+  const double2 b0 = make_double2(x1.x + x3.x, x1.y + x3.y), b1 = make_double2(x1.x - x3.x, x1.y - x3.y);
+  x0 = make_double2(a0.x + b0.x, a0.y + b0.y);
+  x2 = make_double2(a0.x - b0.x, a0.y - b0.y);
+  x1 = make_double2(a1.x - b1.y, a1.y + b1.x);  // a1 + i b1
+  x3 = make_double2(a1.x + b1.y, a1.y - b1.x);  // a1 - i b1
+}
+
+template <int R>
+__device__ __forceinline__ void dft(double2 (&x)[R]) {
+  if constexpr (R == 2) {
+    const double2 a = x[0], b = x[1];
+    x[0] = make_double2(a.x + b.x, a.y + b.y);
+    x[1] = make_double2(a.x - b.x, a.y - b.y);
+  } else if constexpr (R == 4) {
+    dft4(x[0], x[1], x[2], x[3]);
+  } else {
+    constexpr int R2 = R / 4;
+    // radix 4 over the blocks of R2: element t + R2 r, output s goes to register t + R2 s
+#pragma unroll
+    for (int t = 0; t < R2; ++t) {
+      dft4(x[t], x[t + R2], x[t + 2 * R2], x[t + 3 * R2]);
+#pragma unroll
+      for (int s = 1; s < 4; ++s) x[t + R2 * s] = rot<R>(x[t + R2 * s], t * s);
+    }
+    // R2-point DFTs of each s: registers R2 s .. R2 s + R2 - 1, output k' in register R2 s + k'
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      if constexpr (R2 == 2) {
+        const double2 a = x[R2 * s], b = x[R2 * s + 1];
+        x[R2 * s] = make_double2(a.x + b.x, a.y + b.y);
+        x[R2 * s + 1] = make_double2(a.x - b.x, a.y - b.y);
+      } else {
+        dft4(x[R2 * s], x[R2 * s + 1], x[R2 * s + 2], x[R2 * s + 3]);
+      }
+    }
+  }
+}
+
+// One decimation-in-frequency pass of radix R over span L on `nseq` padded sequences of
+// length n: butterfly (b, j), base = b L + j, elements base + r L/R; outputs S times
+// e^{2 pi i j S / L} back to base + S L/R.  tw[i] = e^{2 pi i i / n}.
+template <int R>
+__device__ __forceinline__ void fft_pass(double2* zs, int nseq, int seq_stride, int logn, int logL,
+                                         const double2* __restrict__ tw) {
+  constexpr int logR = R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : 4;
+  const int logs = logL - logR;  // log2 of the stride L/R
+  const int nb = 1 << (logn - logR);
+  for (int q = threadIdx.x; q < nseq * nb; q += blockDim.x) {
+    const int seq = q >> (logn - logR), qq = q & (nb - 1);
+    const int j = qq & ((1 << logs) - 1);
+    const int base = ((qq >> logs) << logL) + j;
+    double2* z = zs + seq * seq_stride;
+    double2 x[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) x[r] = z[padi(base + (r << logs))];
+    dft<R>(x);
+    if (j) {
+      const double2 w1 = tw[j << (logn - logL)];
+      double2 ws = w1;
+#pragma unroll
+      for (int S = 1; S < R; ++S) {
+        x[dreg<R>(S)] = cmul2(x[dreg<R>(S)], ws);
+        if (S + 1 < R) ws = cmul2(ws, w1);
+      }
+    }
+#pragma unroll
+    for (int S = 0; S < R; ++S) z[padi(base + (S << logs))] = x[dreg<R>(S)];
+  }
+}
+
+// Position of output k after the passes (radix 16 first, then 2^(logn % 4)).
+__device__ __forceinline__ int fft_pos(int k, int logn) {
+  int pos = 0, lg = logn;
+  while (lg >= 4) {
+    lg -= 4;
+    pos += (k & 15) << lg;
+    k >>= 4;
+  }
+  return pos + k;  // the last pass (radix 2^lg) leaves its digit in place
+}
+
+template <int NSEQ>
+__device__ void fft_all(double2* zs, int seq_stride, int logn, const double2* __restrict__ tw) {
+  int logL = logn;
+  while (logL >= 4) {
+    fft_pass<16>(zs, NSEQ, seq_stride, logn, logL, tw);
+    logL -= 4;
+    __syncthreads();
+  }
+  if (logL == 1) fft_pass<2>(zs, NSEQ, seq_stride, logn, logL, tw);
+  else if (logL == 2) fft_pass<4>(zs, NSEQ, seq_stride, logn, logL, tw);
+  else if (logL == 3) fft_pass<8>(zs, NSEQ, seq_stride, logn, logL, tw);
+  __syncthreads();
+}
+
+// KP: Hermite weights per pass, 4 (two sequences; n <= 4096) or 2 (one sequence; n = 8192).
+template <int KP>
+__global__ void __launch_bounds__(kNuThreads, 1)
+nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* __restrict__ npieces_p,
+                  int64_t pmax, const int64_t* __restrict__ piece_start, const int* __restrict__ piece_len,
+                  const double* __restrict__ dinv, const double2* __restrict__ tw, const EsPoly es,
+                  double* __restrict__ partial, double* __restrict__ wsum) {
+  constexpr int NSEQ = KP / 2;
+  extern __shared__ double2 zs[];  // [NSEQ][n + n/16]
+  __shared__ double red[kNuThreads / 32];
+  const int n = 1 << logn;
+  const int seq_stride = n + (n >> 4);
+  const double u_per_rad = (double)n * 0.15915494309189533577;  // n / (2 pi)
+  const double two_pi = 6.28318530717958647693;
+  const int npieces = (int)min((int64_t)*npieces_p, pmax);
+  for (int piece = blockIdx.x; piece < npieces; piece += gridDim.x) {
+    const int64_t start = piece_start[piece];
+    const int len = piece_len[piece];
+    // sum |w| of the piece: bounds every grid value (|h_k| <= 1, psi <= 1), so the spread
+    // runs in 64-bit fixed point of step 2^-50 sum|w| -- integer atomics, so the grid (and
+    // every result) does not depend on the order of the adds
+    double wabs = 0.0;
+    for (int p = threadIdx.x; p < len; p += blockDim.x) wabs += fabs(pay[(size_t)kRec * (start + p) + 2]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) wabs += __shfl_xor_sync(0xffffffffu, wabs, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = wabs;
+    __syncthreads();
+    wabs = 0.0;
+    for (int i = 0; i < kNuThreads / 32; ++i) wabs += red[i];
+    if (threadIdx.x == 0) wsum[piece] = wabs;
+    const double fx_scale = wabs > 0.0 ? 0x1p50 / wabs : 1.0;
+    const double fx_step = wabs > 0.0 ? wabs * 0x1p-50 : 1.0;
+    for (int kp = 0; kp < 4; kp += KP) {
+      for (int i = threadIdx.x; i < NSEQ * seq_stride; i += blockDim.x) zs[i] = make_double2(0.0, 0.0);
+      __syncthreads();
+      unsigned long long* zi = reinterpret_cast<unsigned long long*>(zs);
+      for (int p = threadIdx.x; p < len; p += blockDim.x) {
+        const double2* rec = reinterpret_cast<const double2*>(pay + (size_t)kRec * (start + p));
+        const double2 r0 = rec[0], r1 = rec[1];  // (cos phi, sin phi), (w, t)
+        double phi = atan2(r0.y, r0.x);
+        if (phi < 0.0) phi += two_pi;
+        const double u = phi * u_per_rad;
+        const double fl = floor(u);
+        const double sv = 2.0 * (u - fl) - 1.0;
+        const int c0 = (int)fl - kEsW / 2 + 1;
+        double ker[kEsW];
+#pragma unroll
+        for (int i = 0; i < kEsW; ++i) {
+          double acc = es.c[i][kEsDeg];
+#pragma unroll
+          for (int d = kEsDeg - 1; d >= 0; --d) acc = fma(acc, sv, es.c[i][d]);
+          ker[i] = acc * fx_scale;
+        }
+        double h[4];
+        hermite(r1.y, r1.x, h);
+        double ga[NSEQ], gb[NSEQ];  // the pass's weights: sequence q holds k = kp + 2q, kp + 2q + 1
+#pragma unroll
+        for (int q = 0; q < NSEQ; ++q) {
+          const bool lo = kp + 2 * q == 0;
+          ga[q] = lo ? h[0] : h[2];
+          gb[q] = lo ? h[1] : h[3];
+        }
+#pragma unroll
+        for (int i = 0; i < kEsW; ++i) {
+          const int cell = padi((c0 + i) & (n - 1));
+#pragma unroll
+          for (int q = 0; q < NSEQ; ++q) {
+            unsigned long long* z = zi + 2 * (q * seq_stride + cell);
+            atomicAdd(z, fixed_point(ga[q] * ker[i]));
+            atomicAdd(z + 1, fixed_point(gb[q] * ker[i]));
+          }
+        }
+      }
+      __syncthreads();
+      // fixed point -> FP64 (exact: |value| < 2^51); the step is applied to the outputs
+      for (int i = threadIdx.x; i < NSEQ * seq_stride; i += blockDim.x) {
+        const longlong2 v = reinterpret_cast<const longlong2*>(zs)[i];
+        zs[i] = make_double2(from_fixed(v.x), from_fixed(v.y));
+      }
+      __syncthreads();
+      fft_all<NSEQ>(zs, seq_stride, logn, tw);
+      // v_k0 = (Z[m] + conj Z[-m]) / 2, v_k1 = (Z[m] - conj Z[-m]) / 2i, each over Psi(m)
+      for (int m = threadIdx.x; m < Nl; m += blockDim.x) {
+        const int pm = padi(fft_pos(m, logn)), pn = padi(fft_pos((n - m) & (n - 1), logn));
+        const double di = 0.5 * fx_step * dinv[m];
+#pragma unroll
+        for (int q = 0; q < NSEQ; ++q) {
+          const double2 a = zs[q * seq_stride + pm], b = zs[q * seq_stride + pn];
+          const int k0 = kp + 2 * q;
+          double* o = partial + ((size_t)piece * 8 + 2 * k0) * Nl + m;
+          o[0] = (a.x + b.x) * di;
+          o[(size_t)Nl] = (a.y - b.y) * di;
+          o[(size_t)2 * Nl] = (a.y + b.y) * di;
+          o[(size_t)3 * Nl] = (b.x - a.x) * di;
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// ---- host: kernel polynomials and the deconvolution factors ----------------------------
+
+double es_kernel(double x) {
+  const double z = 2.0 * x / kEsW;
+  if (!(std::fabs(z) < 1.0)) return 0.0;
+  return std::exp(kEsBeta * (std::sqrt(1.0 - z * z) - 1.0));
+}
+
+// Chebyshev interpolation of psi(f + W/2 - 1 - i) at kEsDeg + 1 nodes in s = 2f - 1,
+// converted to monomial coefficients in s.
+EsPoly make_es_poly() {
+  EsPoly P{};
+  constexpr int np = kEsDeg + 1;
+  const double pi = 3.14159265358979323846;
+  for (int i = 0; i < kEsW; ++i) {
+    double y[np], s[np];
+    for (int j = 0; j < np; ++j) {
+      s[j] = std::cos(pi * (j + 0.5) / np);
+      y[j] = es_kernel((s[j] + 1.0) / 2.0 + kEsW / 2 - 1 - i);
+    }
+    double a[np];  // Chebyshev coefficients
+    for (int k = 0; k < np; ++k) {
+      double acc = 0.0;
+      for (int j = 0; j < np; ++j) acc += y[j] * std::cos(pi * k * (j + 0.5) / np);
+      a[k] = acc * (k == 0 ? 1.0 : 2.0) / np;
+    }
+    // sum_k a_k T_k(s) in monomials: T_(k+1) = 2 s T_k - T_(k-1)
+    std::vector<double> tkm(np, 0.0), tk(np, 0.0), tkp(np, 0.0);
+    tkm[0] = 1.0;  // T_0
+    tk[1] = 1.0;   // T_1
+    for (int d = 0; d < np; ++d) P.c[i][d] = a[0] * tkm[d] + (np > 1 ? a[1] * tk[d] : 0.0);
+    for (int k = 1; k + 1 < np; ++k) {
+      for (int d = 0; d < np; ++d) tkp[d] = (d > 0 ? 2.0 * tk[d - 1] : 0.0) - tkm[d];
+      for (int d = 0; d < np; ++d) P.c[i][d] += a[k + 1] * tkp[d];
+      tkm.swap(tk);
+      tk.swap(tkp);
+    }
+  }
+  return P;
+}
+
+// Gauss-Legendre nodes and weights on [-1, 1] (Newton iteration on P_q from the
+// Chebyshev-like initial guesses).
+void gauss_legendre(int q, std::vector<double>& x, std::vector<double>& w) {
+  const double pi = 3.14159265358979323846;
+  x.assign(q, 0.0);
+  w.assign(q, 0.0);
+  for (int i = 0; i < (q + 1) / 2; ++i) {
+    double z = std::cos(pi * (i + 0.75) / (q + 0.5)), dp = 0.0;
+    for (int it = 0; it < 100; ++it) {
+      double p0 = 1.0, p1 = z;
+      for (int k = 2; k <= q; ++k) {
+        const double p2 = ((2.0 * k - 1.0) * z * p1 - (k - 1.0) * p0) / k;
+        p0 = p1;
+        p1 = p2;
+      }
+      if (q == 1) p0 = 1.0;
+      dp = q * (z * p1 - p0) / (z * z - 1.0);
+      const double dz = p1 / dp;
+      z -= dz;
+      if (std::fabs(dz) < 1e-16) break;
+    }
+    x[i] = -z;
+    x[q - 1 - i] = z;
+    w[i] = w[q - 1 - i] = 2.0 / ((1.0 - z * z) * dp * dp);
+  }
+}
+
+}  // namespace
+
+int nufft_logn(int Nl) {
+  int lg = 2;  // n = 4 * 2^ceil(log2 Nl), at least 64
+  while ((1 << lg) < Nl) ++lg;
+  lg += 2;
+  return lg < 6 ? 6 : lg;
+}
+
+const EsPoly& es_poly() {
+  static const EsPoly P = make_es_poly();
+  return P;
+}
+
+// 1 / Psi(m), m < Nl, and the twiddles e^{2 pi i i / n}, i < n, for a plan.
+void nufft_host_tables(int Nl, int logn, std::vector<double>& dinv, std::vector<double>& tw) {
+  const int n = 1 << logn;
+  const double pi = 3.14159265358979323846;
+  std::vector<double> gx, gw;
+  gauss_legendre(96, gx, gw);
+  dinv.assign(Nl, 0.0);
+  for (int m = 0; m < Nl; ++m) {
+    double acc = 0.0;
+    for (size_t i = 0; i < gx.size(); ++i) {
+      const double x = gx[i] * (kEsW / 2.0);
+      acc += gw[i] * es_kernel(x) * std::cos(2.0 * pi * m * x / n);
+    }
+    dinv[m] = 1.0 / (acc * (kEsW / 2.0));
+  }
+  tw.assign(2 * (size_t)n, 0.0);
+  for (int i = 0; i < n; ++i) {
+    tw[2 * i] = std::cos(2.0 * pi * i / n);
+    tw[2 * i + 1] = std::sin(2.0 * pi * i / n);
+  }
+}
+
+int launch_bin_sums_nufft(const Geometry& g, const Workspace& ws, int logn, const double* dinv, const double* tw,
+                          cudaStream_t s) {
+  const int n = 1 << logn;
+  const int kp = logn <= 12 ? 4 : 2;
+  const size_t smem = sizeof(double2) * (size_t)(kp / 2) * (n + n / 16);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int64_t grid = ws.pmax < sms ? ws.pmax : sms;
+  if (grid < 1) grid = 1;
+  auto go = [&](auto kern) -> int {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return set_cuda_error(e, "nufft attributes", __FILE__, __LINE__);
+    kern<<<(unsigned)grid, kNuThreads, smem, s>>>(g.Nl, logn, ws.pay, ws.npieces, ws.pmax, ws.piece_start,
+                                                  ws.piece_len, dinv, reinterpret_cast<const double2*>(tw),
+                                                  es_poly(), ws.partial, ws.wsum);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return set_cuda_error(e, "nufft launch", __FILE__, __LINE__);
+    count_launches(1);
+    return DSHT_OK;
+  };
+  if (logn > 13) return set_error(DSHT_ERR_INVALID, "NUFFT bin sums support Nl <= 2048 (Nl=%d)", g.Nl);
+  return kp == 4 ? go(nufft_sums_kernel<4>) : go(nufft_sums_kernel<2>);
+}
+
+}  // namespace dsht

@@ -97,18 +97,27 @@ class DirectSHT:
         self.precision = precision
 
     # -- tables ---------------------------------------------------------------------
-    def tune(self, piece_max=None, maps_per_pass=None):
-        """Set launch-shape parameters (``dsht_plan_tune``); None leaves one unchanged, 0
-        restores the automatic choice.  Returns the current values as a dict."""
+    _BIN_SUMS = {"auto": L.DSHT_BIN_SUMS_AUTO, "nufft": L.DSHT_BIN_SUMS_NUFFT, "tc": L.DSHT_BIN_SUMS_TC}
+
+    def tune(self, piece_max=None, maps_per_pass=None, bin_sums=None):
+        """Set tuning parameters (``dsht_plan_tune``); None leaves one unchanged, 0 (or
+        'auto') restores the automatic choice.  bin_sums picks the mixed levels' per-bin sums:
+        'nufft' (the default) or 'tc' (direct tensor-core sums).  Returns the current values
+        as a dict (bin_sums as its name)."""
         if piece_max is not None:
             L.check(self._lib.dsht_plan_tune(self._plan, L.DSHT_TUNE_PIECE_MAX, int(piece_max)))
         if maps_per_pass is not None:
             L.check(self._lib.dsht_plan_tune(self._plan, L.DSHT_TUNE_MAPS_PER_PASS, int(maps_per_pass)))
+        if bin_sums is not None:
+            code = self._BIN_SUMS[bin_sums] if isinstance(bin_sums, str) else int(bin_sums)
+            L.check(self._lib.dsht_plan_tune(self._plan, L.DSHT_TUNE_BIN_SUMS, code))
         out = {}
-        for name, code in (("piece_max", L.DSHT_TUNE_PIECE_MAX), ("maps_per_pass", L.DSHT_TUNE_MAPS_PER_PASS)):
+        for name, code in (("piece_max", L.DSHT_TUNE_PIECE_MAX), ("maps_per_pass", L.DSHT_TUNE_MAPS_PER_PASS),
+                           ("bin_sums", L.DSHT_TUNE_BIN_SUMS)):
             v = ct.c_int()
             L.check(self._lib.dsht_plan_get_tune(self._plan, code, ct.byref(v)))
             out[name] = v.value
+        out["bin_sums"] = {v: k for k, v in self._BIN_SUMS.items()}[out["bin_sums"]]
         return out
 
     def indx(self, ell, m):

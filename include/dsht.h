@@ -70,22 +70,28 @@ enum {
 /* Arithmetic of a plan's transforms.
  *   DSHT_PREC_FP64  : FP64 CUDA-core per-bin sums and FP64 tables; agrees with the
  *                     reference's numpy path to about 1e-15 (tested at <= 1e-12 x max|alm|).
- *   DSHT_PREC_MIXED : tcgen05 tensor-core per-bin sums (operands quantised to 22-bit fixed
- *                     point, split into int8 slices, slice products accumulated exactly in
- *                     S32 and combined in FP64; unbiased, about 5.6e-8 rms per product) and a
+ *   DSHT_PREC_MIXED : per-bin sums by a type-1 non-uniform FFT in FP64 (each bin's points
+ *                     spread onto a periodic grid of 4 x 2^ceil(log2 Nl) cells with a width-12
+ *                     "exponential of semicircle" kernel, FFT, division by the kernel's Fourier
+ *                     transform; error about 5e-12 of the bin's sum of |w h_k|) -- or, with
+ *                     DSHT_TUNE_BIN_SUMS = DSHT_BIN_SUMS_TC, the direct tcgen05 tensor-core
+ *                     sums (operands quantised to 22-bit fixed point, split into int8 slices,
+ *                     slice products accumulated exactly in S32 and combined in FP64;
+ *                     unbiased, about 5.6e-8 rms per product) -- and a
  *                     tcgen05 tensor-core contraction of 4-byte fixed-point copies of the
  *                     tables (31-bit digits per row and per fold column, five exact S32
  *                     digit-pair classes; contraction error about 1e-9 x max|alm|), built on
  *                     first use; every table tile is read once for up to eight maps or point
  *                     sets of a multi-transform call.  Within 1e-7 x max|alm| of FP64,
- *                     concentrated point sets included.  The fixed-point scale of a bin
- *                     piece is its largest |weight|: weights spanning many decades lose
- *                     accuracy (lognormal sigma <= 1.5 stays within 1e-7), and so do weights
- *                     of both signs whose sums cancel (zero-mean normal weights: ~3e-7).
+ *                     concentrated point sets included.  With the tensor-core sums the
+ *                     fixed-point scale of a bin piece is its largest |weight|: weights
+ *                     spanning many decades lose accuracy (lognormal sigma <= 1.5 stays within
+ *                     1e-7), and so do weights of both signs whose sums cancel (zero-mean
+ *                     normal weights: ~3e-7); the NUFFT sums have neither limit.
  *                     Plans with Nx > 8192 (or without room for the digit tables beside the
  *                     FP64 pair) contract the FP64 tables instead.
- *   DSHT_PREC_MIXED_F64_TABLES : the same tensor-core sums with the FP64 tables streamed
- *                     by the CUDA-core contraction.
+ *   DSHT_PREC_MIXED_F64_TABLES : the same bin sums with the FP64 tables streamed by the
+ *                     CUDA-core contraction.
  * Mixed levels need Nl <= 2048; transforms of fewer than DSHT_MIXED_MIN_POINTS points run
  * the FP64 stages (they cost little, and the quantisation error of a handful of points
  * does not average down).  The rotation stays FP64 in all levels. */
@@ -99,13 +105,18 @@ int64_t dsht_mixed_min_points(void);
 int dsht_set_precision(dsht_plan_t plan, int precision);
 int dsht_get_precision(dsht_plan_t plan, int* precision);
 
-/* Launch-shape tuning of a plan (no counterpart in the reference; results do not depend on
- * it beyond rounding).  DSHT_TUNE_PIECE_MAX: points per bin piece of the per-bin sums, a
- * multiple of 32 in [256, 2048], 0 = chosen from N.  DSHT_TUNE_MAPS_PER_PASS: maps or point
- * sets that share one read of the tables in a multi-transform call, 1..8, 0 = the most
- * (8; the tensor-core contraction only: the FP64 one reads the tables once per map).  Workspace sizes depend on both:
- * query them after tuning. */
-enum { DSHT_TUNE_PIECE_MAX = 1, DSHT_TUNE_MAPS_PER_PASS = 2 };
+/* Tuning of a plan (no counterpart in the reference; results do not depend on it beyond
+ * the stated precision).  DSHT_TUNE_PIECE_MAX: points per bin piece of the per-bin sums, a
+ * multiple of 32 in [256, 65536], 0 = chosen from N and the method (the direct sums, FP64 and
+ * tensor-core, cap it at 2048; the NUFFT sums default to 8192).  DSHT_TUNE_MAPS_PER_PASS:
+ * maps or point sets that share one read of the tables in a multi-transform call, 1..8,
+ * 0 = the most (8; the tensor-core contraction only: the FP64 one reads the tables once per
+ * map).  DSHT_TUNE_BIN_SUMS: the bin sums of the mixed levels, DSHT_BIN_SUMS_NUFFT (the
+ * default, AUTO) or DSHT_BIN_SUMS_TC (the direct int8-slice tensor-core sums).  Workspace
+ * sizes depend on all three: query them after tuning. */
+enum { DSHT_TUNE_PIECE_MAX = 1, DSHT_TUNE_MAPS_PER_PASS = 2, DSHT_TUNE_BIN_SUMS = 3 };
+/* Values of DSHT_TUNE_BIN_SUMS: the bin-sum method of the mixed levels. */
+enum { DSHT_BIN_SUMS_AUTO = 0, DSHT_BIN_SUMS_NUFFT = 1, DSHT_BIN_SUMS_TC = 2 };
 int dsht_plan_tune(dsht_plan_t plan, int param, int value);
 int dsht_plan_get_tune(dsht_plan_t plan, int param, int* value);
 

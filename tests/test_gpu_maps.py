@@ -98,8 +98,9 @@ def test_maps_empty_and_polar_failure():
 
 
 def test_maps_per_pass_does_not_change_results():
-    """The mixed path's integer bin sums are exact (every bin here fits one piece), so the
-    grouping of maps into contraction passes leaves every map's alm bit for bit the same."""
+    """The bin sums of a map do not depend on the grouping of maps into contraction passes,
+    and the contraction's integer sums are exact, so every map's alm is bit for bit the
+    same for every grouping."""
     Nl, Nx, N = 96, 192, 60000
     rng, th, ph = _points(N, 31)
     W = rng.normal(1.0, 0.3, (5, N)).astype(np.float32)
@@ -129,10 +130,11 @@ def test_piece_size_tuning(piece):
 def test_tune_rejects_bad_values():
     from directsht_b200 import _lib as L
     d = DirectSHT(16, 32)
-    for param, value in ((L.DSHT_TUNE_PIECE_MAX, 100), (L.DSHT_TUNE_PIECE_MAX, 4096),
-                         (L.DSHT_TUNE_MAPS_PER_PASS, 9), (77, 1)):
+    for param, value in ((L.DSHT_TUNE_PIECE_MAX, 100), (L.DSHT_TUNE_PIECE_MAX, 70000),
+                         (L.DSHT_TUNE_PIECE_MAX, 4100), (L.DSHT_TUNE_MAPS_PER_PASS, 9),
+                         (L.DSHT_TUNE_BIN_SUMS, 3), (77, 1)):
         assert d._lib.dsht_plan_tune(d._plan, param, value) == L.DSHT_ERR_INVALID
-    assert d.tune() == {"piece_max": 0, "maps_per_pass": 0}
+    assert d.tune() == {"piece_max": 0, "maps_per_pass": 0, "bin_sums": "auto"}
 
 
 @pytest.mark.slow

@@ -1,5 +1,6 @@
-"""GPU tests of the mixed-precision path (tensor-core per-bin sums): results within
-1e-7 x max|alm| of the FP64 path, which the parity tests pin to the oracle."""
+"""GPU tests of the mixed-precision levels, with both bin-sum methods (the NUFFT sums, the
+default, and the direct tensor-core sums): results within 1e-7 x max|alm| of the FP64
+path, which the parity tests pin to the oracle."""
 import numpy as np
 import pytest
 
@@ -45,10 +46,12 @@ def test_mixed_matches_fp64(Nl, Nx, N, seed):
     w = rng.lognormal(0, 0.5, N)
     d = DirectSHT(Nl, Nx)
     ref = d(th, ph, w)
-    for level in ("mixed", "mixed_f64_tables"):
-        d.set_precision(level)
-        a = d(th, ph, w)
-        assert _rel(a, ref) <= TOL_MIXED, level
+    for bin_sums in ("nufft", "tc"):
+        d.tune(bin_sums=bin_sums)
+        for level in ("mixed", "mixed_f64_tables"):
+            d.set_precision(level)
+            a = d(th, ph, w)
+            assert _rel(a, ref) <= TOL_MIXED, (level, bin_sums)
 
 
 def test_small_transforms_use_fp64_sums():
@@ -70,9 +73,10 @@ def test_small_transforms_use_fp64_sums():
 def test_mixed_heavy_bin_and_wide_weights():
     """Many points in one bin (several pieces) and lognormal(0, 1) weights.
 
-    The fixed-point operands are scaled by the largest |weight| of each bin piece, so the
-    error of every point is relative to that largest weight; weight sets spanning many
-    more decades lose accuracy on the small weights (see DSHT_PREC_MIXED)."""
+    The tensor-core sums scale their fixed-point operands by the largest |weight| of each
+    bin piece, so the error of every point is relative to that largest weight; weight sets
+    spanning many more decades lose accuracy on the small weights (see DSHT_PREC_MIXED).
+    The NUFFT sums err relative to the bin's sum |w|."""
     rng = np.random.default_rng(9)
     N = 50000
     th = np.arccos(np.concatenate([rng.uniform(0.40, 0.401, N // 2), rng.uniform(-0.7, 0.7, N // 2)]))
@@ -82,10 +86,12 @@ def test_mixed_heavy_bin_and_wide_weights():
     ref = d.basic_sht(th, ph, w.copy(), verbose=False)
     # Half of the weight sits in one bin: the digit tables' fixed point is relative to each
     # row's and fold column's scale, so both levels hold 1e-7.
-    for level in ("mixed_f64_tables", "mixed"):
-        d.set_precision(level)
-        a = d.basic_sht(th, ph, w.copy(), verbose=False)
-        assert _rel(a, ref) <= TOL_MIXED, level
+    for bin_sums in ("nufft", "tc"):
+        d.tune(bin_sums=bin_sums)
+        for level in ("mixed_f64_tables", "mixed"):
+            d.set_precision(level)
+            a = d.basic_sht(th, ph, w.copy(), verbose=False)
+            assert _rel(a, ref) <= TOL_MIXED, (level, bin_sums)
 
 
 def _oracle_basic(Nl, Nx, th, ph, w):
@@ -119,8 +125,10 @@ def test_mixed_concentrated_weight_vs_oracle(case):
     ref = _oracle_basic(Nl, Nx, th, ph, w)
     for kwargs in (dict(precision="mixed"), dict(compact_tables=True)):
         d = DirectSHT(Nl, Nx, **kwargs)
-        a = d.basic_sht(th, ph, w.copy(), verbose=False)
-        assert _rel(a, ref) <= TOL_MIXED, (case, kwargs)
+        for bin_sums in ("nufft", "tc"):
+            d.tune(bin_sums=bin_sums)
+            a = d.basic_sht(th, ph, w.copy(), verbose=False)
+            assert _rel(a, ref) <= TOL_MIXED, (case, kwargs, bin_sums)
 
 
 @pytest.mark.parametrize("N,seed", [(1, 0), (700, 1), (5000, 2)])
@@ -168,5 +176,7 @@ def test_mixed_c2_full_size():
     d = DirectSHT(1024, 2048)
     ref = d(th, ph, w)
     d.set_precision("mixed")
-    a = d(th, ph, w)
-    assert _rel(a, ref) <= TOL_MIXED
+    for bin_sums in ("nufft", "tc"):
+        d.tune(bin_sums=bin_sums)
+        a = d(th, ph, w)
+        assert _rel(a, ref) <= TOL_MIXED, bin_sums

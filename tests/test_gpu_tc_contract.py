@@ -51,9 +51,8 @@ def test_signed_zero_mean_weights():
     """Weights of both signs summing to about zero, so that max|alm| is far below sum|w| and
     the fold columns' scales (bounds from sum |w| per node) are loose.  The contraction
     alone (FP64 bin sums below 1024 points) stays within 1e-9 of the oracle, and with the
-    tensor-core bin sums it differs from the FP64-table contraction of the same bin sums by
-    less than 1e-8.  (The tensor-core bin sums themselves quantise relative to each piece's
-    largest |w|, so zero-mean weights lose about max|w| / rms|w| of their 1e-7 budget.)"""
+    NUFFT bin sums it differs from the FP64-table contraction of the same bin sums by less
+    than 1e-8."""
     Nl, Nx = 128, 256
     th, ph, w = _full_sky(900, 3, wkind="normal")
     ref = O.direct_sht(O.build_tables(Nl, Nx), th, ph, w)
