@@ -104,6 +104,7 @@ size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* ba
   const size_t fdig_bytes = (size_t)g.Nl * 8 * 4 * w.tc_maps * (size_t)digit_kp(g.Nx);
   w.fold = reinterpret_cast<double*>(take(std::max(fold_bytes, fdig_bytes)));
   w.cexp = reinterpret_cast<int16_t*>(take(sizeof(int16_t) * 2 * w.tc_maps));
+  w.cmax = reinterpret_cast<unsigned long long*>(take(sizeof(unsigned long long) * 2 * w.tc_maps));
   w.tile_live = reinterpret_cast<uint8_t*>(take(2 * (size_t)ntile));
   w.tile_live2 = reinterpret_cast<uint8_t*>(take(2 * (size_t)((g.Nx + 255) / 256)));
   w.alm_equ = reinterpret_cast<double*>(take(sizeof(double) * 2 * (size_t)g.Nlm));
@@ -247,8 +248,8 @@ int run_after_sort(dsht_plan_s* p, int64_t N, int mode, double* alm, const Works
   if (rt.digits) {
     mark(DSHT_STAGE_FOLD);
     uint8_t* fdig = reinterpret_cast<uint8_t*>(ws.fold);
-    launch_fold_scale(g, w2, ws.cexp, s);
-    launch_fold_digits(g, w2, ws.cexp, 0, 4, fdig, s);
+    launch_fold_scale(g, w2, ws.cmax, s);
+    launch_fold_digits(g, w2, ws.cmax, ws.cexp, 0, 4, fdig, s);
     mark(DSHT_STAGE_CONTRACT);
     TcOut out{};
     out.equ[0] = ws.alm_equ;
@@ -325,8 +326,8 @@ static int run_class_digits(dsht_plan_s* p, const Item* items, const std::vector
       w2.partial_f32 = 0;
     }
     prof_mark(p, DSHT_STAGE_FOLD, s);
-    launch_fold_scale(g, w2, ws.cexp + 2 * slot, s);
-    launch_fold_digits(g, w2, ws.cexp + 2 * slot, slot, fcols, fdig, s);
+    launch_fold_scale(g, w2, ws.cmax + 2 * slot, s);
+    launch_fold_digits(g, w2, ws.cmax + 2 * slot, ws.cexp + 2 * slot, slot, fcols, fdig, s);
     pass.push_back(i);
     if ((int)pass.size() < G && li + 1 < list.size()) continue;
     TcOut out{};

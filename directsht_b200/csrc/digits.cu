@@ -134,16 +134,20 @@ __global__ void table_decode_kernel(int Nl, int Nx, int Kp, double dx, int which
   }
 }
 
-// Per-map fold scales: exponent of the largest |w| sum feeding a node of each half (the
-// node sums as heavy_select_kernel forms them), which bounds |A| and |B/dx| for every m.
-constexpr int kScaleThreads = 1024;
-__global__ void __launch_bounds__(kScaleThreads)
+// Per-map fold scales: the largest |w| sum feeding a node of each half (bins j - 1 and j of
+// both sets of the half), which bounds |A| and |B/dx| for every m.
+__global__ void __launch_bounds__(256)
 fold_scale_kernel(int nbins, int Nx, const int* __restrict__ piece_first, const double* __restrict__ wsum,
-                  int16_t* __restrict__ cexp) {
-  __shared__ double red[2][32];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  double mx[2] = {0.0, 0.0};
-  for (int e = warp; e < 2 * Nx; e += blockDim.x >> 5) {
+                  unsigned long long* __restrict__ cmax) {
+  // one warp per node entry e = (half h, node j): the sum of |w| over the pieces of bins
+  // j - 1 and j of both sets of the half; the largest per half goes to cmax[h] as the bits
+  // of a non-negative double (which order like the values)
+  __shared__ unsigned long long red[2];
+  const int lane = threadIdx.x & 31;
+  if (threadIdx.x < 2) red[threadIdx.x] = 0ull;
+  __syncthreads();
+  const int e = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (e < 2 * Nx) {
     const int h = e / Nx, j = e - h * Nx;
     double s = 0.0;
     for (int sset = 2 * h; sset < 2 * h + 2; ++sset)
@@ -154,22 +158,10 @@ fold_scale_kernel(int nbins, int Nx, const int* __restrict__ piece_first, const 
       }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    mx[h] = fmax(mx[h], s);
-  }
-  if (lane == 0) {
-    red[0][warp] = mx[0];
-    red[1][warp] = mx[1];
+    if (lane == 0 && s > 0.0) atomicMax(&red[h], (unsigned long long)__double_as_longlong(s));
   }
   __syncthreads();
-  if (warp == 0) {
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      double v = lane < (int)(blockDim.x >> 5) ? red[h][lane] : 0.0;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-      if (lane == 0) cexp[h] = (int16_t)scale_exp(v);
-    }
-  }
+  if (threadIdx.x < 2 && red[threadIdx.x]) atomicMax(&cmax[threadIdx.x], red[threadIdx.x]);
 }
 
 // Fold of one map straight into digits.  A block covers 32 m x 32 nodes: warp = node,
@@ -182,15 +174,21 @@ fold_scale_kernel(int nbins, int Nx, const int* __restrict__ piece_first, const 
 template <typename PT>
 __global__ void __launch_bounds__(1024)
 fold_digits_kernel(int Nl, int Nx, int nbins, int Kp, const int* __restrict__ piece_first,
-                   const PT* __restrict__ partial, const int16_t* __restrict__ cexp, int map, int ncols,
-                   uint8_t* __restrict__ fdig) {
+                   const PT* __restrict__ partial, const unsigned long long* __restrict__ cmax,
+                   int16_t* __restrict__ cexp, int map, int ncols, uint8_t* __restrict__ fdig) {
   // stage[row][36], row = (((par * 4 + d) * 4 + c) * 2 + kh) * 32 + m, byte j of the row
   // = node j0 + j (dynamic: 72 KB)
   extern __shared__ __align__(16) uint8_t stage[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int m0 = blockIdx.y * 32, j0 = blockIdx.x * 32;
   const int m = m0 + lane, j = j0 + warp;
-  const int sh0 = 31 - cexp[0], sh1 = 31 - cexp[1];
+  const int e0 = scale_exp(__longlong_as_double((long long)cmax[0]));
+  const int e1 = scale_exp(__longlong_as_double((long long)cmax[1]));
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {  // the column scales of the contraction
+    cexp[0] = (int16_t)e0;
+    cexp[1] = (int16_t)e1;
+  }
+  const int sh0 = 31 - e0, sh1 = 31 - e1;
   double A[4][2], Bv[4][2];
 #pragma unroll
   for (int s = 0; s < 4; ++s) {
@@ -300,13 +298,15 @@ void launch_table_decode(const Geometry& g, int which, int64_t r0, int64_t n, co
   count_launches(1);
 }
 
-void launch_fold_scale(const Geometry& g, const Workspace& ws, int16_t* cexp, cudaStream_t s) {
-  fold_scale_kernel<<<1, kScaleThreads, 0, s>>>(g.nbins, g.Nx, ws.piece_first, ws.wsum, cexp);
+void launch_fold_scale(const Geometry& g, const Workspace& ws, unsigned long long* cmax, cudaStream_t s) {
+  cudaMemsetAsync(cmax, 0, 2 * sizeof(unsigned long long), s);
+  const int blocks = (2 * g.Nx + 7) / 8;
+  fold_scale_kernel<<<blocks, 256, 0, s>>>(g.nbins, g.Nx, ws.piece_first, ws.wsum, cmax);
   count_launches(1);
 }
 
-void launch_fold_digits(const Geometry& g, const Workspace& ws, const int16_t* cexp, int map, int ncols,
-                        uint8_t* fdig, cudaStream_t s) {
+void launch_fold_digits(const Geometry& g, const Workspace& ws, const unsigned long long* cmax, int16_t* cexp,
+                        int map, int ncols, uint8_t* fdig, cudaStream_t s) {
   const int Kp = digit_kp(g.Nx);
   dim3 grid((g.Nx + 31) / 32, (g.Nl + 31) / 32);
   constexpr int kStageBytes = 32 * 2 * 4 * 4 * 2 * kStageRow;
@@ -314,10 +314,11 @@ void launch_fold_digits(const Geometry& g, const Workspace& ws, const int16_t* c
   cudaFuncSetAttribute(fold_digits_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStageBytes);
   if (ws.partial_f32)
     fold_digits_kernel<float><<<grid, 1024, kStageBytes, s>>>(g.Nl, g.Nx, g.nbins, Kp, ws.piece_first,
-                                                    reinterpret_cast<const float*>(ws.partial), cexp, map, ncols, fdig);
+                                                              reinterpret_cast<const float*>(ws.partial), cmax,
+                                                              cexp, map, ncols, fdig);
   else
-    fold_digits_kernel<double><<<grid, 1024, kStageBytes, s>>>(g.Nl, g.Nx, g.nbins, Kp, ws.piece_first, ws.partial, cexp, map,
-                                                     ncols, fdig);
+    fold_digits_kernel<double><<<grid, 1024, kStageBytes, s>>>(g.Nl, g.Nx, g.nbins, Kp, ws.piece_first,
+                                                               ws.partial, cmax, cexp, map, ncols, fdig);
   count_launches(1);
 }
 

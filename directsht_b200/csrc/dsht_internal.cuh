@@ -86,6 +86,7 @@ struct Workspace {
   double* fold;         // [Nl][4][Nx][4] FP64 fold; the tensor-core route's fold digits
                         // [Nl][2][4][4 tc_maps][Kp] (int8) share this region
   int16_t* cexp;        // [tc_maps][2] fold column scale exponents (tensor-core route)
+  unsigned long long* cmax;  // [tc_maps][2] largest node |w| sum per half (bits of a double)
   int tc_maps;          // maps one tensor-core contraction pass can hold
   uint8_t* tile_live;   // [2][ceil(Nx/128)] tiles of the fallback contraction
   uint8_t* tile_live2;  // [2][ceil(Nx/256)] tiles of the streaming contraction
@@ -143,8 +144,9 @@ void launch_table_digits(const Geometry& g, int64_t row0, int64_t nrows, const d
                          const int16_t* rexp, uint8_t* dig, cudaStream_t s);
 void launch_table_decode(const Geometry& g, int which, int64_t r0, int64_t n, const uint8_t* dig,
                          const int16_t* rexp, double* out, cudaStream_t s);
-void launch_fold_scale(const Geometry& g, const Workspace& ws, int16_t* cexp, cudaStream_t s);
-void launch_fold_digits(const Geometry& g, const Workspace& ws, const int16_t* cexp, int map, int ncols,
+void launch_fold_scale(const Geometry& g, const Workspace& ws, unsigned long long* cmax, cudaStream_t s);
+void launch_fold_digits(const Geometry& g, const Workspace& ws, const unsigned long long* cmax, int16_t* cexp,
+                        int map, int ncols,
                         uint8_t* fdig, cudaStream_t s);
 int make_table_digit_tmap(CUtensorMap* tm, const uint8_t* dig, int Nx, int64_t Nlm);
 std::vector<uint32_t> tc_items(int Nl);
