@@ -283,7 +283,7 @@ int run_pipeline(dsht_plan_s* p, const double* theta, const double* phi, const d
                         int mode, double* alm, const Workspace& ws, cudaStream_t s) {
   p->ev_n = 0;
   prof_mark(p, DSHT_STAGE_POINTS, s);
-  launch_points(p->g, theta, phi, w, 0, N, mode, ws, s);
+  launch_points(p->g, theta, phi, w, 0, N, mode, ws, s, plan_route(p, N).tc && plan_uses_nufft(p));
   prof_mark(p, DSHT_STAGE_BIN_SUMS, s);
   return run_after_sort(p, N, mode, alm, ws, s, true);
 }
@@ -313,7 +313,8 @@ static int run_class_digits(dsht_plan_s* p, const Item* items, const std::vector
       prof_mark(p, DSHT_STAGE_POINTS, s);
       Workspace wp = ws;
       if (!(li + 1 < list.size() && items[list[li + 1]].same_points)) wp.sidx = nullptr;
-      launch_points(g, item.theta, item.phi, item.w, item.w_f32, item.N, mode, wp, s);
+      launch_points(g, item.theta, item.phi, item.w, item.w_f32, item.N, mode, wp, s,
+                    rt.tc && plan_uses_nufft(p));
       *sorted_item = i;
     }
     prof_mark(p, DSHT_STAGE_BIN_SUMS, s);
@@ -416,7 +417,8 @@ int run_items(dsht_plan_s* p, const Item* items, int n, int mode, const Workspac
         // The sort keeps the input index of every slot when later items share it.
         Workspace wp = ws;
         if (!(li + 1 < list.size() && items[list[li + 1]].same_points)) wp.sidx = nullptr;
-        launch_points(g, item.theta, item.phi, item.w, item.w_f32, item.N, mode, wp, s);
+        launch_points(g, item.theta, item.phi, item.w, item.w_f32, item.N, mode, wp, s,
+                      mixed && plan_uses_nufft(p));
         sorted_item = i;
       }
       prof_mark(p, DSHT_STAGE_BIN_SUMS, s);

@@ -118,7 +118,8 @@ Route plan_route(const dsht_plan_s* p, int64_t N);
 // Kernels launched by api.cu (each file owns its launch helpers).
 void launch_tables(const Geometry& g, double* Yv, double* Yd, cudaStream_t s);
 void launch_points(const Geometry& g, const double* theta, const double* phi, const void* w, int w_f32,
-                   int64_t N, int mode, const Workspace& ws, cudaStream_t s);
+                   int64_t N, int mode, const Workspace& ws, cudaStream_t s,
+                   bool phi_record = false);
 void launch_gather(const Geometry& g, const void* w, int w_f32, int64_t N, const Workspace& ws, cudaStream_t s);
 // Largest |w h_k| of every piece of the sorted records (needed by the tensor-core sums).
 void launch_piece_maxima(const Workspace& ws, cudaStream_t s);

@@ -220,7 +220,6 @@ nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* _
   const int n = 1 << logn;
   const int seq_stride = n + (n >> 4);
   const double u_per_rad = (double)n * 0.15915494309189533577;  // n / (2 pi)
-  const double two_pi = 6.28318530717958647693;
   const int npieces = (int)min((int64_t)*npieces_p, pmax);
   for (int piece = blockIdx.x; piece < npieces; piece += gridDim.x) {
     const int64_t start = piece_start[piece];
@@ -245,9 +244,8 @@ nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* _
       unsigned long long* zi = reinterpret_cast<unsigned long long*>(zs);
       for (int p = threadIdx.x; p < len; p += blockDim.x) {
         const double2* rec = reinterpret_cast<const double2*>(pay + (size_t)kRec * (start + p));
-        const double2 r0 = rec[0], r1 = rec[1];  // (cos phi, sin phi), (w, t)
-        double phi = atan2(r0.y, r0.x);
-        if (phi < 0.0) phi += two_pi;
+        const double phi = rec[0].x;  // in [0, 2 pi): the sort's azimuth record
+        const double2 r1 = rec[1];     // (w, t)
         const double u = phi * u_per_rad;
         const double fl = floor(u);
         const double sv = 2.0 * (u - fl) - 1.0;

@@ -11,7 +11,8 @@
 // exclusive scan cuts every key into pieces of at most piece_max points; the scatter pass
 // reserves a contiguous range per key and block with one global add, recomputes each
 // point's 32-byte record (cos phi, sin phi, w, t) -- one DRAM sector -- from its inputs and
-// writes it to its sorted slot; the bin-sum kernels form w h_k(t) themselves.  HBM bytes
+// writes it to its sorted slot; the bin-sum kernels form w h_k(t) themselves (the NUFFT bin
+// sums take the record (phi, 0, w, t) instead).  HBM bytes
 // per point: 12-16 read + 4 written (count), 28 read + 32 written (scatter), against the
 // algorithmic 24 read + 32 written.
 #include "dsht_internal.cuh"
@@ -277,7 +278,10 @@ __device__ __forceinline__ uint32_t gmax_bits(const double* h) {
 // to its sorted slot.  The record is recomputed from theta, phi, w and the key of the count
 // pass: for a rotated polar point the azimuth of (c, s sin p, -s cos p), kept as its cosine
 // and sine (c / rho, s sin p / rho), and t = (|x| - x_j) / dx (sht/sht.py:221).
-template <typename WT>
+// PHI: the record holds (phi, 0, w, t) instead -- the azimuth itself (of the rotated point
+// for polar points, in [0, 2 pi)), which is what the NUFFT bin sums spread by; equatorial
+// points then need no sine or cosine of phi at all.
+template <typename WT, bool PHI>
 __global__ void __launch_bounds__(kPointThreads)
 scatter_kernel(Geometry g, const double* __restrict__ theta, const double* __restrict__ phi,
                const WT* __restrict__ w, int64_t N, const uint32_t* __restrict__ keys, uint32_t* __restrict__ cursor,
@@ -326,18 +330,34 @@ scatter_kernel(Geometry g, const double* __restrict__ theta, const double* __res
       if (k[u] == DSHT_KEY_DROP) continue;
       double st, c, sp, cp;
       sincos(th[u], &st, &c);
-      sincos(ph[u], &sp, &cp);
-      double cphi = cp, sphi = sp, x = c;
-      if ((int)k[u] >= polar_key0) {
-        x = -__dmul_rn(st, cp);
-        const double ny = st * sp;
-        const double rho = sqrt(ny * ny + c * c);
-        cphi = 1.0;
+      double cphi, sphi, x = c;
+      if constexpr (PHI) {
+        constexpr double two_pi = 6.28318530717958647693;
         sphi = 0.0;
-        if (rho > 0.0) {
-          const double ir = 1.0 / rho;
-          cphi = c * ir;
-          sphi = ny * ir;
+        if ((int)k[u] >= polar_key0) {
+          sincos(ph[u], &sp, &cp);
+          x = -__dmul_rn(st, cp);
+          cphi = atan2(st * sp, c);  // azimuth of the rotated point (c, s sin p, -s cos p)
+        } else {
+          cphi = ph[u];
+          if (!(cphi >= 0.0 && cphi < two_pi)) cphi -= two_pi * floor(cphi / two_pi);
+        }
+        if (cphi < 0.0) cphi += two_pi;
+      } else {
+        sincos(ph[u], &sp, &cp);
+        cphi = cp;
+        sphi = sp;
+        if ((int)k[u] >= polar_key0) {
+          x = -__dmul_rn(st, cp);
+          const double ny = st * sp;
+          const double rho = sqrt(ny * ny + c * c);
+          cphi = 1.0;
+          sphi = 0.0;
+          if (rho > 0.0) {
+            const double ir = 1.0 / rho;
+            cphi = c * ir;
+            sphi = ny * ir;
+          }
         }
       }
       const int j = (int)(k[u] % (uint32_t)g.nbins);
@@ -422,7 +442,7 @@ __global__ void publish_flags_kernel(const StatusOut st, int n, unsigned* all) {
 }  // namespace
 
 void launch_points(const Geometry& g, const double* theta, const double* phi, const void* w, int w_f32,
-                   int64_t N, int mode, const Workspace& ws, cudaStream_t s) {
+                   int64_t N, int mode, const Workspace& ws, cudaStream_t s, bool phi_record) {
   cudaMemsetAsync(ws.count, 0, sizeof(uint32_t) * (g.nkeys + 1), s);
   cudaMemsetAsync(ws.flags, 0, sizeof(unsigned), s);
   const size_t hsmem = sizeof(uint32_t) * g.nkeys;
@@ -449,8 +469,13 @@ void launch_points(const Geometry& g, const double* theta, const double* phi, co
       kern<<<(unsigned)blocks, kPointThreads, hsmem, s>>>(g, theta, phi, wp, N, ws.key, ws.cursor, ws.pay,
                                                           ws.sidx);
     };
-    if (w_f32) go(scatter_kernel<float>, reinterpret_cast<const float*>(w));
-    else go(scatter_kernel<double>, reinterpret_cast<const double*>(w));
+    if (phi_record) {
+      if (w_f32) go(scatter_kernel<float, true>, reinterpret_cast<const float*>(w));
+      else go(scatter_kernel<double, true>, reinterpret_cast<const double*>(w));
+    } else {
+      if (w_f32) go(scatter_kernel<float, false>, reinterpret_cast<const float*>(w));
+      else go(scatter_kernel<double, false>, reinterpret_cast<const double*>(w));
+    }
     count_launches(1);
   }
 }
