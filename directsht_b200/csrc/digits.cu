@@ -41,6 +41,13 @@ __device__ __forceinline__ uint32_t digit_word(double v, int sh) {
   return (uint32_t)((int)X + 0x808080) ^ 0x808080u;
 }
 
+// The same for v 2^sh given as the product (|v 2^sh| < 2^31): one DADD puts it into the
+// binade of 1.5 2^52, whose low word is then the rounded integer.
+__device__ __forceinline__ uint32_t digit_word_scaled(double vs) {
+  const int X = __double2loint(vs + 6755399441055744.0);
+  return (uint32_t)(X + 0x808080) ^ 0x808080u;
+}
+
 // Grouped row of Healpy row (l, m).
 __device__ __forceinline__ int64_t grouped_row(int l, int m, int Nl) {
   const int64_t base = hp_index(m, m, Nl);
@@ -188,56 +195,67 @@ fold_digits_kernel(int Nl, int Nx, int nbins, int Kp, const int* __restrict__ pi
     cexp[0] = (int16_t)e0;
     cexp[1] = (int16_t)e1;
   }
-  const int sh0 = 31 - e0, sh1 = 31 - e1;
-  double A[4][2], Bv[4][2];
+  // 2^(31 - e): the fixed-point factor of each half (exact products)
+  const double f0 = ldexp(1.0, 31 - e0), f1 = ldexp(1.0, 31 - e1);
+  // Per half h (sets 2h, 2h+1): the piece ranges of the four keys feeding node j -- bin j
+  // (rows 0-3 of its pieces) and bin j - 1 (rows 4-7) of each set.  The first piece of
+  // every key is read before any further ones, so 16 loads are in flight together (most
+  // bins are one piece).  acc[set][A re, A im, B re, B im] with V = vr - i vi.
 #pragma unroll
-  for (int s = 0; s < 4; ++s) {
-    double ar = 0.0, ai = 0.0, br = 0.0, bi = 0.0;
-    if (m < Nl && j < Nx) {
-      if (j < nbins) {
-        const int key = s * nbins + j;
-        for (int p = piece_first[key]; p < piece_first[key + 1]; ++p) {
-          const PT* v = partial + (size_t)p * 8 * Nl + m;
-          ar += v[0];
-          ai -= v[(size_t)Nl];
-          br += v[(size_t)2 * Nl];
-          bi -= v[(size_t)3 * Nl];
-        }
+  for (int h = 0; h < 2; ++h) {
+    int pa[2][2], pb[2][2];
+#pragma unroll
+    for (int si = 0; si < 2; ++si)
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        const bool ok = m < Nl && j < Nx && (b ? j >= 1 : j < nbins);
+        const int key = (2 * h + si) * nbins + j - b;
+        pa[si][b] = ok ? piece_first[key] : 0;
+        pb[si][b] = ok ? piece_first[key + 1] : 0;
       }
-      if (j >= 1) {
-        const int key = s * nbins + j - 1;
-        for (int p = piece_first[key]; p < piece_first[key + 1]; ++p) {
-          const PT* v = partial + (size_t)p * 8 * Nl + m;
-          ar += v[(size_t)4 * Nl];
-          ai -= v[(size_t)5 * Nl];
-          br += v[(size_t)6 * Nl];
-          bi -= v[(size_t)7 * Nl];
+    double acc[2][4];
+#pragma unroll
+    for (int si = 0; si < 2; ++si) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[si][q] = 0.0;
+#pragma unroll
+      for (int b = 0; b < 2; ++b)
+        if (pa[si][b] < pb[si][b]) {
+          const PT* v = partial + (size_t)pa[si][b] * 8 * Nl + (size_t)(4 * b) * Nl + m;
+          acc[si][0] += v[0];
+          acc[si][1] -= v[(size_t)Nl];
+          acc[si][2] += v[(size_t)2 * Nl];
+          acc[si][3] -= v[(size_t)3 * Nl];
         }
-      }
     }
-    A[s][0] = ar;
-    A[s][1] = ai;
-    Bv[s][0] = br;
-    Bv[s][1] = bi;
-  }
-  // values[par][h][ri][kh]: kh = 0 the A entry, 1 the B/dx entry
 #pragma unroll
-  for (int par = 0; par < 2; ++par)
+    for (int si = 0; si < 2; ++si)
 #pragma unroll
-    for (int h = 0; h < 2; ++h)
+      for (int b = 0; b < 2; ++b)
+        for (int p = pa[si][b] + 1; p < pb[si][b]; ++p) {
+          const PT* v = partial + (size_t)p * 8 * Nl + (size_t)(4 * b) * Nl + m;
+          acc[si][0] += v[0];
+          acc[si][1] -= v[(size_t)Nl];
+          acc[si][2] += v[(size_t)2 * Nl];
+          acc[si][3] -= v[(size_t)3 * Nl];
+        }
+    const double fh = h ? f1 : f0;
+    // entries (par, ri, kh): kh = 0 the A entry, 1 the B/dx entry; even rows A+ + A-, odd A+ - A-
+#pragma unroll
+    for (int par = 0; par < 2; ++par)
 #pragma unroll
       for (int ri = 0; ri < 2; ++ri)
 #pragma unroll
         for (int kh = 0; kh < 2; ++kh) {
-          const double (*X)[2] = kh ? Bv : A;
-          const double v = par ? X[2 * h][ri] - X[2 * h + 1][ri] : X[2 * h][ri] + X[2 * h + 1][ri];
-          const uint32_t w = digit_word(v, h ? sh1 : sh0);
+          const double a = acc[0][2 * kh + ri], b = acc[1][2 * kh + ri];
+          const uint32_t w = digit_word_scaled((par ? a - b : a + b) * fh);
           const int c = 2 * h + ri;
 #pragma unroll
           for (int d = 0; d < 4; ++d)
             stage[(((((par * 4 + d) * 4 + c) * 2 + kh) * 32) + lane) * kStageRow + warp] =
                 (uint8_t)(w >> (8 * (3 - d)));
         }
+  }
   __syncthreads();
   // 2048 rows x 8 words; word w covers 4 nodes of one (par, d, c, kh, m) row.
   const int nj = min(32, Nx - j0);
