@@ -216,7 +216,7 @@ nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* _
                   double* __restrict__ partial, double* __restrict__ wsum) {
   constexpr int NSEQ = KP / 2;
   extern __shared__ double2 zs[];  // [NSEQ][n + n/16]
-  __shared__ double red[kNuThreads / 32];
+  __shared__ unsigned long long red[2];
   const int n = 1 << logn;
   const int seq_stride = n + (n >> 4);
   const double u_per_rad = (double)n * 0.15915494309189533577;  // n / (2 pi)
@@ -224,20 +224,40 @@ nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* _
   for (int piece = blockIdx.x; piece < npieces; piece += gridDim.x) {
     const int64_t start = piece_start[piece];
     const int len = piece_len[piece];
-    // sum |w| of the piece: bounds every grid value (|h_k| <= 1, psi <= 1), so the spread
-    // runs in 64-bit fixed point of step 2^-50 sum|w| -- integer atomics, so the grid (and
-    // every result) does not depend on the order of the adds
-    double wabs = 0.0;
-    for (int p = threadIdx.x; p < len; p += blockDim.x) wabs += fabs(pay[(size_t)kRec * (start + p) + 2]);
+    // A bound of sum |w| over the piece that does not depend on the order of its points (the
+    // sort places the points of a key in any order): M = max |w|, then the exact integer
+    // sum of rint(|w| 2^40 / M).  It bounds every grid value (|h_k| <= 1, psi <= 1), so the
+    // spread runs in 64-bit fixed point of step 2^(e - 50), 2^e >= the bound -- integer
+    // atomics, so the grid (and every result) does not depend on the order of the adds.
+    unsigned long long mbits = 0ull;
+    for (int p = threadIdx.x; p < len; p += blockDim.x)
+      mbits = max(mbits, (unsigned long long)__double_as_longlong(fabs(pay[(size_t)kRec * (start + p) + 2])));
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) wabs += __shfl_xor_sync(0xffffffffu, wabs, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = wabs;
+    for (int o = 16; o > 0; o >>= 1) mbits = max(mbits, __shfl_xor_sync(0xffffffffu, mbits, o));
+    if (threadIdx.x == 0) red[0] = 0ull;
     __syncthreads();
-    wabs = 0.0;
-    for (int i = 0; i < kNuThreads / 32; ++i) wabs += red[i];
-    if (threadIdx.x == 0) wsum[piece] = wabs;
-    const double fx_scale = wabs > 0.0 ? 0x1p50 / wabs : 1.0;
-    const double fx_step = wabs > 0.0 ? wabs * 0x1p-50 : 1.0;
+    if ((threadIdx.x & 31) == 0) atomicMax(&red[0], mbits);
+    __syncthreads();
+    const double wmax = __longlong_as_double((long long)red[0]);
+    const double to_int = wmax > 0.0 ? 0x1p40 / wmax : 0.0;
+    unsigned long long isum = 0ull;
+    for (int p = threadIdx.x; p < len; p += blockDim.x)
+      isum += fixed_point(fabs(pay[(size_t)kRec * (start + p) + 2]) * to_int);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) isum += __shfl_xor_sync(0xffffffffu, isum, o);
+    if (threadIdx.x == 0) red[1] = 0ull;
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) atomicAdd(&red[1], isum);
+    __syncthreads();
+    // each rounding is at most 1/2: (isum + len) 2^-40 M >= sum |w|
+    const double wbound = wmax > 0.0 ? (double)(red[1] + (unsigned long long)len) * (wmax * 0x1p-40) : 0.0;
+    if (threadIdx.x == 0) wsum[piece] = wbound;
+    int ebound = 0;
+    if (wbound > 0.0) frexp(wbound, &ebound);  // wbound < 2^ebound
+    // a NaN or infinite weight makes every sum of the piece NaN, as the direct sums would
+    const double fx_step = red[0] >= 0x7ff0000000000000ull ? __longlong_as_double(0x7ff8000000000000ll)
+                                                             : ldexp(1.0, ebound - 50);
+    const double fx_scale = ldexp(1.0, 50 - ebound);
     for (int kp = 0; kp < 4; kp += KP) {
       for (int i = threadIdx.x; i < NSEQ * seq_stride; i += blockDim.x) zs[i] = make_double2(0.0, 0.0);
       __syncthreads();
