@@ -18,17 +18,20 @@
 // converted to monomials on the host; max error 1e-13 of psi(0)).  They are passed as a
 // kernel parameter, so every Horner step is one DFMA with a uniform operand.
 //
-// One CTA per piece (persistent over pieces): zero the padded grids in shared memory,
-// spread every point of the piece (64-bit fixed point of step 2^-50 of the piece's sum |w|,
-// shared-memory integer atomics: 4 x W per point, so the sums are exact and do not depend
-// on the order of the adds), convert to FP64, an in-place decimation-in-frequency FFT (radix-16 passes and one radix-2/4/8 pass, the
-// 16-point DFTs in registers), then each thread reads the outputs of its m from their
-// digit-reversed positions, divides by Psi(m) and writes the piece's partial sums
-// [8][Nl] (FP64, k-major, re | im).  The grid index i is stored at i + i/16 (one 16-byte
-// pad per 16 entries) so that the last pass's unit-stride butterflies hit distinct banks.
-// FP64 throughout; no tensor cores: per point about 130 DFMA for the kernel values and 96
-// for the spread, per piece 2 x 5 n log2 n for the FFTs -- against 24 x Nl flop per point
-// for the direct sums.
+// One CTA per piece (persistent over pieces): an order-independent bound of the piece's
+// sum |w| sets a fixed-point step; the piece's points are bucketed by 16-cell group (a
+// counting sort in shared memory) and spread in that order as 46-bit fixed-point values,
+// each added as two native 32-bit shared-memory reductions (low 16 bits, high bits), so the
+// sums are exact, independent of the order of the adds, and a warp's adds land on
+// neighbouring cells; the planes are converted to FP64 in place, then an in-place
+// decimation-in-frequency FFT (radix-16 passes and one radix-2/4/8 pass, the 16-point DFTs
+// in registers, twiddles staged in shared memory), then each thread reads the outputs of
+// its m from their digit-reversed positions, divides by Psi(m) and writes the piece's
+// partial sums [8][Nl] (FP64, k-major, re | im).  The grid index i is stored at i + i/16
+// (one 16-byte pad per 16 entries) so that the last pass's unit-stride butterflies hit
+// distinct banks.  FP64 throughout; no tensor cores: per point about 130 DFMA for the
+// kernel values and 96 reductions for the spread, per piece 2 x 5 n log2 n for the FFTs --
+// against 24 x Nl flop per point for the direct sums.
 #include <cmath>
 #include <mutex>
 #include <vector>
@@ -207,7 +210,60 @@ __device__ void fft_all(double2* zs, int seq_stride, int logn, const double2* __
   __syncthreads();
 }
 
+constexpr int kSortChunk = 8192;  // points bucketed at a time (order indices are 16-bit)
+constexpr int kMaxGroups = 512;   // 16-cell groups of the largest grid (n = 8192)
+constexpr int kMaxNl = 2048;
+
+// Shared-memory bytes of a launch: the grids, then the bucket order, bucket offsets,
+// twiddles e^{2 pi i j/n} (j < n/16) and 1/Psi(m).
+size_t nufft_smem_bytes(int logn, int nseq) {
+  const size_t n = (size_t)1 << logn;
+  return 16 * nseq * (n + n / 16) + 2 * kSortChunk + 4 * kMaxGroups + 16 * kMaxGroups + 8 * kMaxNl;
+}
+
+// Exclusive prefix sum over the block (every thread passes one value).
+__device__ __forceinline__ unsigned block_excl_scan(unsigned v, unsigned* wsc) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsc[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    const unsigned t = lane < (int)(blockDim.x >> 5) ? wsc[lane] : 0u;
+    unsigned sc = t;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned y = __shfl_up_sync(0xffffffffu, sc, o);
+      if (lane >= o) sc += y;
+    }
+    if (lane < (int)(blockDim.x >> 5)) wsc[lane] = sc - t;
+  }
+  __syncthreads();
+  const unsigned r = x - v + wsc[warp];
+  __syncthreads();
+  return r;
+}
+
+// V = hi 2^16 + lo (|V| < 2^51) as a double, exactly.
+__device__ __forceinline__ double from_parts(unsigned hi, unsigned lo) {
+  return from_fixed((long long)(int)hi * 65536 + (long long)lo);
+}
+
 // KP: Hermite weights per pass, 4 (two sequences; n <= 4096) or 2 (one sequence; n = 8192).
+//
+// Spread layout: while points are spread, the 16 slots of the cells of group g = cell/16
+// (slots 17 g .. 17 g + 15 of the padded grid) hold four planes of 16 words: the low 16
+// bits and the high bits of the fixed-point sums of the sequence's real part (k) and
+// imaginary part (k + 1), word 68 g + 16 plane + (cell % 16).  Every fixed-point value
+// X (|X| < 2^47) is added as two native 32-bit reductions, lo = X mod 2^16 and hi = X >> 16:
+// the low sums stay below 2^32 for up to 65536 points per cell and the high sums below 2^31,
+// so hi 2^16 + lo is the exact sum.  Points are taken in the order of their 16-cell group
+// (a counting sort per chunk of 8192), so the lanes of a warp add to neighbouring cells,
+// i.e. different banks.
 template <int KP>
 __global__ void __launch_bounds__(kNuThreads, 1)
 nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* __restrict__ npieces_p,
@@ -215,23 +271,34 @@ nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* _
                   const double* __restrict__ dinv, const double2* __restrict__ tw, const EsPoly es,
                   double* __restrict__ partial, double* __restrict__ wsum) {
   constexpr int NSEQ = KP / 2;
-  extern __shared__ double2 zs[];  // [NSEQ][n + n/16]
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ unsigned long long red[2];
-  const int n = 1 << logn;
-  const int seq_stride = n + (n >> 4);
+  __shared__ unsigned wsc[kNuThreads / 32];
+  const int n = 1 << logn, ng = n >> 4;
+  const int seq_stride = n + (n >> 4);  // double2 slots per sequence
+  double2* zs = reinterpret_cast<double2*>(smem_raw);
+  unsigned* zw = reinterpret_cast<unsigned*>(smem_raw);
+  uint16_t* order = reinterpret_cast<uint16_t*>(smem_raw + (size_t)16 * NSEQ * seq_stride);
+  unsigned* bucket = reinterpret_cast<unsigned*>(order + kSortChunk);
+  double2* tws = reinterpret_cast<double2*>(bucket + kMaxGroups);
+  double* dinvs = reinterpret_cast<double*>(tws + kMaxGroups);
+  for (int i = threadIdx.x; i < ng; i += blockDim.x) tws[i] = tw[i];
+  for (int m = threadIdx.x; m < Nl; m += blockDim.x) dinvs[m] = dinv[m];
+  __syncthreads();
   const double u_per_rad = (double)n * 0.15915494309189533577;  // n / (2 pi)
   const int npieces = (int)min((int64_t)*npieces_p, pmax);
   for (int piece = blockIdx.x; piece < npieces; piece += gridDim.x) {
     const int64_t start = piece_start[piece];
     const int len = piece_len[piece];
+    const double* rec0 = pay + (size_t)kRec * start;
     // A bound of sum |w| over the piece that does not depend on the order of its points (the
     // sort places the points of a key in any order): M = max |w|, then the exact integer
     // sum of rint(|w| 2^40 / M).  It bounds every grid value (|h_k| <= 1, psi <= 1), so the
-    // spread runs in 64-bit fixed point of step 2^(e - 50), 2^e >= the bound -- integer
-    // atomics, so the grid (and every result) does not depend on the order of the adds.
+    // spread runs in fixed point of step 2^(e - 46), 2^e >= the bound -- integer
+    // reductions, so the grid (and every result) does not depend on the order of the adds.
     unsigned long long mbits = 0ull;
     for (int p = threadIdx.x; p < len; p += blockDim.x)
-      mbits = max(mbits, (unsigned long long)__double_as_longlong(fabs(pay[(size_t)kRec * (start + p) + 2])));
+      mbits = max(mbits, (unsigned long long)__double_as_longlong(fabs(rec0[(size_t)kRec * p + 2])));
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) mbits = max(mbits, __shfl_xor_sync(0xffffffffu, mbits, o));
     if (threadIdx.x == 0) red[0] = 0ull;
@@ -242,7 +309,7 @@ nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* _
     const double to_int = wmax > 0.0 ? 0x1p40 / wmax : 0.0;
     unsigned long long isum = 0ull;
     for (int p = threadIdx.x; p < len; p += blockDim.x)
-      isum += fixed_point(fabs(pay[(size_t)kRec * (start + p) + 2]) * to_int);
+      isum += fixed_point(fabs(rec0[(size_t)kRec * p + 2]) * to_int);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) isum += __shfl_xor_sync(0xffffffffu, isum, o);
     if (threadIdx.x == 0) red[1] = 0ull;
@@ -256,64 +323,100 @@ nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* _
     if (wbound > 0.0) frexp(wbound, &ebound);  // wbound < 2^ebound
     // a NaN or infinite weight makes every sum of the piece NaN, as the direct sums would
     const double fx_step = red[0] >= 0x7ff0000000000000ull ? __longlong_as_double(0x7ff8000000000000ll)
-                                                             : ldexp(1.0, ebound - 50);
-    const double fx_scale = ldexp(1.0, 50 - ebound);
+                                                             : ldexp(1.0, ebound - 46);
+    const double fx_scale = ldexp(1.0, 46 - ebound);
     for (int kp = 0; kp < 4; kp += KP) {
       for (int i = threadIdx.x; i < NSEQ * seq_stride; i += blockDim.x) zs[i] = make_double2(0.0, 0.0);
-      __syncthreads();
-      unsigned long long* zi = reinterpret_cast<unsigned long long*>(zs);
-      for (int p = threadIdx.x; p < len; p += blockDim.x) {
-        const double2* rec = reinterpret_cast<const double2*>(pay + (size_t)kRec * (start + p));
-        const double phi = rec[0].x;  // in [0, 2 pi): the sort's azimuth record
-        const double2 r1 = rec[1];     // (w, t)
-        const double u = phi * u_per_rad;
-        const double fl = floor(u);
-        const double sv = 2.0 * (u - fl) - 1.0;
-        const int c0 = (int)fl - kEsW / 2 + 1;
-        double ker[kEsW];
-#pragma unroll
-        for (int i = 0; i < kEsW; ++i) {
-          double acc = es.c[i][kEsDeg];
-#pragma unroll
-          for (int d = kEsDeg - 1; d >= 0; --d) acc = fma(acc, sv, es.c[i][d]);
-          ker[i] = acc * fx_scale;
+      for (int c0 = 0; c0 < len; c0 += kSortChunk) {
+        const int clen = min(kSortChunk, len - c0);
+        const double* rc = rec0 + (size_t)kRec * c0;
+        // counting sort of the chunk by 16-cell group
+        for (int g = threadIdx.x; g < ng; g += blockDim.x) bucket[g] = 0u;
+        __syncthreads();
+        for (int p = threadIdx.x; p < clen; p += blockDim.x) {
+          const int cell = (int)floor(rc[(size_t)kRec * p] * u_per_rad) & (n - 1);
+          atomicAdd(&bucket[cell >> 4], 1u);
         }
-        double h[4];
-        hermite(r1.y, r1.x, h);
-        double ga[NSEQ], gb[NSEQ];  // the pass's weights: sequence q holds k = kp + 2q, kp + 2q + 1
-#pragma unroll
-        for (int q = 0; q < NSEQ; ++q) {
-          const bool lo = kp + 2 * q == 0;
-          ga[q] = lo ? h[0] : h[2];
-          gb[q] = lo ? h[1] : h[3];
+        __syncthreads();
+        {
+          const unsigned c = threadIdx.x < ng ? bucket[threadIdx.x] : 0u;  // ng <= 512 = blockDim
+          const unsigned o = block_excl_scan(c, wsc);
+          if (threadIdx.x < ng) bucket[threadIdx.x] = o;
         }
+        __syncthreads();
+        for (int p = threadIdx.x; p < clen; p += blockDim.x) {
+          const int cell = (int)floor(rc[(size_t)kRec * p] * u_per_rad) & (n - 1);
+          order[atomicAdd(&bucket[cell >> 4], 1u)] = (uint16_t)p;
+        }
+        __syncthreads();
+        for (int q = threadIdx.x; q < clen; q += blockDim.x) {
+          const double2* rec = reinterpret_cast<const double2*>(rc + (size_t)kRec * order[q]);
+          const double phi = rec[0].x;  // in [0, 2 pi): the sort's azimuth record
+          const double2 r1 = rec[1];     // (w, t)
+          const double u = phi * u_per_rad;
+          const double fl = floor(u);
+          const double sv = 2.0 * (u - fl) - 1.0;
+          const int cb = (int)fl - kEsW / 2 + 1;
+          double h[4];
+          hermite(r1.y, r1.x, h);
+          double ga[NSEQ], gb[NSEQ];  // the pass's weights: sequence q holds k = kp + 2q, kp + 2q + 1
 #pragma unroll
-        for (int i = 0; i < kEsW; ++i) {
-          const int cell = padi((c0 + i) & (n - 1));
+          for (int sq = 0; sq < NSEQ; ++sq) {
+            const bool lo = kp + 2 * sq == 0;
+            ga[sq] = lo ? h[0] : h[2];
+            gb[sq] = lo ? h[1] : h[3];
+          }
+          // kernel values six at a time (six independent Horner chains; a rolled loop keeps the
+          // live registers within the 128 of a 512-thread CTA)
+#pragma unroll 1
+          for (int i0 = 0; i0 < kEsW; i0 += 6) {
+            double ker[6];
 #pragma unroll
-          for (int q = 0; q < NSEQ; ++q) {
-            unsigned long long* z = zi + 2 * (q * seq_stride + cell);
-            atomicAdd(z, fixed_point(ga[q] * ker[i]));
-            atomicAdd(z + 1, fixed_point(gb[q] * ker[i]));
+            for (int i = 0; i < 6; ++i) {
+              double acc = es.c[i0 + i][kEsDeg];
+#pragma unroll
+              for (int d = kEsDeg - 1; d >= 0; --d) acc = fma(acc, sv, es.c[i0 + i][d]);
+              ker[i] = acc * fx_scale;
+            }
+#pragma unroll
+            for (int i = 0; i < 6; ++i) {
+              const int cell = (cb + i0 + i) & (n - 1);
+              const int wo = 68 * (cell >> 4) + (cell & 15);
+#pragma unroll
+              for (int sq = 0; sq < NSEQ; ++sq) {
+                unsigned* z = zw + 4 * sq * seq_stride + wo;
+                const long long xa = (long long)fixed_point(ga[sq] * ker[i]);
+                const long long xb = (long long)fixed_point(gb[sq] * ker[i]);
+                atomicAdd(z, (unsigned)xa & 0xffffu);
+                atomicAdd(z + 16, (unsigned)(xa >> 16));
+                atomicAdd(z + 32, (unsigned)xb & 0xffffu);
+                atomicAdd(z + 48, (unsigned)(xb >> 16));
+              }
+            }
           }
         }
+        __syncthreads();
+      }
+      // planes -> FP64 complex slots, one 16-cell group per half warp (in place: the half
+      // warp reads its group's 64 words before writing its 16 slots)
+      for (int gi = threadIdx.x >> 4; gi < NSEQ * ng; gi += blockDim.x >> 4) {
+        const int sq = gi / ng, g = gi - sq * ng, r = threadIdx.x & 15;
+        const unsigned* w = zw + 4 * sq * seq_stride + 68 * g;
+        const unsigned la = w[r], ha = w[16 + r], lb = w[32 + r], hb = w[48 + r];
+        __syncwarp();
+        zs[sq * seq_stride + 17 * g + r] = make_double2(from_parts(ha, la), from_parts(hb, lb));
+        __syncwarp();
       }
       __syncthreads();
-      // fixed point -> FP64 (exact: |value| < 2^51); the step is applied to the outputs
-      for (int i = threadIdx.x; i < NSEQ * seq_stride; i += blockDim.x) {
-        const longlong2 v = reinterpret_cast<const longlong2*>(zs)[i];
-        zs[i] = make_double2(from_fixed(v.x), from_fixed(v.y));
-      }
-      __syncthreads();
-      fft_all<NSEQ>(zs, seq_stride, logn, tw);
+      fft_all<NSEQ>(zs, seq_stride, logn, tws);
       // v_k0 = (Z[m] + conj Z[-m]) / 2, v_k1 = (Z[m] - conj Z[-m]) / 2i, each over Psi(m)
       for (int m = threadIdx.x; m < Nl; m += blockDim.x) {
         const int pm = padi(fft_pos(m, logn)), pn = padi(fft_pos((n - m) & (n - 1), logn));
-        const double di = 0.5 * fx_step * dinv[m];
+        const double di = 0.5 * fx_step * dinvs[m];
 #pragma unroll
-        for (int q = 0; q < NSEQ; ++q) {
-          const double2 a = zs[q * seq_stride + pm], b = zs[q * seq_stride + pn];
-          const int k0 = kp + 2 * q;
+        for (int sq = 0; sq < NSEQ; ++sq) {
+          const double2 a = zs[sq * seq_stride + pm], b = zs[sq * seq_stride + pn];
+          const int k0 = kp + 2 * sq;
           double* o = partial + ((size_t)piece * 8 + 2 * k0) * Nl + m;
           o[0] = (a.x + b.x) * di;
           o[(size_t)Nl] = (a.y - b.y) * di;
@@ -326,7 +429,11 @@ nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* _
   }
 }
 
+}  // namespace
+
 // ---- host: kernel polynomials and the deconvolution factors ----------------------------
+
+namespace {
 
 double es_kernel(double x) {
   const double z = 2.0 * x / kEsW;
@@ -432,9 +539,8 @@ void nufft_host_tables(int Nl, int logn, std::vector<double>& dinv, std::vector<
 
 int launch_bin_sums_nufft(const Geometry& g, const Workspace& ws, int logn, const double* dinv, const double* tw,
                           cudaStream_t s) {
-  const int n = 1 << logn;
   const int kp = logn <= 12 ? 4 : 2;
-  const size_t smem = sizeof(double2) * (size_t)(kp / 2) * (n + n / 16);
+  const size_t smem = nufft_smem_bytes(logn, kp / 2);
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
