@@ -139,9 +139,9 @@ def dram_traffic(stage, precision, N, Nlm, Nx):
 
 
 def nufft_logn(Nl):
-    """log2 of the NUFFT grid: 4 x 2^ceil(log2 Nl) cells, at least 64 (nufft.cu)."""
+    """log2 of the NUFFT grid: 4 x 2^ceil(log2 Nl) cells, at least 128 (nufft.cu)."""
     lg = max(int(np.ceil(np.log2(max(Nl, 1)))), 0) + 2
-    return max(lg, 6)
+    return max(lg, 7)
 
 
 def nufft_pieces(th, ph, Nx, xmax, piece):

@@ -19,7 +19,7 @@
 // kernel parameter, so every Horner step is one DFMA with a uniform operand.
 //
 // One CTA per piece (persistent over pieces): an order-independent bound of the piece's
-// sum |w| sets a fixed-point step; the piece's points are bucketed by 16-cell group (a
+// sum |w| sets a fixed-point step; the piece's points are bucketed by grid cell (a
 // counting sort in shared memory) and spread in that order as 46-bit fixed-point values,
 // each added as two native 32-bit shared-memory reductions (low 16 bits, high bits), so the
 // sums are exact, independent of the order of the adds, and a warp's adds land on
@@ -211,14 +211,15 @@ __device__ void fft_all(double2* zs, int seq_stride, int logn, const double2* __
 }
 
 constexpr int kSortChunk = 8192;  // points bucketed at a time (order indices are 16-bit)
-constexpr int kMaxGroups = 512;   // 16-cell groups of the largest grid (n = 8192)
+constexpr int kMaxCells = 8192;   // cells of the largest grid (Nl = 2048)
+constexpr int kMaxTw = kMaxCells / 16;
 constexpr int kMaxNl = 2048;
 
-// Shared-memory bytes of a launch: the grids, then the bucket order, bucket offsets,
+// Shared-memory bytes of a launch: the grids, then the bucket order, per-cell offsets,
 // twiddles e^{2 pi i j/n} (j < n/16) and 1/Psi(m).
 size_t nufft_smem_bytes(int logn, int nseq) {
   const size_t n = (size_t)1 << logn;
-  return 16 * nseq * (n + n / 16) + 2 * kSortChunk + 4 * kMaxGroups + 16 * kMaxGroups + 8 * kMaxNl;
+  return 16 * nseq * (n + n / 16) + 2 * kSortChunk + 4 * kMaxCells + 16 * kMaxTw + 8 * kMaxNl;
 }
 
 // Exclusive prefix sum over the block (every thread passes one value).
@@ -255,15 +256,16 @@ __device__ __forceinline__ double from_parts(unsigned hi, unsigned lo) {
 
 // KP: Hermite weights per pass, 4 (two sequences; n <= 4096) or 2 (one sequence; n = 8192).
 //
-// Spread layout: while points are spread, the 16 slots of the cells of group g = cell/16
-// (slots 17 g .. 17 g + 15 of the padded grid) hold four planes of 16 words: the low 16
-// bits and the high bits of the fixed-point sums of the sequence's real part (k) and
-// imaginary part (k + 1), word 68 g + 16 plane + (cell % 16).  Every fixed-point value
-// X (|X| < 2^47) is added as two native 32-bit reductions, lo = X mod 2^16 and hi = X >> 16:
-// the low sums stay below 2^32 for up to 65536 points per cell and the high sums below 2^31,
-// so hi 2^16 + lo is the exact sum.  Points are taken in the order of their 16-cell group
-// (a counting sort per chunk of 8192), so the lanes of a warp add to neighbouring cells,
-// i.e. different banks.
+// Spread layout: while points are spread, the 136 slots (544 words) of each 128-cell group g
+// of a sequence hold four planes of 128 words: the low 16 bits and the high bits of the
+// fixed-point sums of the sequence's real part (k) and imaginary part (k + 1), word
+// 544 g + 128 plane + cell % 128 -- a multiple of 32 plus the cell, so consecutive cells
+// fall in consecutive banks, across groups too.  Every fixed-point value X (|X| < 2^47)
+// is added as two native 32-bit reductions, lo = X mod 2^16 and hi = X >> 16: the low sums
+// stay below 2^32 for up to 65536 points per cell and the high sums below 2^31, so
+// hi 2^16 + lo is the exact sum.  Points are taken in the order of their cell (a counting
+// sort per chunk of 8192), so the lanes of a warp add to consecutive words, i.e.
+// different banks.
 template <int KP>
 __global__ void __launch_bounds__(kNuThreads, 1)
 nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* __restrict__ npieces_p,
@@ -275,13 +277,14 @@ nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* _
   __shared__ unsigned long long red[2];
   __shared__ unsigned wsc[kNuThreads / 32];
   const int n = 1 << logn, ng = n >> 4;
+  const int cper = (n + kNuThreads - 1) / kNuThreads;  // cells per thread in the offset scan
   const int seq_stride = n + (n >> 4);  // double2 slots per sequence
   double2* zs = reinterpret_cast<double2*>(smem_raw);
   unsigned* zw = reinterpret_cast<unsigned*>(smem_raw);
   uint16_t* order = reinterpret_cast<uint16_t*>(smem_raw + (size_t)16 * NSEQ * seq_stride);
   unsigned* bucket = reinterpret_cast<unsigned*>(order + kSortChunk);
-  double2* tws = reinterpret_cast<double2*>(bucket + kMaxGroups);
-  double* dinvs = reinterpret_cast<double*>(tws + kMaxGroups);
+  double2* tws = reinterpret_cast<double2*>(bucket + kMaxCells);
+  double* dinvs = reinterpret_cast<double*>(tws + kMaxTw);
   for (int i = threadIdx.x; i < ng; i += blockDim.x) tws[i] = tw[i];
   for (int m = threadIdx.x; m < Nl; m += blockDim.x) dinvs[m] = dinv[m];
   __syncthreads();
@@ -330,23 +333,30 @@ nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* _
       for (int c0 = 0; c0 < len; c0 += kSortChunk) {
         const int clen = min(kSortChunk, len - c0);
         const double* rc = rec0 + (size_t)kRec * c0;
-        // counting sort of the chunk by 16-cell group
-        for (int g = threadIdx.x; g < ng; g += blockDim.x) bucket[g] = 0u;
+        // counting sort of the chunk by cell
+        for (int c = threadIdx.x; c < n; c += blockDim.x) bucket[c] = 0u;
         __syncthreads();
         for (int p = threadIdx.x; p < clen; p += blockDim.x) {
           const int cell = (int)floor(rc[(size_t)kRec * p] * u_per_rad) & (n - 1);
-          atomicAdd(&bucket[cell >> 4], 1u);
+          atomicAdd(&bucket[cell], 1u);
         }
         __syncthreads();
         {
-          const unsigned c = threadIdx.x < ng ? bucket[threadIdx.x] : 0u;  // ng <= 512 = blockDim
-          const unsigned o = block_excl_scan(c, wsc);
-          if (threadIdx.x < ng) bucket[threadIdx.x] = o;
+          // thread t scans cells [t cper, (t + 1) cper)
+          const int b0 = min(n, (int)threadIdx.x * cper), b1 = min(n, b0 + cper);
+          unsigned tot = 0u;
+          for (int c = b0; c < b1; ++c) tot += bucket[c];
+          unsigned o = block_excl_scan(tot, wsc);
+          for (int c = b0; c < b1; ++c) {
+            const unsigned v = bucket[c];
+            bucket[c] = o;
+            o += v;
+          }
         }
         __syncthreads();
         for (int p = threadIdx.x; p < clen; p += blockDim.x) {
           const int cell = (int)floor(rc[(size_t)kRec * p] * u_per_rad) & (n - 1);
-          order[atomicAdd(&bucket[cell >> 4], 1u)] = (uint16_t)p;
+          order[atomicAdd(&bucket[cell], 1u)] = (uint16_t)p;
         }
         __syncthreads();
         for (int q = threadIdx.x; q < clen; q += blockDim.x) {
@@ -381,33 +391,49 @@ nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* _
 #pragma unroll
             for (int i = 0; i < 6; ++i) {
               const int cell = (cb + i0 + i) & (n - 1);
-              const int wo = 68 * (cell >> 4) + (cell & 15);
+              const int wo = 544 * (cell >> 7) + (cell & 127);
 #pragma unroll
               for (int sq = 0; sq < NSEQ; ++sq) {
                 unsigned* z = zw + 4 * sq * seq_stride + wo;
                 const long long xa = (long long)fixed_point(ga[sq] * ker[i]);
                 const long long xb = (long long)fixed_point(gb[sq] * ker[i]);
                 atomicAdd(z, (unsigned)xa & 0xffffu);
-                atomicAdd(z + 16, (unsigned)(xa >> 16));
-                atomicAdd(z + 32, (unsigned)xb & 0xffffu);
-                atomicAdd(z + 48, (unsigned)(xb >> 16));
+                atomicAdd(z + 128, (unsigned)(xa >> 16));
+                atomicAdd(z + 256, (unsigned)xb & 0xffffu);
+                atomicAdd(z + 384, (unsigned)(xb >> 16));
               }
             }
           }
         }
         __syncthreads();
       }
-      // planes -> FP64 complex slots, one 16-cell group per half warp (in place: the half
-      // warp reads its group's 64 words before writing its 16 slots)
-      for (int gi = threadIdx.x >> 4; gi < NSEQ * ng; gi += blockDim.x >> 4) {
-        const int sq = gi / ng, g = gi - sq * ng, r = threadIdx.x & 15;
-        const unsigned* w = zw + 4 * sq * seq_stride + 68 * g;
-        const unsigned la = w[r], ha = w[16 + r], lb = w[32 + r], hb = w[48 + r];
-        __syncwarp();
-        zs[sq * seq_stride + 17 * g + r] = make_double2(from_parts(ha, la), from_parts(hb, lb));
-        __syncwarp();
+      // planes -> FP64 complex slots, in place, 2048 cells (16 whole groups) at a time:
+      // every thread reads four cells' words, then all write their padded slots
+      for (int e0 = 0; e0 < NSEQ * n; e0 += 4 * kNuThreads) {
+        unsigned v[4][4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int e = e0 + threadIdx.x + kNuThreads * i;
+          if (e < NSEQ * n) {
+            const int sq = e >> logn, c = e & (n - 1);
+            const unsigned* w = zw + 4 * sq * seq_stride + 544 * (c >> 7) + (c & 127);
+            v[i][0] = w[0];
+            v[i][1] = w[128];
+            v[i][2] = w[256];
+            v[i][3] = w[384];
+          }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int e = e0 + threadIdx.x + kNuThreads * i;
+          if (e < NSEQ * n) {
+            const int sq = e >> logn, c = e & (n - 1);
+            zs[sq * seq_stride + padi(c)] = make_double2(from_parts(v[i][1], v[i][0]), from_parts(v[i][3], v[i][2]));
+          }
+        }
+        __syncthreads();
       }
-      __syncthreads();
       fft_all<NSEQ>(zs, seq_stride, logn, tws);
       // v_k0 = (Z[m] + conj Z[-m]) / 2, v_k1 = (Z[m] - conj Z[-m]) / 2i, each over Psi(m)
       for (int m = threadIdx.x; m < Nl; m += blockDim.x) {
@@ -504,10 +530,10 @@ void gauss_legendre(int q, std::vector<double>& x, std::vector<double>& w) {
 }  // namespace
 
 int nufft_logn(int Nl) {
-  int lg = 2;  // n = 4 * 2^ceil(log2 Nl), at least 64
+  int lg = 0;  // n = 4 * 2^ceil(log2 Nl), at least 128 (one 128-cell spread group)
   while ((1 << lg) < Nl) ++lg;
   lg += 2;
-  return lg < 6 ? 6 : lg;
+  return lg < 7 ? 7 : lg;
 }
 
 const EsPoly& es_poly() {

@@ -21,7 +21,8 @@ namespace dsht {
 namespace {
 
 constexpr int kPointThreads = 256;
-constexpr int kScatterTile = 16384;  // points per block in the scatter pass
+constexpr int kScatterTile = 8192;  // points per block in the scatter pass: 1221 blocks at N = 1e7,
+                                    // several waves of 3 resident blocks per SM
 
 // The binning of one point: key = set * nbins + bin (DSHT_KEY_DROP when it is in no set)
 // and its flag bits.  x = cos(theta) for equatorial points; a polar point (|cos theta| >=
@@ -311,6 +312,7 @@ scatter_kernel(Geometry g, const double* __restrict__ theta, const double* __res
   }
   __syncthreads();
   const int polar_key0 = 2 * g.nbins;
+  const double inv_dx = 1.0 / g.dx;
   for (int64_t b = lo + threadIdx.x; b < hi; b += step) {
     uint32_t k[kUnroll];
     double th[kUnroll], ph[kUnroll], wi[kUnroll];
@@ -361,7 +363,10 @@ scatter_kernel(Geometry g, const double* __restrict__ theta, const double* __res
         }
       }
       const int j = (int)(k[u] % (uint32_t)g.nbins);
-      const double t = __ddiv_rn(__dadd_rn(fabs(x), -(double)j * g.dx), g.dx);
+      // t = (|x| - x_j) / dx in the reference's rounding (sht/sht.py:221); the NUFFT route
+      // (mixed levels) takes the product with 1/dx, within an ulp of it
+      const double t = PHI ? (fabs(x) - (double)j * g.dx) * inv_dx
+                           : __ddiv_rn(__dadd_rn(fabs(x), -(double)j * g.dx), g.dx);
       const uint32_t pos = atomicAdd(&loc[k[u]], 1u);
       double2* out = reinterpret_cast<double2*>(pay + (size_t)kRec * pos);  // one 32-byte sector
       out[0] = make_double2(cphi, sphi);
@@ -450,7 +455,7 @@ void launch_points(const Geometry& g, const double* theta, const double* phi, co
   cudaFuncSetAttribute(count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csmem);
   if (N > 0) {
     int64_t blocks = (N + kPointThreads * 8 - 1) / (kPointThreads * 8);
-    if (blocks > 148 * 8) blocks = 148 * 8;
+    if (blocks > 148 * 4) blocks = 148 * 4;  // fewer, longer blocks: fewer per-block key flushes
     // fraction-of-bin guard of the FP32 screen: the x bound over dx, plus the rounding of
     // u = |x| / dx (four roundings of a value below nbins)
     const float guard = (float)(kScreenX / g.dx + 4.0 * g.nbins * 5.960464477539063e-08 + 1e-6);
