@@ -19,11 +19,10 @@
 // kernel parameter, so every Horner step is one DFMA with a uniform operand.
 //
 // One CTA per piece (persistent over pieces): an order-independent bound of the piece's
-// sum |w| sets a fixed-point step; the piece's points are bucketed by grid cell (a
-// counting sort in shared memory) and spread in that order as 46-bit fixed-point values,
-// each added as two native 32-bit shared-memory reductions (low 16 bits, high bits), so the
-// sums are exact, independent of the order of the adds, and a warp's adds land on
-// neighbouring cells; the planes are converted to FP64 in place, then an in-place
+// sum |w| sets a fixed-point step; the piece's points are spread as 46-bit fixed-point
+// values, each added as two native 32-bit shared-memory reductions (low 16 bits, high
+// bits), so the sums are exact and independent of the order of the adds; the planes
+// (bank = cell mod 32) are converted to FP64 in place, then an in-place
 // decimation-in-frequency FFT (radix-16 passes and one radix-2/4/8 pass, the 16-point DFTs
 // in registers, twiddles staged in shared memory), then each thread reads the outputs of
 // its m from their digit-reversed positions, divides by Psi(m) and writes the piece's
@@ -210,43 +209,14 @@ __device__ void fft_all(double2* zs, int seq_stride, int logn, const double2* __
   __syncthreads();
 }
 
-constexpr int kSortChunk = 8192;  // points bucketed at a time (order indices are 16-bit)
-constexpr int kMaxCells = 8192;   // cells of the largest grid (Nl = 2048)
-constexpr int kMaxTw = kMaxCells / 16;
+constexpr int kMaxTw = 8192 / 16;  // twiddles of the largest grid (Nl = 2048)
 constexpr int kMaxNl = 2048;
 
-// Shared-memory bytes of a launch: the grids, then the bucket order, per-cell offsets,
-// twiddles e^{2 pi i j/n} (j < n/16) and 1/Psi(m).
+// Shared-memory bytes of a launch: the grids, then the twiddles e^{2 pi i j/n} (j < n/16)
+// and 1/Psi(m).
 size_t nufft_smem_bytes(int logn, int nseq) {
   const size_t n = (size_t)1 << logn;
-  return 16 * nseq * (n + n / 16) + 2 * kSortChunk + 4 * kMaxCells + 16 * kMaxTw + 8 * kMaxNl;
-}
-
-// Exclusive prefix sum over the block (every thread passes one value).
-__device__ __forceinline__ unsigned block_excl_scan(unsigned v, unsigned* wsc) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  unsigned x = v;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) wsc[warp] = x;
-  __syncthreads();
-  if (warp == 0) {
-    const unsigned t = lane < (int)(blockDim.x >> 5) ? wsc[lane] : 0u;
-    unsigned sc = t;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const unsigned y = __shfl_up_sync(0xffffffffu, sc, o);
-      if (lane >= o) sc += y;
-    }
-    if (lane < (int)(blockDim.x >> 5)) wsc[lane] = sc - t;
-  }
-  __syncthreads();
-  const unsigned r = x - v + wsc[warp];
-  __syncthreads();
-  return r;
+  return 16 * nseq * (n + n / 16) + 16 * kMaxTw + 8 * kMaxNl;
 }
 
 // V = hi 2^16 + lo (|V| < 2^51) as a double, exactly.
@@ -263,9 +233,9 @@ __device__ __forceinline__ double from_parts(unsigned hi, unsigned lo) {
 // fall in consecutive banks, across groups too.  Every fixed-point value X (|X| < 2^47)
 // is added as two native 32-bit reductions, lo = X mod 2^16 and hi = X >> 16: the low sums
 // stay below 2^32 for up to 65536 points per cell and the high sums below 2^31, so
-// hi 2^16 + lo is the exact sum.  Points are taken in the order of their cell (a counting
-// sort per chunk of 8192), so the lanes of a warp add to consecutive words, i.e.
-// different banks.
+// hi 2^16 + lo is the exact sum.  Points are taken in record order (random cells): a warp's
+// 32 reductions fall on random banks.  (Taking them in cell order was measured slower:
+// several points of a piece share a cell, and same-word reductions serialise.)
 template <int KP>
 __global__ void __launch_bounds__(kNuThreads, 1)
 nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* __restrict__ npieces_p,
@@ -275,15 +245,11 @@ nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* _
   constexpr int NSEQ = KP / 2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ unsigned long long red[2];
-  __shared__ unsigned wsc[kNuThreads / 32];
   const int n = 1 << logn, ng = n >> 4;
-  const int cper = (n + kNuThreads - 1) / kNuThreads;  // cells per thread in the offset scan
   const int seq_stride = n + (n >> 4);  // double2 slots per sequence
   double2* zs = reinterpret_cast<double2*>(smem_raw);
   unsigned* zw = reinterpret_cast<unsigned*>(smem_raw);
-  uint16_t* order = reinterpret_cast<uint16_t*>(smem_raw + (size_t)16 * NSEQ * seq_stride);
-  unsigned* bucket = reinterpret_cast<unsigned*>(order + kSortChunk);
-  double2* tws = reinterpret_cast<double2*>(bucket + kMaxCells);
+  double2* tws = reinterpret_cast<double2*>(smem_raw + (size_t)16 * NSEQ * seq_stride);
   double* dinvs = reinterpret_cast<double*>(tws + kMaxTw);
   for (int i = threadIdx.x; i < ng; i += blockDim.x) tws[i] = tw[i];
   for (int m = threadIdx.x; m < Nl; m += blockDim.x) dinvs[m] = dinv[m];
@@ -330,37 +296,10 @@ nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* _
     const double fx_scale = ldexp(1.0, 46 - ebound);
     for (int kp = 0; kp < 4; kp += KP) {
       for (int i = threadIdx.x; i < NSEQ * seq_stride; i += blockDim.x) zs[i] = make_double2(0.0, 0.0);
-      for (int c0 = 0; c0 < len; c0 += kSortChunk) {
-        const int clen = min(kSortChunk, len - c0);
-        const double* rc = rec0 + (size_t)kRec * c0;
-        // counting sort of the chunk by cell
-        for (int c = threadIdx.x; c < n; c += blockDim.x) bucket[c] = 0u;
-        __syncthreads();
-        for (int p = threadIdx.x; p < clen; p += blockDim.x) {
-          const int cell = (int)floor(rc[(size_t)kRec * p] * u_per_rad) & (n - 1);
-          atomicAdd(&bucket[cell], 1u);
-        }
-        __syncthreads();
-        {
-          // thread t scans cells [t cper, (t + 1) cper)
-          const int b0 = min(n, (int)threadIdx.x * cper), b1 = min(n, b0 + cper);
-          unsigned tot = 0u;
-          for (int c = b0; c < b1; ++c) tot += bucket[c];
-          unsigned o = block_excl_scan(tot, wsc);
-          for (int c = b0; c < b1; ++c) {
-            const unsigned v = bucket[c];
-            bucket[c] = o;
-            o += v;
-          }
-        }
-        __syncthreads();
-        for (int p = threadIdx.x; p < clen; p += blockDim.x) {
-          const int cell = (int)floor(rc[(size_t)kRec * p] * u_per_rad) & (n - 1);
-          order[atomicAdd(&bucket[cell], 1u)] = (uint16_t)p;
-        }
-        __syncthreads();
-        for (int q = threadIdx.x; q < clen; q += blockDim.x) {
-          const double2* rec = reinterpret_cast<const double2*>(rc + (size_t)kRec * order[q]);
+      __syncthreads();
+      {
+        for (int q = threadIdx.x; q < len; q += blockDim.x) {
+          const double2* rec = reinterpret_cast<const double2*>(rec0 + (size_t)kRec * q);
           const double phi = rec[0].x;  // in [0, 2 pi): the sort's azimuth record
           const double2 r1 = rec[1];     // (w, t)
           const double u = phi * u_per_rad;
