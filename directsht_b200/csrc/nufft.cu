@@ -211,12 +211,13 @@ __device__ void fft_all(double2* zs, int seq_stride, int logn, const double2* __
 
 constexpr int kMaxTw = 8192 / 16;  // twiddles of the largest grid (Nl = 2048)
 constexpr int kMaxNl = 2048;
+constexpr int kOrderChunk = 8192;  // points ordered at a time (16-bit order indices)
 
-// Shared-memory bytes of a launch: the grids, then the twiddles e^{2 pi i j/n} (j < n/16)
-// and 1/Psi(m).
+// Shared-memory bytes of a launch: the grids, then the twiddles e^{2 pi i j/n} (j < n/16),
+// 1/Psi(m) and the bank-balanced point order.
 size_t nufft_smem_bytes(int logn, int nseq) {
   const size_t n = (size_t)1 << logn;
-  return 16 * nseq * (n + n / 16) + 16 * kMaxTw + 8 * kMaxNl;
+  return 16 * nseq * (n + n / 16) + 16 * kMaxTw + 8 * kMaxNl + 2 * kOrderChunk;
 }
 
 // V = hi 2^16 + lo (|V| < 2^51) as a double, exactly.
@@ -251,6 +252,10 @@ nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* _
   unsigned* zw = reinterpret_cast<unsigned*>(smem_raw);
   double2* tws = reinterpret_cast<double2*>(smem_raw + (size_t)16 * NSEQ * seq_stride);
   double* dinvs = reinterpret_cast<double*>(tws + kMaxTw);
+  uint16_t* order = reinterpret_cast<uint16_t*>(dinvs + kMaxNl);
+  __shared__ unsigned bcnt[32], boff[33];
+  __shared__ int bmax;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   for (int i = threadIdx.x; i < ng; i += blockDim.x) tws[i] = tw[i];
   for (int m = threadIdx.x; m < Nl; m += blockDim.x) dinvs[m] = dinv[m];
   __syncthreads();
@@ -297,9 +302,41 @@ nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* _
     for (int kp = 0; kp < 4; kp += KP) {
       for (int i = threadIdx.x; i < NSEQ * seq_stride; i += blockDim.x) zs[i] = make_double2(0.0, 0.0);
       __syncthreads();
-      {
-        for (int q = threadIdx.x; q < len; q += blockDim.x) {
-          const double2* rec = reinterpret_cast<const double2*>(rec0 + (size_t)kRec * q);
+      for (int c0 = 0; c0 < len; c0 += kOrderChunk) {
+        // Bank-balanced order: bucket the chunk's points by (first cell) mod 32, then round r
+        // of a warp gives lane l the r-th point of bucket l, so the 32 lanes start on 32
+        // different banks and every one of their reductions is conflict-free.
+        const int clen = min(kOrderChunk, len - c0);
+        const double* rc = rec0 + (size_t)kRec * c0;
+        if (threadIdx.x < 32) bcnt[threadIdx.x] = 0u;
+        __syncthreads();
+        for (int p = threadIdx.x; p < clen; p += blockDim.x)
+          atomicAdd(&bcnt[(int)floor(rc[(size_t)kRec * p] * u_per_rad) & 31], 1u);
+        __syncthreads();
+        if (warp == 0) {
+          const unsigned c = bcnt[lane];
+          unsigned x = c;
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+          }
+          unsigned mx = c;
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+          boff[lane] = x - c;
+          bcnt[lane] = x - c;  // cursor
+          if (lane == 31) boff[32] = x;
+          if (lane == 0) bmax = (int)mx;
+        }
+        __syncthreads();
+        for (int p = threadIdx.x; p < clen; p += blockDim.x)
+          order[atomicAdd(&bcnt[(int)floor(rc[(size_t)kRec * p] * u_per_rad) & 31], 1u)] = (uint16_t)p;
+        __syncthreads();
+        for (int r = warp; r < bmax; r += nwarps) {
+          const unsigned idx = boff[lane] + (unsigned)r;
+          if (idx >= boff[lane + 1]) continue;
+          const double2* rec = reinterpret_cast<const double2*>(rc + (size_t)kRec * order[idx]);
           const double phi = rec[0].x;  // in [0, 2 pi): the sort's azimuth record
           const double2 r1 = rec[1];     // (w, t)
           const double u = phi * u_per_rad;
