@@ -212,6 +212,7 @@ __device__ void fft_all(double2* zs, int seq_stride, int logn, const double2* __
 constexpr int kMaxTw = 8192 / 16;  // twiddles of the largest grid (Nl = 2048)
 constexpr int kMaxNl = 2048;
 constexpr int kOrderChunk = 8192;  // points ordered at a time (16-bit order indices)
+constexpr int kBalanceMin = 4096;  // smallest chunk given the bank-balanced order
 
 // Shared-memory bytes of a launch: the grids, then the twiddles e^{2 pi i j/n} (j < n/16),
 // 1/Psi(m) and the bank-balanced point order.
@@ -242,7 +243,7 @@ __global__ void __launch_bounds__(kNuThreads, 1)
 nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* __restrict__ npieces_p,
                   int64_t pmax, const int64_t* __restrict__ piece_start, const int* __restrict__ piece_len,
                   const double* __restrict__ dinv, const double2* __restrict__ tw, const EsPoly es,
-                  double* __restrict__ partial, double* __restrict__ wsum) {
+                  double* __restrict__ partial, double* __restrict__ wsum, int balance_min) {
   constexpr int NSEQ = KP / 2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ unsigned long long red[2];
@@ -308,35 +309,48 @@ nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* _
         // different banks and every one of their reductions is conflict-free.
         const int clen = min(kOrderChunk, len - c0);
         const double* rc = rec0 + (size_t)kRec * c0;
-        if (threadIdx.x < 32) bcnt[threadIdx.x] = 0u;
-        __syncthreads();
-        for (int p = threadIdx.x; p < clen; p += blockDim.x)
-          atomicAdd(&bcnt[(int)floor(rc[(size_t)kRec * p] * u_per_rad) & 31], 1u);
-        __syncthreads();
-        if (warp == 0) {
-          const unsigned c = bcnt[lane];
-          unsigned x = c;
+        // small chunks keep their record order (lane l of round r takes point 32 r + l): the
+        // ordering passes would cost more than the bank conflicts they remove
+        const bool balanced = clen >= balance_min;
+        if (balanced) {
+          if (threadIdx.x < 32) bcnt[threadIdx.x] = 0u;
+          __syncthreads();
+          for (int p = threadIdx.x; p < clen; p += blockDim.x)
+            atomicAdd(&bcnt[(int)floor(rc[(size_t)kRec * p] * u_per_rad) & 31], 1u);
+          __syncthreads();
+          if (warp == 0) {
+            const unsigned c = bcnt[lane];
+            unsigned x = c;
 #pragma unroll
-          for (int o = 1; o < 32; o <<= 1) {
-            const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
+            for (int o = 1; o < 32; o <<= 1) {
+              const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+              if (lane >= o) x += y;
+            }
+            unsigned mx = c;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+            boff[lane] = x - c;
+            bcnt[lane] = x - c;  // cursor
+            if (lane == 31) boff[32] = x;
+            if (lane == 0) bmax = (int)mx;
           }
-          unsigned mx = c;
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-          boff[lane] = x - c;
-          bcnt[lane] = x - c;  // cursor
-          if (lane == 31) boff[32] = x;
-          if (lane == 0) bmax = (int)mx;
+          __syncthreads();
+          for (int p = threadIdx.x; p < clen; p += blockDim.x)
+            order[atomicAdd(&bcnt[(int)floor(rc[(size_t)kRec * p] * u_per_rad) & 31], 1u)] = (uint16_t)p;
+          __syncthreads();
         }
-        __syncthreads();
-        for (int p = threadIdx.x; p < clen; p += blockDim.x)
-          order[atomicAdd(&bcnt[(int)floor(rc[(size_t)kRec * p] * u_per_rad) & 31], 1u)] = (uint16_t)p;
-        __syncthreads();
-        for (int r = warp; r < bmax; r += nwarps) {
-          const unsigned idx = boff[lane] + (unsigned)r;
-          if (idx >= boff[lane + 1]) continue;
-          const double2* rec = reinterpret_cast<const double2*>(rc + (size_t)kRec * order[idx]);
+        const int rounds = balanced ? bmax : (clen + 31) >> 5;
+        for (int r = warp; r < rounds; r += nwarps) {
+          int pnt;
+          if (balanced) {
+            const unsigned idx = boff[lane] + (unsigned)r;
+            if (idx >= boff[lane + 1]) continue;
+            pnt = order[idx];
+          } else {
+            pnt = 32 * r + lane;
+            if (pnt >= clen) continue;
+          }
+          const double2* rec = reinterpret_cast<const double2*>(rc + (size_t)kRec * pnt);
           const double phi = rec[0].x;  // in [0, 2 pi): the sort's azimuth record
           const double2 r1 = rec[1];     // (w, t)
           const double u = phi * u_per_rad;
@@ -345,12 +359,13 @@ nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* _
           const int cb = (int)fl - kEsW / 2 + 1;
           double h[4];
           hermite(r1.y, r1.x, h);
-          double ga[NSEQ], gb[NSEQ];  // the pass's weights: sequence q holds k = kp + 2q, kp + 2q + 1
+          // the pass's weights in fixed-point units: sequence q holds k = kp + 2q, kp + 2q + 1
+          double ga[NSEQ], gb[NSEQ];
 #pragma unroll
           for (int sq = 0; sq < NSEQ; ++sq) {
             const bool lo = kp + 2 * sq == 0;
-            ga[sq] = lo ? h[0] : h[2];
-            gb[sq] = lo ? h[1] : h[3];
+            ga[sq] = (lo ? h[0] : h[2]) * fx_scale;
+            gb[sq] = (lo ? h[1] : h[3]) * fx_scale;
           }
           // kernel values six at a time (six independent Horner chains; a rolled loop keeps the
           // live registers within the 128 of a 512-thread CTA)
@@ -362,7 +377,7 @@ nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* _
               double acc = es.c[i0 + i][kEsDeg];
 #pragma unroll
               for (int d = kEsDeg - 1; d >= 0; --d) acc = fma(acc, sv, es.c[i0 + i][d]);
-              ker[i] = acc * fx_scale;
+              ker[i] = acc;
             }
 #pragma unroll
             for (int i = 0; i < 6; ++i) {
@@ -371,12 +386,17 @@ nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* _
 #pragma unroll
               for (int sq = 0; sq < NSEQ; ++sq) {
                 unsigned* z = zw + 4 * sq * seq_stride + wo;
-                const long long xa = (long long)fixed_point(ga[sq] * ker[i]);
-                const long long xb = (long long)fixed_point(gb[sq] * ker[i]);
-                atomicAdd(z, (unsigned)xa & 0xffffu);
-                atomicAdd(z + 128, (unsigned)(xa >> 16));
-                atomicAdd(z + 256, (unsigned)xb & 0xffffu);
-                atomicAdd(z + 384, (unsigned)(xb >> 16));
+                // X = rint(g ker) by one FMA into the 1.5 2^52 binade (one rounding); its low
+                // 16 bits and X >> 16 straight from the two words of the result
+                const double da = fma(ga[sq], ker[i], 6755399441055744.0);
+                const double db = fma(gb[sq], ker[i], 6755399441055744.0);
+                const unsigned la = (unsigned)__double2loint(da), lb = (unsigned)__double2loint(db);
+                const unsigned ha = (unsigned)(__double2hiint(da) - 0x43380000);
+                const unsigned hb = (unsigned)(__double2hiint(db) - 0x43380000);
+                atomicAdd(z, la & 0xffffu);
+                atomicAdd(z + 128, __funnelshift_r(la, ha, 16));
+                atomicAdd(z + 256, lb & 0xffffu);
+                atomicAdd(z + 384, __funnelshift_r(lb, hb, 16));
               }
             }
           }
@@ -553,7 +573,7 @@ int launch_bin_sums_nufft(const Geometry& g, const Workspace& ws, int logn, cons
     if (e != cudaSuccess) return set_cuda_error(e, "nufft attributes", __FILE__, __LINE__);
     kern<<<(unsigned)grid, kNuThreads, smem, s>>>(g.Nl, logn, ws.pay, ws.npieces, ws.pmax, ws.piece_start,
                                                   ws.piece_len, dinv, reinterpret_cast<const double2*>(tw),
-                                                  es_poly(), ws.partial, ws.wsum);
+                                                  es_poly(), ws.partial, ws.wsum, kBalanceMin);
     e = cudaGetLastError();
     if (e != cudaSuccess) return set_cuda_error(e, "nufft launch", __FILE__, __LINE__);
     count_launches(1);
