@@ -211,14 +211,12 @@ __device__ void fft_all(double2* zs, int seq_stride, int logn, const double2* __
 
 constexpr int kMaxTw = 8192 / 16;  // twiddles of the largest grid (Nl = 2048)
 constexpr int kMaxNl = 2048;
-constexpr int kOrderChunk = 8192;  // points ordered at a time (16-bit order indices)
-constexpr int kBalanceMin = 4096;  // smallest chunk given the bank-balanced order
 
-// Shared-memory bytes of a launch: the grids, then the twiddles e^{2 pi i j/n} (j < n/16),
-// 1/Psi(m) and the bank-balanced point order.
+// Shared-memory bytes of a launch: the grids, then the twiddles e^{2 pi i j/n} (j < n/16)
+// and 1/Psi(m).
 size_t nufft_smem_bytes(int logn, int nseq) {
   const size_t n = (size_t)1 << logn;
-  return 16 * nseq * (n + n / 16) + 16 * kMaxTw + 8 * kMaxNl + 2 * kOrderChunk;
+  return 16 * nseq * (n + n / 16) + 16 * kMaxTw + 8 * kMaxNl;
 }
 
 // V = hi 2^16 + lo (|V| < 2^51) as a double, exactly.
@@ -243,7 +241,7 @@ __global__ void __launch_bounds__(kNuThreads, 1)
 nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* __restrict__ npieces_p,
                   int64_t pmax, const int64_t* __restrict__ piece_start, const int* __restrict__ piece_len,
                   const double* __restrict__ dinv, const double2* __restrict__ tw, const EsPoly es,
-                  double* __restrict__ partial, double* __restrict__ wsum, int balance_min) {
+                  double* __restrict__ partial, double* __restrict__ wsum) {
   constexpr int NSEQ = KP / 2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ unsigned long long red[2];
@@ -253,9 +251,6 @@ nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* _
   unsigned* zw = reinterpret_cast<unsigned*>(smem_raw);
   double2* tws = reinterpret_cast<double2*>(smem_raw + (size_t)16 * NSEQ * seq_stride);
   double* dinvs = reinterpret_cast<double*>(tws + kMaxTw);
-  uint16_t* order = reinterpret_cast<uint16_t*>(dinvs + kMaxNl);
-  __shared__ unsigned bcnt[32], boff[33];
-  __shared__ int bmax;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   for (int i = threadIdx.x; i < ng; i += blockDim.x) tws[i] = tw[i];
   for (int m = threadIdx.x; m < Nl; m += blockDim.x) dinvs[m] = dinv[m];
@@ -272,8 +267,20 @@ nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* _
     // spread runs in fixed point of step 2^(e - 46), 2^e >= the bound -- integer
     // reductions, so the grid (and every result) does not depend on the order of the adds.
     unsigned long long mbits = 0ull;
-    for (int p = threadIdx.x; p < len; p += blockDim.x)
-      mbits = max(mbits, (unsigned long long)__double_as_longlong(fabs(rec0[(size_t)kRec * p + 2])));
+    {
+      const int bd = blockDim.x;
+      int p = threadIdx.x;
+      for (; p + 3 * bd < len; p += 4 * bd) {  // four loads in flight
+        const double a0 = rec0[(size_t)kRec * p + 2], a1 = rec0[(size_t)kRec * (p + bd) + 2];
+        const double a2 = rec0[(size_t)kRec * (p + 2 * bd) + 2], a3 = rec0[(size_t)kRec * (p + 3 * bd) + 2];
+        mbits = max(max(mbits, (unsigned long long)__double_as_longlong(fabs(a0))),
+                    (unsigned long long)__double_as_longlong(fabs(a1)));
+        mbits = max(max(mbits, (unsigned long long)__double_as_longlong(fabs(a2))),
+                    (unsigned long long)__double_as_longlong(fabs(a3)));
+      }
+      for (; p < len; p += bd)
+        mbits = max(mbits, (unsigned long long)__double_as_longlong(fabs(rec0[(size_t)kRec * p + 2])));
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) mbits = max(mbits, __shfl_xor_sync(0xffffffffu, mbits, o));
     if (threadIdx.x == 0) red[0] = 0ull;
@@ -303,56 +310,30 @@ nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* _
     for (int kp = 0; kp < 4; kp += KP) {
       for (int i = threadIdx.x; i < NSEQ * seq_stride; i += blockDim.x) zs[i] = make_double2(0.0, 0.0);
       __syncthreads();
-      for (int c0 = 0; c0 < len; c0 += kOrderChunk) {
-        // Bank-balanced order: bucket the chunk's points by (first cell) mod 32, then round r
-        // of a warp gives lane l the r-th point of bucket l, so the 32 lanes start on 32
-        // different banks and every one of their reductions is conflict-free.
-        const int clen = min(kOrderChunk, len - c0);
-        const double* rc = rec0 + (size_t)kRec * c0;
-        // small chunks keep their record order (lane l of round r takes point 32 r + l): the
-        // ordering passes would cost more than the bank conflicts they remove
-        const bool balanced = clen >= balance_min;
-        if (balanced) {
-          if (threadIdx.x < 32) bcnt[threadIdx.x] = 0u;
-          __syncthreads();
-          for (int p = threadIdx.x; p < clen; p += blockDim.x)
-            atomicAdd(&bcnt[(int)floor(rc[(size_t)kRec * p] * u_per_rad) & 31], 1u);
-          __syncthreads();
-          if (warp == 0) {
-            const unsigned c = bcnt[lane];
-            unsigned x = c;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-              const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
-              if (lane >= o) x += y;
-            }
-            unsigned mx = c;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-            boff[lane] = x - c;
-            bcnt[lane] = x - c;  // cursor
-            if (lane == 31) boff[32] = x;
-            if (lane == 0) bmax = (int)mx;
-          }
-          __syncthreads();
-          for (int p = threadIdx.x; p < clen; p += blockDim.x)
-            order[atomicAdd(&bcnt[(int)floor(rc[(size_t)kRec * p] * u_per_rad) & 31], 1u)] = (uint16_t)p;
-          __syncthreads();
+      {
+        // Points in record order, lane l of round r taking point 32 r + l.  (An order that
+        // starts the lanes of a warp on 32 different banks removed 90 % of the reductions'
+        // bank conflicts but was measured no faster.)  The next round's record is loaded
+        // while the current point is spread.
+        const int rounds = (len + 31) >> 5;
+        int r = warp;
+        double2 nx0 = make_double2(0.0, 0.0), nx1 = make_double2(0.0, 0.0);
+        if (r < rounds && 32 * r + lane < len) {
+          const double2* rec = reinterpret_cast<const double2*>(rec0 + (size_t)kRec * (32 * r + lane));
+          nx0 = rec[0];
+          nx1 = rec[1];
         }
-        const int rounds = balanced ? bmax : (clen + 31) >> 5;
-        for (int r = warp; r < rounds; r += nwarps) {
-          int pnt;
-          if (balanced) {
-            const unsigned idx = boff[lane] + (unsigned)r;
-            if (idx >= boff[lane + 1]) continue;
-            pnt = order[idx];
-          } else {
-            pnt = 32 * r + lane;
-            if (pnt >= clen) continue;
+        for (; r < rounds; r += nwarps) {
+          const int pnt = 32 * r + lane;
+          const double phi = nx0.x;  // in [0, 2 pi): the sort's azimuth record
+          const double2 r1 = nx1;    // (w, t)
+          const int pn = pnt + 32 * nwarps;
+          if (pn < len) {
+            const double2* rec = reinterpret_cast<const double2*>(rec0 + (size_t)kRec * pn);
+            nx0 = rec[0];
+            nx1 = rec[1];
           }
-          const double2* rec = reinterpret_cast<const double2*>(rc + (size_t)kRec * pnt);
-          const double phi = rec[0].x;  // in [0, 2 pi): the sort's azimuth record
-          const double2 r1 = rec[1];     // (w, t)
+          if (pnt >= len) continue;
           const double u = phi * u_per_rad;
           const double fl = floor(u);
           const double sv = 2.0 * (u - fl) - 1.0;
@@ -573,7 +554,7 @@ int launch_bin_sums_nufft(const Geometry& g, const Workspace& ws, int logn, cons
     if (e != cudaSuccess) return set_cuda_error(e, "nufft attributes", __FILE__, __LINE__);
     kern<<<(unsigned)grid, kNuThreads, smem, s>>>(g.Nl, logn, ws.pay, ws.npieces, ws.pmax, ws.piece_start,
                                                   ws.piece_len, dinv, reinterpret_cast<const double2*>(tw),
-                                                  es_poly(), ws.partial, ws.wsum, kBalanceMin);
+                                                  es_poly(), ws.partial, ws.wsum);
     e = cudaGetLastError();
     if (e != cudaSuccess) return set_cuda_error(e, "nufft launch", __FILE__, __LINE__);
     count_launches(1);
