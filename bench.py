@@ -478,8 +478,9 @@ def main(argv=None):
                          "~/.cache/directsht_b200/autotune.json)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-fp64-compare", action="store_true")
-    ap.add_argument("--bin-sums", default="nufft", choices=["nufft", "tc"],
-                    help="bin sums of the mixed level: type-1 NUFFT (default) or direct tensor-core sums")
+    ap.add_argument("--bin-sums", default="auto", choices=["auto", "nufft", "tc"],
+                    help="bin sums of the mixed level: type-1 NUFFT, direct tensor-core sums, or the "
+                         "library's choice by points per bin key (default)")
     ap.add_argument("--maps-per-pass", type=int, default=0, help="DSHT_TUNE_MAPS_PER_PASS (0: automatic)")
     ap.add_argument("--batch", type=int, default=None,
                     help="point sets per step for the headline (dsht_enqueue_batch); default 4 for c2, else 1")
@@ -574,6 +575,9 @@ def main(argv=None):
     if args.maps_per_pass:
         d.tune(maps_per_pass=args.maps_per_pass)
     d.tune(bin_sums=args.bin_sums)
+    # the method that runs: AUTO takes the NUFFT from 512 points per bin key (DSHT_TUNE_BIN_SUMS)
+    bin_method = args.bin_sums if args.bin_sums != "auto" else (
+        "nufft" if N >= 512 * 4 * (Nx - 1) else "tc")
     batch = args.batch if args.batch is not None else (4 if args.workload == "c2" else 1)
     if maps > 1 or w_dtype != L.DSHT_W_F64:
         batch = 1
@@ -675,7 +679,7 @@ def main(argv=None):
             return {"kernel": "count/scan/scatter (counting sort by bin)", "bound": "hbm", "achieved": a,
                     "peak": hbm_peak, "unit": "GB/s", "frac": a / hbm_peak, "peak_source": peak_src,
                     "algorithmic": "24 B of inputs read + 32 B of sorted record written per point"}
-        if name == "bin_sums" and args.precision != "fp64" and args.bin_sums == "nufft":
+        if name == "bin_sums" and args.precision != "fp64" and bin_method == "nufft":
             # the NUFFT kernel's own FP64 work: per point 132 DFMA of kernel values, 48
             # products and fixed-point conversions of the spread, ~50 for atan2 and the
             # Hermite weights; per piece two complex FFTs of n cells (5 n log2 n each)
@@ -720,7 +724,8 @@ def main(argv=None):
     roofs = {n: stage_roof(n, ms) for n, ms in stages.items()}
     top = max(stages, key=stages.get)
     roof = dict(roofs[top] or {"kernel": top, "bound": None})
-    roof["traffic"] = dram_traffic(top, args.precision, N, d.Nlm, Nx)
+    roof["traffic"] = dram_traffic(top, args.precision + (":tc" if top == "bin_sums" and bin_method == "tc" else ""),
+                                   N, d.Nlm, Nx)
     roof["stage_ms"] = stages[top]
 
     # End to end from pinned host buffers: inputs copied in and alm copied out every step.
@@ -840,10 +845,10 @@ def main(argv=None):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": ("f64" if args.precision != "mixed" else
-                      "f64 NUFFT sums + i8 digit-table contraction + f64" if args.bin_sums == "nufft" else
+                      "f64 NUFFT sums + i8 digit-table contraction + f64" if bin_method == "nufft" else
                       "i8 tensor sums + i8 digit-table contraction + f64"), "data": "synthetic",
             "config": {"workload": spec["name"], "Nl": Nl, "Nx": Nx, "N": N, "maps": maps,
-                       "point_sets_per_step": batch, "precision": args.precision, "bin_sums": args.bin_sums,
+                       "point_sets_per_step": batch, "precision": args.precision, "bin_sums": bin_method,
                        "l2": f"inputs ({(th.nbytes + ph.nbytes + w.nbytes) / 1e6:.0f} MB) and tables "
                              f"({16 * d.Nlm * Nx / 1e9:.1f} GB FP64) exceed L2 every step",
                        "parallelism": f"replicas x{world}"},

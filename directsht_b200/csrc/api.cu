@@ -117,19 +117,27 @@ size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* ba
   return off;
 }
 
-bool plan_uses_nufft(const dsht_plan_s* p) { return p->nu_dinv && p->tune_bin_sums != DSHT_BIN_SUMS_TC; }
+// The mixed levels' bin-sum method for a call whose workspace is laid out for N points.
+// AUTO takes the NUFFT sums when there are at least kNufftMinPerKey points per bin key on
+// average: a NUFFT piece pays a fixed FFT (about 15 us of one SM at Nl = 1024) and little
+// per point, the tensor-core sums little per piece and more per point (measured crossover
+// near 500 points per piece); fewer points per key take the tensor-core sums.
+bool plan_uses_nufft(const dsht_plan_s* p, int64_t N) {
+  if (!p->nu_dinv || p->tune_bin_sums == DSHT_BIN_SUMS_TC) return false;
+  return p->tune_bin_sums == DSHT_BIN_SUMS_NUFFT || N >= (int64_t)kNufftMinPerKey * p->g.nkeys;
+}
 
 // Pieces of the direct sums stay at or below 2048 points (the tensor path's S32 sums stay
 // exact); the NUFFT sums pay one FFT per piece, so theirs are larger.
 int plan_piece_max(const dsht_plan_s* p, int64_t N) {
-  const bool nufft = plan_route(p, N).tc && plan_uses_nufft(p);
+  const bool nufft = plan_route(p, N).tc && plan_uses_nufft(p, N);
   int pm = p->tune_piece_max > 0 ? p->tune_piece_max : nufft ? kNufftPiece : default_piece_max(p->g, N);
   if (!nufft && pm > 2048) pm = 2048;
   return pm;
 }
 
 int launch_bin_sums_mixed(const dsht_plan_s* p, Workspace& w2, cudaStream_t s) {
-  if (plan_uses_nufft(p)) {
+  if (plan_uses_nufft(p, w2.npts)) {
     w2.partial_f32 = 0;
     return launch_bin_sums_nufft(p->g, w2, p->nu_logn, p->nu_dinv, p->nu_tw, s);
   }
@@ -283,7 +291,7 @@ int run_pipeline(dsht_plan_s* p, const double* theta, const double* phi, const d
                         int mode, double* alm, const Workspace& ws, cudaStream_t s) {
   p->ev_n = 0;
   prof_mark(p, DSHT_STAGE_POINTS, s);
-  launch_points(p->g, theta, phi, w, 0, N, mode, ws, s, plan_route(p, N).tc && plan_uses_nufft(p));
+  launch_points(p->g, theta, phi, w, 0, N, mode, ws, s, plan_route(p, N).tc && plan_uses_nufft(p, ws.npts));
   prof_mark(p, DSHT_STAGE_BIN_SUMS, s);
   return run_after_sort(p, N, mode, alm, ws, s, true);
 }
@@ -314,7 +322,7 @@ static int run_class_digits(dsht_plan_s* p, const Item* items, const std::vector
       Workspace wp = ws;
       if (!(li + 1 < list.size() && items[list[li + 1]].same_points)) wp.sidx = nullptr;
       launch_points(g, item.theta, item.phi, item.w, item.w_f32, item.N, mode, wp, s,
-                    rt.tc && plan_uses_nufft(p));
+                    rt.tc && plan_uses_nufft(p, ws.npts));
       *sorted_item = i;
     }
     prof_mark(p, DSHT_STAGE_BIN_SUMS, s);
@@ -418,7 +426,7 @@ int run_items(dsht_plan_s* p, const Item* items, int n, int mode, const Workspac
         Workspace wp = ws;
         if (!(li + 1 < list.size() && items[list[li + 1]].same_points)) wp.sidx = nullptr;
         launch_points(g, item.theta, item.phi, item.w, item.w_f32, item.N, mode, wp, s,
-                      mixed && plan_uses_nufft(p));
+                      mixed && plan_uses_nufft(p, ws.npts));
         sorted_item = i;
       }
       prof_mark(p, DSHT_STAGE_BIN_SUMS, s);

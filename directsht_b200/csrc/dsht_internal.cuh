@@ -132,6 +132,7 @@ void nufft_host_tables(int Nl, int logn, std::vector<double>& dinv, std::vector<
 int launch_bin_sums_nufft(const Geometry& g, const Workspace& ws, int logn, const double* dinv, const double* tw,
                           cudaStream_t s);
 constexpr int kNufftPiece = 8192;  // default points per piece of the NUFFT sums
+constexpr int kNufftMinPerKey = 512;  // AUTO bin sums: NUFFT from this many points per key on average
 int tc_inner_factor(int Nl);
 // FP64 fold of the current map into ws.fold, and the live-tile flags of the contractions.
 void launch_fold(const Geometry& g, const Workspace& ws, cudaStream_t s);
@@ -263,7 +264,7 @@ struct Item {
 // Bin sums of a tensor-core-route transform: the NUFFT (default) or the tensor-core direct
 // sums; sets w2.partial_f32 to the layout written.
 int launch_bin_sums_mixed(const dsht_plan_s* p, Workspace& w2, cudaStream_t s);
-bool plan_uses_nufft(const dsht_plan_s* p);
+bool plan_uses_nufft(const dsht_plan_s* p, int64_t N);
 // Runs the items in order; every finished item's flags are OR-ed into ws.all_flags.
 int run_items(dsht_plan_s* p, const Item* items, int n, int mode, const Workspace& ws, cudaStream_t s);
 // After the stream has been synchronised: fold the stage events into the plan's totals.

@@ -70,11 +70,12 @@ enum {
 /* Arithmetic of a plan's transforms.
  *   DSHT_PREC_FP64  : FP64 CUDA-core per-bin sums and FP64 tables; agrees with the
  *                     reference's numpy path to about 1e-15 (tested at <= 1e-12 x max|alm|).
- *   DSHT_PREC_MIXED : per-bin sums by a type-1 non-uniform FFT in FP64 (each bin's points
+ *   DSHT_PREC_MIXED : per-bin sums (see DSHT_TUNE_BIN_SUMS for the choice) by a type-1
+ *                     non-uniform FFT in FP64 (each bin's points
  *                     spread onto a periodic grid of 4 x 2^ceil(log2 Nl) cells with a width-12
  *                     "exponential of semicircle" kernel, FFT, division by the kernel's Fourier
- *                     transform; error about 5e-12 of the bin's sum of |w h_k|) -- or, with
- *                     DSHT_TUNE_BIN_SUMS = DSHT_BIN_SUMS_TC, the direct tcgen05 tensor-core
+ *                     transform; error about 5e-12 of the bin's sum of |w h_k|) -- or the
+ *                     direct tcgen05 tensor-core
  *                     sums (operands quantised to 22-bit fixed point, split into int8 slices,
  *                     slice products accumulated exactly in S32 and combined in FP64;
  *                     unbiased, about 5.6e-8 rms per product) -- and a
@@ -111,8 +112,10 @@ int dsht_get_precision(dsht_plan_t plan, int* precision);
  * tensor-core, cap it at 2048; the NUFFT sums default to 8192).  DSHT_TUNE_MAPS_PER_PASS:
  * maps or point sets that share one read of the tables in a multi-transform call, 1..8,
  * 0 = the most (8; the tensor-core contraction only: the FP64 one reads the tables once per
- * map).  DSHT_TUNE_BIN_SUMS: the bin sums of the mixed levels, DSHT_BIN_SUMS_NUFFT (the
- * default, AUTO) or DSHT_BIN_SUMS_TC (the direct int8-slice tensor-core sums).  Workspace
+ * map).  DSHT_TUNE_BIN_SUMS: the bin sums of the mixed levels, DSHT_BIN_SUMS_NUFFT or
+ * DSHT_BIN_SUMS_TC (the direct int8-slice tensor-core sums); AUTO (the default) takes the
+ * NUFFT sums when a call has at least 512 points per bin key on average (N >= 2048 (Nx - 1)),
+ * where its fixed cost per bin piece pays off, and the tensor-core sums below.  Workspace
  * sizes depend on all three: query them after tuning. */
 enum { DSHT_TUNE_PIECE_MAX = 1, DSHT_TUNE_MAPS_PER_PASS = 2, DSHT_TUNE_BIN_SUMS = 3 };
 /* Values of DSHT_TUNE_BIN_SUMS: the bin-sum method of the mixed levels. */

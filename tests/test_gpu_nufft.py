@@ -6,7 +6,8 @@ deconvolution), error about 5e-12 of the bin's sum |g_k|.  With the FP64 tables 
 contraction (mixed_f64_tables) that is the only approximation, so those results must agree
 with the plain FP64 transform to 1e-10 of max|alm|; with the digit tables (mixed) to 1e-8.
 The spread adds 64-bit fixed-point values with integer atomics, so results are bitwise
-repeatable.  The direct tensor-core sums stay selectable (tune(bin_sums='tc'))."""
+repeatable.  The direct tensor-core sums stay selectable (tune(bin_sums='tc')); AUTO picks
+by the average number of points per bin key."""
 import numpy as np
 import pytest
 
@@ -38,6 +39,7 @@ def test_nufft_bin_sums_vs_fp64(Nl, Nx, N):
     ref = d(th, ph, w)
     d.set_precision("mixed_f64_tables")
     assert d.tune()["bin_sums"] == "auto"
+    assert d.tune(bin_sums="nufft")["bin_sums"] == "nufft"
     a = d(th, ph, w)
     assert _rel(a, ref) <= 1e-10
     assert np.array_equal(a, d(th, ph, w))  # integer spreading: bitwise repeatable
@@ -52,6 +54,7 @@ def test_nufft_vs_oracle_and_tensor_core_sums():
     th, ph, w = _sky(N, 5)
     ref = O.direct_sht(O.build_tables(Nl, Nx), th, ph, w)
     d = DirectSHT(Nl, Nx, precision="mixed_f64_tables")
+    d.tune(bin_sums="nufft")
     e_nufft = _rel(d(th, ph, w), ref)
     assert d.tune(bin_sums="tc")["bin_sums"] == "tc"
     e_tc = _rel(d(th, ph, w), ref)
@@ -70,6 +73,7 @@ def test_nufft_weights_without_the_fixed_point_limits(wkind):
     d = DirectSHT(Nl, Nx)
     ref = d(th, ph, w)
     d.set_precision("mixed_f64_tables")
+    d.tune(bin_sums="nufft")
     assert _rel(d(th, ph, w), ref) <= (1e-9 if wkind == "normal" else 1e-10)
 
 
@@ -85,7 +89,7 @@ def test_nufft_piece_sizes_and_heavy_bins(piece):
     d = DirectSHT(Nl, Nx)
     ref = d(th, ph, w)
     d.set_precision("mixed_f64_tables")
-    d.tune(piece_max=piece)
+    d.tune(piece_max=piece, bin_sums="nufft")
     assert _rel(d(th, ph, w), ref) <= 1e-10
 
 
@@ -94,6 +98,20 @@ def test_nufft_many_maps_match_single_calls():
     th, ph, _ = _sky(N, 21)
     W = np.random.default_rng(22).normal(1.0, 0.3, (5, N))
     d = DirectSHT(Nl, Nx, precision="mixed")
+    d.tune(bin_sums="nufft")
     A = d.call_maps(th, ph, W)
     for k in range(5):
         assert _rel(A[k], d(th, ph, W[k])) <= 1e-12
+
+
+def test_auto_bin_sums_follow_points_per_key():
+    """AUTO takes the NUFFT sums from 512 points per bin key on average and the tensor-core
+    sums below: the two calls here agree with the forced methods bit for bit."""
+    Nl, Nx = 64, 32  # 4 x 31 = 124 keys: the NUFFT from 63488 points
+    th, ph, w = _sky(100000, 31)
+    d = DirectSHT(Nl, Nx, precision="mixed")
+    for N, method in ((100000, "nufft"), (20000, "tc")):
+        a = d(th[:N], ph[:N], w[:N])
+        d.tune(bin_sums=method)
+        assert np.array_equal(a, d(th[:N], ph[:N], w[:N])), (N, method)
+        d.tune(bin_sums="auto")
