@@ -215,13 +215,17 @@ def cpu_reference_run(spec, sample_n, steps, warmup, seed=0, probe_n=1000):
     sec = float(np.mean(times))
     t_fixed = float(np.median(fixed))
     per_point = max(sec - t_fixed, 0.0) / sample_n
-    t_full = t_fixed + per_point * N_full if N_full else None
+    # a split is only resolved when the sample step clearly exceeds the fixed part (the probe
+    # steps' noise is a few percent of the fixed part)
+    resolved = sec > 1.05 * t_fixed
+    t_full = t_fixed + per_point * N_full if (N_full and resolved) else None
     return {"value": sample_n * Nl / sec, "unit": "points*ell/s", "cores": os.cpu_count(),
             "kind": "reference", "seconds_per_step": sec, "table_build_s": t_tables, "dmatrix_build_s": t_dmat,
             "sample_points": sample_n, "same_config": sample_n == N_full,
             "split": {"fixed_s_per_step": t_fixed, "per_point_s": per_point,
                       "probe": f"{max(warmup, 1)} steps of {probe_n} points (the warm-up steps)",
-                      "note": "fixed = four do_transform calls and the alm rotation at ~no points"},
+                      "note": "fixed = four do_transform calls and the alm rotation at ~no points",
+                      "resolved": resolved},
             "at_config": None if t_full is None else {
                 "N": N_full, "seconds_per_transform": t_full, "value": N_full * Nl / t_full,
                 "how": "fixed + per_point x N from this run's split (extrapolated, not timed)"},
