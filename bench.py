@@ -469,7 +469,7 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--e2e-steps", type=int, default=30)
     ap.add_argument("--cpu-sample", type=int, default=1_000_000,
                     help="points of the cpu_baseline step (the reference's C transform on the host cores)")
     ap.add_argument("--ref-sample", type=int, default=1_000_000,

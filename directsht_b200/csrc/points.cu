@@ -306,9 +306,20 @@ scatter_kernel(Geometry g, const double* __restrict__ theta, const double* __res
       if (k[u] != DSHT_KEY_DROP) atomicAdd(&loc[k[u]], 1u);
   }
   __syncthreads();
-  for (int k = threadIdx.x; k < g.nkeys; k += blockDim.x) {
-    const uint32_t c = loc[k];
-    if (c) loc[k] = atomicAdd(&cursor[k], c);
+  // one global reservation per (block, key); four of a thread's in flight at once
+  for (int k0 = threadIdx.x; k0 < g.nkeys; k0 += 4 * blockDim.x) {
+    uint32_t c[4], r[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int k = k0 + u * blockDim.x;
+      c[u] = k < g.nkeys ? loc[k] : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (c[u]) r[u] = atomicAdd(&cursor[k0 + u * blockDim.x], c[u]);
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (c[u]) loc[k0 + u * blockDim.x] = r[u];
   }
   __syncthreads();
   const int polar_key0 = 2 * g.nbins;
