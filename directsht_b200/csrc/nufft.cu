@@ -55,11 +55,8 @@ constexpr int kNuThreads = 512;
 
 __device__ __forceinline__ int padi(int i) { return i + (i >> 4); }
 
-// rint(x) as a two's-complement integer for |x| < 2^51: one DFMA puts x into the binade of
-// 1.5 2^52, whose low bits are then the rounded integer (no conversion instruction).
-__device__ __forceinline__ unsigned long long fixed_point(double x) {
-  return (unsigned long long)(__double_as_longlong(x + 6755399441055744.0) - 0x4338000000000000ll);
-}
+// v (|v| < 2^51) as a double, exactly, through the binade of 1.5 2^52 (no conversion
+// instruction).
 __device__ __forceinline__ double from_fixed(long long v) {
   return __longlong_as_double(v + 0x4338000000000000ll) - 6755399441055744.0;
 }
@@ -244,7 +241,8 @@ nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* _
                   double* __restrict__ partial, double* __restrict__ wsum) {
   constexpr int NSEQ = KP / 2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ unsigned long long red[2];
+  __shared__ unsigned long long red[1];
+  __shared__ double wred[32];
   const int n = 1 << logn, ng = n >> 4;
   const int seq_stride = n + (n >> 4);  // double2 slots per sequence
   double2* zs = reinterpret_cast<double2*>(smem_raw);
@@ -261,45 +259,47 @@ nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* _
     const int64_t start = piece_start[piece];
     const int len = piece_len[piece];
     const double* rec0 = pay + (size_t)kRec * start;
-    // A bound of sum |w| over the piece that does not depend on the order of its points (the
-    // sort places the points of a key in any order): M = max |w|, then the exact integer
-    // sum of rint(|w| 2^40 / M).  It bounds every grid value (|h_k| <= 1, psi <= 1), so the
-    // spread runs in fixed point of step 2^(e - 46), 2^e >= the bound -- integer
-    // reductions, so the grid (and every result) does not depend on the order of the adds.
+    // sum |w| of the piece (one pass, four loads in flight) with a margin for its own rounding,
+    // and max |w| (only to detect non-finite weights).  The bound 2^e above it bounds every
+    // grid value (|h_k| <= 1, psi <= 1), so the spread runs in fixed point of step 2^(e - 46)
+    // with integer reductions: the grid does not depend on the order of the adds.  The sum
+    // itself is summed in whatever order the sort left the points; e can only differ between
+    // runs when the sum lies within its rounding (~len 2^-53 relative) of a power of two.
     unsigned long long mbits = 0ull;
+    double wabs = 0.0;
     {
       const int bd = blockDim.x;
       int p = threadIdx.x;
-      for (; p + 3 * bd < len; p += 4 * bd) {  // four loads in flight
-        const double a0 = rec0[(size_t)kRec * p + 2], a1 = rec0[(size_t)kRec * (p + bd) + 2];
-        const double a2 = rec0[(size_t)kRec * (p + 2 * bd) + 2], a3 = rec0[(size_t)kRec * (p + 3 * bd) + 2];
-        mbits = max(max(mbits, (unsigned long long)__double_as_longlong(fabs(a0))),
-                    (unsigned long long)__double_as_longlong(fabs(a1)));
-        mbits = max(max(mbits, (unsigned long long)__double_as_longlong(fabs(a2))),
-                    (unsigned long long)__double_as_longlong(fabs(a3)));
+      for (; p + 3 * bd < len; p += 4 * bd) {
+        const double a0 = fabs(rec0[(size_t)kRec * p + 2]), a1 = fabs(rec0[(size_t)kRec * (p + bd) + 2]);
+        const double a2 = fabs(rec0[(size_t)kRec * (p + 2 * bd) + 2]), a3 = fabs(rec0[(size_t)kRec * (p + 3 * bd) + 2]);
+        wabs += (a0 + a1) + (a2 + a3);
+        mbits = max(max(mbits, (unsigned long long)__double_as_longlong(a0)),
+                    max((unsigned long long)__double_as_longlong(a1),
+                        max((unsigned long long)__double_as_longlong(a2), (unsigned long long)__double_as_longlong(a3))));
       }
-      for (; p < len; p += bd)
-        mbits = max(mbits, (unsigned long long)__double_as_longlong(fabs(rec0[(size_t)kRec * p + 2])));
+      for (; p < len; p += bd) {
+        const double a = fabs(rec0[(size_t)kRec * p + 2]);
+        wabs += a;
+        mbits = max(mbits, (unsigned long long)__double_as_longlong(a));
+      }
     }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) mbits = max(mbits, __shfl_xor_sync(0xffffffffu, mbits, o));
+    for (int o = 16; o > 0; o >>= 1) {
+      mbits = max(mbits, __shfl_xor_sync(0xffffffffu, mbits, o));
+      wabs += __shfl_xor_sync(0xffffffffu, wabs, o);
+    }
     if (threadIdx.x == 0) red[0] = 0ull;
     __syncthreads();
-    if ((threadIdx.x & 31) == 0) atomicMax(&red[0], mbits);
+    if ((threadIdx.x & 31) == 0) {
+      atomicMax(&red[0], mbits);
+      wred[threadIdx.x >> 5] = wabs;
+    }
     __syncthreads();
-    const double wmax = __longlong_as_double((long long)red[0]);
-    const double to_int = wmax > 0.0 ? 0x1p40 / wmax : 0.0;
-    unsigned long long isum = 0ull;
-    for (int p = threadIdx.x; p < len; p += blockDim.x)
-      isum += fixed_point(fabs(rec0[(size_t)kRec * p + 2]) * to_int);
+    double wsum_p = 0.0;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) isum += __shfl_xor_sync(0xffffffffu, isum, o);
-    if (threadIdx.x == 0) red[1] = 0ull;
-    __syncthreads();
-    if ((threadIdx.x & 31) == 0) atomicAdd(&red[1], isum);
-    __syncthreads();
-    // each rounding is at most 1/2: (isum + len) 2^-40 M >= sum |w|
-    const double wbound = wmax > 0.0 ? (double)(red[1] + (unsigned long long)len) * (wmax * 0x1p-40) : 0.0;
+    for (int i = 0; i < kNuThreads / 32; ++i) wsum_p += wred[i];
+    const double wbound = wsum_p * (1.0 + (double)len * 0x1p-52);
     if (threadIdx.x == 0) wsum[piece] = wbound;
     int ebound = 0;
     if (wbound > 0.0) frexp(wbound, &ebound);  // wbound < 2^ebound
