@@ -67,24 +67,24 @@ __device__ __forceinline__ double2 cmul2(double2 a, double2 b) {
 
 // cos, sin of 2 pi e / 16 for a compile-time e (after unrolling).
 __device__ __forceinline__ double cos16(int e) {
-  constexpr double C1 = 0.92387953251128675613, C2 = 0.70710678118654752440, C3 = 0.38268343236508977173;
+  constexpr double kCos1 = 0.92387953251128675613, kCos2 = 0.70710678118654752440, kCos3 = 0.38268343236508977173;
   switch (e & 15) {
     case 0: return 1.0;
-    case 1: return C1;
-    case 2: return C2;
-    case 3: return C3;
+    case 1: return kCos1;
+    case 2: return kCos2;
+    case 3: return kCos3;
     case 4: return 0.0;
-    case 5: return -C3;
-    case 6: return -C2;
-    case 7: return -C1;
+    case 5: return -kCos3;
+    case 6: return -kCos2;
+    case 7: return -kCos1;
     case 8: return -1.0;
-    case 9: return -C1;
-    case 10: return -C2;
-    case 11: return -C3;
+    case 9: return -kCos1;
+    case 10: return -kCos2;
+    case 11: return -kCos3;
     case 12: return 0.0;
-    case 13: return C3;
-    case 14: return C2;
-    default: return C1;
+    case 13: return kCos3;
+    case 14: return kCos2;
+    default: return kCos1;
   }
 }
 __device__ __forceinline__ double sin16(int e) { return cos16(e - 4); }

@@ -92,7 +92,7 @@ def test_chebyshev_anchors_match_exp():
 
 
 def test_piece_sums_error_within_bound():
-    """One 2048-point piece of C2-like weights: the fixed-point sums against exact FP64 sums
+    """One 2048-point piece of lognormal(0, 0.5) weights: the fixed-point sums against exact FP64 sums
     of g_k e^{i m phi}, relative to the largest |sum| (the kernel's accuracy claim: below
     1e-7 for pieces of spread weights)."""
     rng = np.random.default_rng(3)
