@@ -24,7 +24,9 @@
 namespace dsht {
 namespace {
 
-constexpr int kStageRow = 36;  // bytes per staging row of fold_digits_kernel (32 used)
+constexpr int kFoldNodes = 16;  // nodes per fold_digits block (32 m x 16 nodes, 512 threads)
+constexpr int kStageRow = kFoldNodes + 4;  // bytes per staging row (a 4-byte pad: lanes store to
+                                           // rows 20 bytes apart, i.e. 32 different banks)
 constexpr double kScaleMargin = 1.01;  // scale > 1.01 x bound: |X| < 2^31 / 1.01 < 2^31 - 2^24
 
 // Smallest e with kScaleMargin * v <= 2^e (v >= 0; 0 for v = 0).
@@ -171,23 +173,24 @@ fold_scale_kernel(int nbins, int Nx, const int* __restrict__ piece_first, const 
   if (threadIdx.x < 2 && red[threadIdx.x]) atomicMax(&cmax[threadIdx.x], red[threadIdx.x]);
 }
 
-// Fold of one map straight into digits.  A block covers 32 m x 32 nodes: warp = node,
-// lane = m while the per-piece sums are read (consecutive m: coalesced), then the digit
-// bytes go through shared memory so that consecutive threads store consecutive nodes.
-// Staging rows (one per (parity, digit, column, K half, m), 32 node bytes each) are 36
-// bytes apart with m fastest, so the 32 lanes of a warp store into 32 different banks.
+// Fold of one map straight into digits.  A block covers 32 m x 16 nodes (512 threads, two
+// blocks per SM, so one block's loads overlap the other's stores): warp = node, lane = m
+// while the per-piece sums are read (consecutive m: coalesced), then the digit bytes go
+// through shared memory so that consecutive threads store consecutive nodes.  Staging rows
+// (one per (parity, digit, column, K half, m), 16 node bytes each) are 20 bytes apart with
+// m fastest, so the 32 lanes of a warp store into 32 different banks.
 // Sums as fold_kernel forms them (set s: A = V0(bin j) + V2(bin j-1), B = dx (V1(bin j) +
 // V3(bin j-1)), V = vr - i vi; even rows A+ + A-, odd rows A+ - A-), stored as B/dx.
 template <typename PT>
-__global__ void __launch_bounds__(1024)
+__global__ void __launch_bounds__(32 * kFoldNodes, 2)
 fold_digits_kernel(int Nl, int Nx, int nbins, int Kp, const int* __restrict__ piece_first,
                    const PT* __restrict__ partial, const unsigned long long* __restrict__ cmax,
                    int16_t* __restrict__ cexp, int map, int ncols, uint8_t* __restrict__ fdig) {
-  // stage[row][36], row = (((par * 4 + d) * 4 + c) * 2 + kh) * 32 + m, byte j of the row
-  // = node j0 + j (dynamic: 72 KB)
+  // stage[row][kStageRow], row = (((par * 4 + d) * 4 + c) * 2 + kh) * 32 + m, byte j of the
+  // row = node j0 + j (dynamic: 2048 rows)
   extern __shared__ __align__(16) uint8_t stage[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int m0 = blockIdx.y * 32, j0 = blockIdx.x * 32;
+  const int m0 = blockIdx.y * 32, j0 = blockIdx.x * kFoldNodes;
   const int m = m0 + lane, j = j0 + warp;
   const int e0 = scale_exp(__longlong_as_double((long long)cmax[0]));
   const int e1 = scale_exp(__longlong_as_double((long long)cmax[1]));
@@ -257,11 +260,12 @@ fold_digits_kernel(int Nl, int Nx, int nbins, int Kp, const int* __restrict__ pi
         }
   }
   __syncthreads();
-  // 2048 rows x 8 words; word w covers 4 nodes of one (par, d, c, kh, m) row.
-  const int nj = min(32, Nx - j0);
-  for (int w = threadIdx.x; w < 32 * 2 * 4 * 4 * 2 * 8; w += blockDim.x) {
-    const int q = w & 7;           // 4-node group
-    const int row = w >> 3;        // (((par * 4 + d) * 4 + c) * 2 + kh) * 32 + ml
+  // 2048 rows x kFoldNodes/4 words; word w covers 4 nodes of one (par, d, c, kh, m) row.
+  constexpr int kWords = kFoldNodes / 4;
+  const int nj = min(kFoldNodes, Nx - j0);
+  for (int w = threadIdx.x; w < 32 * 2 * 4 * 4 * 2 * kWords; w += blockDim.x) {
+    const int q = w % kWords;      // 4-node group
+    const int row = w / kWords;    // (((par * 4 + d) * 4 + c) * 2 + kh) * 32 + ml
     const int ml = row & 31;
     const int kh = (row >> 5) & 1;
     const int c = (row >> 6) & 3;
@@ -326,16 +330,16 @@ void launch_fold_scale(const Geometry& g, const Workspace& ws, unsigned long lon
 void launch_fold_digits(const Geometry& g, const Workspace& ws, const unsigned long long* cmax, int16_t* cexp,
                         int map, int ncols, uint8_t* fdig, cudaStream_t s) {
   const int Kp = digit_kp(g.Nx);
-  dim3 grid((g.Nx + 31) / 32, (g.Nl + 31) / 32);
+  dim3 grid((g.Nx + kFoldNodes - 1) / kFoldNodes, (g.Nl + 31) / 32);
   constexpr int kStageBytes = 32 * 2 * 4 * 4 * 2 * kStageRow;
   cudaFuncSetAttribute(fold_digits_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStageBytes);
   cudaFuncSetAttribute(fold_digits_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStageBytes);
   if (ws.partial_f32)
-    fold_digits_kernel<float><<<grid, 1024, kStageBytes, s>>>(g.Nl, g.Nx, g.nbins, Kp, ws.piece_first,
+    fold_digits_kernel<float><<<grid, 32 * kFoldNodes, kStageBytes, s>>>(g.Nl, g.Nx, g.nbins, Kp, ws.piece_first,
                                                               reinterpret_cast<const float*>(ws.partial), cmax,
                                                               cexp, map, ncols, fdig);
   else
-    fold_digits_kernel<double><<<grid, 1024, kStageBytes, s>>>(g.Nl, g.Nx, g.nbins, Kp, ws.piece_first,
+    fold_digits_kernel<double><<<grid, 32 * kFoldNodes, kStageBytes, s>>>(g.Nl, g.Nx, g.nbins, Kp, ws.piece_first,
                                                                ws.partial, cmax, cexp, map, ncols, fdig);
   count_launches(1);
 }
