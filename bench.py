@@ -339,6 +339,24 @@ def run_batch(args, spec):
     b.run()
     torch.cuda.synchronize()
     launches = lib.dsht_launch_count() - l0
+    # each (Nl, Nx) group alone, eager, with its tuned configuration (where the time goes)
+    group_ms = {}
+    for key in b.groups:
+        sub = TransformBatch.__new__(TransformBatch)
+        sub.__dict__.update(b.__dict__)
+        sub.groups = {key: b.groups[key]}
+        sub.config = {key: b.config[key]}
+        sub.graph = None
+        sub._build()
+        sub.run()
+        torch.cuda.synchronize()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        sub.run()
+        g1.record(stream)
+        torch.cuda.synchronize()
+        group_ms[f"{key[0]}x{key[1]}"] = g0.elapsed_time(g1)
+        del sub
     # accuracy of a sample against FP64 plans (Nl <= 512, whose FP64 tables fit beside the rest)
     fp64 = PlanCache(device=dev, precision="fp64")
     errs = []
@@ -377,11 +395,12 @@ def run_batch(args, spec):
         torch.distributed.destroy_process_group()
     if rank == 0:
         groups = {f"{k[0]}x{k[1]}": {"transforms": len(v), "points": int(sum(b.Ns[i] for i in v)),
-                                       "config": cfg.get(k)} for k, v in b.groups.items()}
+                                       "config": cfg.get(k), "ms_alone": group_ms.get(f"{k[0]}x{k[1]}")}
+                  for k, v in b.groups.items()}
         line = {"metric": "points*ell/s", "value": world * pe / (ms_step / 1e3), "unit": "points*ell/s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "i8 tensor sums + i8 digit-table contraction + f64", "data": "synthetic",
+                "dtype": "f64 NUFFT or i8 tensor-core bin sums (AUTO) + i8 digit-table contraction + f64", "data": "synthetic",
                 "config": {"workload": spec["name"], "transforms": len(ts), "points": int(sum(b.Ns)),
                            "points_ell": pe, "precision": "mixed (compact digit tables only for Nl >= 1024)",
                            "l2": "inputs (GBs) and tables (79 GB) exceed L2", "parallelism": f"replicas x{world}",
@@ -445,7 +464,7 @@ def run_serve(args, spec):
         line = {"metric": "points*ell/s", "value": value, "unit": "points*ell/s", "n_gpus": world,
                 "steps": spec["nreq"], "warmup": len(warm), "ms_per_step": st["mean_ms"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "i8 tensor sums + i8 digit-table contraction + f64", "data": "synthetic",
+                "dtype": "f64 NUFFT or i8 tensor-core bin sums (AUTO) + i8 digit-table contraction + f64", "data": "synthetic",
                 "config": {"workload": spec["name"], "requests": spec["nreq"], "rate_hz": spec["rate"],
                            "points_ell": st["points_ell"], "budget_GB": budget / 1e9, "slots": 8,
                            "plans_resident_GB": cache.resident_bytes() / 1e9, "parallelism": f"replicas x{world}",
