@@ -86,6 +86,7 @@ SIGNATURES = {
     "dsht_launch_count": (ct.c_int64, []),
     "dsht_test_stall_next_contraction": (ct.c_int, []),
     "dsht_test_point_keys": (ct.c_int, [_vp, _vp, _vp, ct.c_int64, ct.c_int, _vp, _vp, _vp]),
+    "dsht_test_nufft_tables": (ct.c_int, [ct.c_int, ct.POINTER(ct.c_int), _dp, _dp]),
     "dsht_mixed_min_points": (ct.c_int64, []),
     "dsht_last_error": (ct.c_char_p, []),
     "dsht_version": (ct.c_char_p, []),

@@ -565,3 +565,16 @@ int launch_bin_sums_nufft(const Geometry& g, const Workspace& ws, int logn, cons
 }
 
 }  // namespace dsht
+
+extern "C" int dsht_test_nufft_tables(int Nl, int* logn, double* poly, double* dinv) {
+  if (Nl < 1 || Nl > 2048 || !logn || !poly || !dinv)
+    return dsht::set_error(DSHT_ERR_INVALID, "invalid arguments");
+  *logn = dsht::nufft_logn(Nl);
+  const dsht::EsPoly& P = dsht::es_poly();
+  for (int i = 0; i < dsht::kEsW; ++i)
+    for (int d = 0; d <= dsht::kEsDeg; ++d) poly[i * (dsht::kEsDeg + 1) + d] = P.c[i][d];
+  std::vector<double> dv, tw;
+  dsht::nufft_host_tables(Nl, *logn, dv, tw);
+  for (int m = 0; m < Nl; ++m) dinv[m] = dv[m];
+  return DSHT_OK;
+}

@@ -300,6 +300,12 @@ int dsht_test_stall_next_contraction(void);
 int dsht_test_point_keys(dsht_plan_t plan, const double* theta, const double* phi, int64_t N, int mode,
                          uint32_t* keys, unsigned* flags, void* stream);
 
+/* Test hook, no counterpart in the reference: the host-side tables of the NUFFT bin sums for
+ * Nl <= 2048 -- *logn = log2 of the grid cells, poly[12][12] the monomial coefficients (in
+ * s = 2f - 1) of the kernel values at the 12 cells next to a point of fractional cell offset
+ * f, dinv[Nl] = 1 / Psi(m).  Needs no GPU. */
+int dsht_test_nufft_tables(int Nl, int* logn, double* poly, double* dinv);
+
 /* Kernels this library has launched in this process (all devices). */
 int64_t dsht_launch_count(void);
 
