@@ -18,8 +18,8 @@
 // converted to monomials on the host; max error 1e-13 of psi(0)).  They are passed as a
 // kernel parameter, so every Horner step is one DFMA with a uniform operand.
 //
-// One CTA per piece (persistent over pieces): an order-independent bound of the piece's
-// sum |w| sets a fixed-point step; the piece's points are spread as 46-bit fixed-point
+// One CTA per piece (persistent over pieces): the power of two above the piece's sum |w|
+// sets a fixed-point step; the piece's points are spread as 46-bit fixed-point
 // values, each added as two native 32-bit shared-memory reductions (low 16 bits, high
 // bits), so the sums are exact and independent of the order of the adds; the planes
 // (bank = cell mod 32) are converted to FP64 in place, then an in-place
