@@ -400,7 +400,7 @@ def run_batch(args, spec):
         line = {"metric": "points*ell/s", "value": world * pe / (ms_step / 1e3), "unit": "points*ell/s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f64 NUFFT or i8 tensor-core bin sums (AUTO) + i8 digit-table contraction + f64", "data": "synthetic",
+                "dtype": "f64 NUFFT, i8 tensor-core or f64 direct bin sums (AUTO) + i8 digit-table contraction + f64", "data": "synthetic",
                 "config": {"workload": spec["name"], "transforms": len(ts), "points": int(sum(b.Ns)),
                            "points_ell": pe, "precision": "mixed (compact digit tables only for Nl >= 1024)",
                            "l2": "inputs (GBs) and tables (79 GB) exceed L2", "parallelism": f"replicas x{world}",
@@ -464,7 +464,7 @@ def run_serve(args, spec):
         line = {"metric": "points*ell/s", "value": value, "unit": "points*ell/s", "n_gpus": world,
                 "steps": spec["nreq"], "warmup": len(warm), "ms_per_step": st["mean_ms"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f64 NUFFT or i8 tensor-core bin sums (AUTO) + i8 digit-table contraction + f64", "data": "synthetic",
+                "dtype": "f64 NUFFT, i8 tensor-core or f64 direct bin sums (AUTO) + i8 digit-table contraction + f64", "data": "synthetic",
                 "config": {"workload": spec["name"], "requests": spec["nreq"], "rate_hz": spec["rate"],
                            "points_ell": st["points_ell"], "budget_GB": budget / 1e9, "slots": 8,
                            "plans_resident_GB": cache.resident_bytes() / 1e9, "parallelism": f"replicas x{world}",
@@ -501,7 +501,7 @@ def main(argv=None):
                          "~/.cache/directsht_b200/autotune.json)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-fp64-compare", action="store_true")
-    ap.add_argument("--bin-sums", default="auto", choices=["auto", "nufft", "tc"],
+    ap.add_argument("--bin-sums", default="auto", choices=["auto", "nufft", "tc", "fp64"],
                     help="bin sums of the mixed level: type-1 NUFFT, direct tensor-core sums, or the "
                          "library's choice by points per bin key (default)")
     ap.add_argument("--maps-per-pass", type=int, default=0, help="DSHT_TUNE_MAPS_PER_PASS (0: automatic)")
@@ -598,9 +598,10 @@ def main(argv=None):
     if args.maps_per_pass:
         d.tune(maps_per_pass=args.maps_per_pass)
     d.tune(bin_sums=args.bin_sums)
-    # the method that runs: AUTO takes the NUFFT from 512 points per bin key (DSHT_TUNE_BIN_SUMS)
+    # the method that runs: AUTO takes the NUFFT from 512 points per bin key on average, the
+    # FP64 direct sums below 28 and the tensor-core sums in between (DSHT_TUNE_BIN_SUMS)
     bin_method = args.bin_sums if args.bin_sums != "auto" else (
-        "nufft" if N >= 512 * 4 * (Nx - 1) else "tc")
+        "nufft" if N >= 512 * 4 * (Nx - 1) else "fp64" if N < 28 * 4 * (Nx - 1) else "tc")
     batch = args.batch if args.batch is not None else (4 if args.workload == "c2" else 1)
     if maps > 1 or w_dtype != L.DSHT_W_F64:
         batch = 1
@@ -717,7 +718,7 @@ def main(argv=None):
                     "equivalent_direct": {"value": 24.0 * N * Nl * maps / (ms * 1e-3) / 1e12, "unit": "TFLOP/s",
                                           "what": "24 flop per (point, m, map) of the direct sums over the "
                                                   "stage time: the rate the direct method would need"}}
-        if name == "bin_sums" and args.precision != "fp64":
+        if name == "bin_sums" and args.precision != "fp64" and bin_method == "tc":
             alg = 24.0 * N * Nl * maps
             a = alg / (ms * 1e-3) / 1e12
             ops = 2.0 * 128 * (2 * C) * 8 * N * maps
@@ -869,6 +870,7 @@ def main(argv=None):
             "scaling": "weak", "vs_baseline": None,
             "dtype": ("f64" if args.precision != "mixed" else
                       "f64 NUFFT sums + i8 digit-table contraction + f64" if bin_method == "nufft" else
+                      "f64 direct sums + i8 digit-table contraction + f64" if bin_method == "fp64" else
                       "i8 tensor sums + i8 digit-table contraction + f64"), "data": "synthetic",
             "config": {"workload": spec["name"], "Nl": Nl, "Nx": Nx, "N": N, "maps": maps,
                        "point_sets_per_step": batch, "precision": args.precision, "bin_sums": bin_method,

@@ -36,6 +36,7 @@ DSHT_TUNE_BIN_SUMS = 3
 DSHT_BIN_SUMS_AUTO = 0
 DSHT_BIN_SUMS_NUFFT = 1
 DSHT_BIN_SUMS_TC = 2
+DSHT_BIN_SUMS_FP64 = 3
 
 DSHT_PREC_FP64 = 0
 DSHT_PREC_MIXED = 1

@@ -71,7 +71,16 @@ size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* ba
     return p;
   };
   const int64_t n = N > 0 ? N : 1;
-  const int64_t pmax = std::min<int64_t>(g.nkeys, n) + (n + piece_max - 1) / piece_max;
+  // Pieces of a transform of up to n points.  A workspace laid out for the NUFFT sums' large
+  // pieces also serves the smaller transforms of a batch, which may take the direct sums:
+  // their pieces of default_piece_max(N) or at most 2048 points number at most
+  // max(2048, N / 2048) beyond one per key, with N below the NUFFT threshold.
+  int64_t extra = (n + piece_max - 1) / piece_max;
+  if (piece_max > 2048) {
+    const int64_t direct_n = std::min<int64_t>(n, (int64_t)kNufftMinPerKey * g.nkeys);
+    extra = std::max<int64_t>(extra, std::max<int64_t>(2048, (direct_n + 2047) / 2048));
+  }
+  const int64_t pmax = std::min<int64_t>(g.nkeys, n) + extra;
   const int tile = 128;
   const int ntile = (g.Nx + tile - 1) / tile;
   Workspace w{};
@@ -117,32 +126,50 @@ size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* ba
   return off;
 }
 
-// The mixed levels' bin-sum method for a call whose workspace is laid out for N points.
-// AUTO takes the NUFFT sums when there are at least kNufftMinPerKey points per bin key on
-// average: a NUFFT piece pays a fixed FFT (about 15 us of one SM at Nl = 1024) and little
-// per point, the tensor-core sums little per piece and more per point (measured crossover
-// near 500 points per piece); fewer points per key take the tensor-core sums.
+// The mixed levels' bin-sum method for one transform of N points (chosen per transform, so
+// the transforms of one batch call may differ).  AUTO compares the average points per bin
+// key with two measured crossovers: a NUFFT piece pays a fixed FFT (about 15 us of one SM at
+// Nl = 1024) and little per point, so it wins from kNufftMinPerKey points per key; the
+// tensor-core sums pay a GEMM tile and its epilogue per piece and 0.2-0.3 ns per point
+// (device-wide), the FP64 direct sums little per piece and 1-2 ns per point, so below
+// kFp64MaxPerKey points per key (pieces of a few points) the FP64 sums are the fastest.
+int plan_bin_method(const dsht_plan_s* p, int64_t N) {
+  const int t = p->tune_bin_sums;
+  if (t == DSHT_BIN_SUMS_FP64 || t == DSHT_BIN_SUMS_TC) return t;
+  if (p->nu_dinv && (t == DSHT_BIN_SUMS_NUFFT || N >= (int64_t)kNufftMinPerKey * p->g.nkeys))
+    return DSHT_BIN_SUMS_NUFFT;
+  if (t == DSHT_BIN_SUMS_AUTO && N < (int64_t)kFp64MaxPerKey * p->g.nkeys) return DSHT_BIN_SUMS_FP64;
+  return DSHT_BIN_SUMS_TC;
+}
+
 bool plan_uses_nufft(const dsht_plan_s* p, int64_t N) {
-  if (!p->nu_dinv || p->tune_bin_sums == DSHT_BIN_SUMS_TC) return false;
-  return p->tune_bin_sums == DSHT_BIN_SUMS_NUFFT || N >= (int64_t)kNufftMinPerKey * p->g.nkeys;
+  return plan_route(p, N).tc && plan_bin_method(p, N) == DSHT_BIN_SUMS_NUFFT;
 }
 
 // Pieces of the direct sums stay at or below 2048 points (the tensor path's S32 sums stay
 // exact); the NUFFT sums pay one FFT per piece, so theirs are larger.
 int plan_piece_max(const dsht_plan_s* p, int64_t N) {
-  const bool nufft = plan_route(p, N).tc && plan_uses_nufft(p, N);
+  const bool nufft = plan_uses_nufft(p, N);
   int pm = p->tune_piece_max > 0 ? p->tune_piece_max : nufft ? kNufftPiece : default_piece_max(p->g, N);
   if (!nufft && pm > 2048) pm = 2048;
   return pm;
 }
 
-int launch_bin_sums_mixed(const dsht_plan_s* p, Workspace& w2, cudaStream_t s) {
-  if (plan_uses_nufft(p, w2.npts)) {
-    w2.partial_f32 = 0;
-    return launch_bin_sums_nufft(p->g, w2, p->nu_logn, p->nu_dinv, p->nu_tw, s);
+// Bin sums of one transform of N points on the mixed route (sorted records in w2.pay).
+int launch_bin_sums_mixed(const dsht_plan_s* p, Workspace& w2, int64_t N, cudaStream_t s) {
+  switch (plan_bin_method(p, N)) {
+    case DSHT_BIN_SUMS_NUFFT:
+      w2.partial_f32 = 0;
+      return launch_bin_sums_nufft(p->g, w2, p->nu_logn, p->nu_dinv, p->nu_tw, s);
+    case DSHT_BIN_SUMS_FP64:
+      w2.partial_f32 = 0;
+      launch_piece_maxima(w2, s);  // the |w| sums (fold digit scales)
+      launch_bin_sums_fp64(p->g, w2, s);
+      return DSHT_OK;
+    default:
+      w2.partial_f32 = 1;
+      return launch_bin_sums_tc(p->g, w2, s);  // piece maxima and |w| sums first
   }
-  w2.partial_f32 = 1;
-  return launch_bin_sums_tc(p->g, w2, s);  // piece maxima and |w| sums first
 }
 
 Route plan_route(const dsht_plan_s* p, int64_t N) {
@@ -247,7 +274,7 @@ int run_after_sort(dsht_plan_s* p, int64_t N, int mode, double* alm, const Works
   // Small transforms run the FP64 stages even on a mixed-precision plan.
   const Route rt = plan_route(p, N);
   if (rt.tc) {
-    if (int rc = launch_bin_sums_mixed(p, w2, s)) return rc;
+    if (int rc = launch_bin_sums_mixed(p, w2, N, s)) return rc;
   } else {
     if (rt.digits) launch_piece_maxima(ws, s);  // the |w| sums (fold digit scales)
     launch_bin_sums_fp64(g, ws, s);
@@ -291,7 +318,7 @@ int run_pipeline(dsht_plan_s* p, const double* theta, const double* phi, const d
                         int mode, double* alm, const Workspace& ws, cudaStream_t s) {
   p->ev_n = 0;
   prof_mark(p, DSHT_STAGE_POINTS, s);
-  launch_points(p->g, theta, phi, w, 0, N, mode, ws, s, plan_route(p, N).tc && plan_uses_nufft(p, ws.npts));
+  launch_points(p->g, theta, phi, w, 0, N, mode, ws, s, plan_uses_nufft(p, N));
   prof_mark(p, DSHT_STAGE_BIN_SUMS, s);
   return run_after_sort(p, N, mode, alm, ws, s, true);
 }
@@ -320,15 +347,15 @@ static int run_class_digits(dsht_plan_s* p, const Item* items, const std::vector
     } else {
       prof_mark(p, DSHT_STAGE_POINTS, s);
       Workspace wp = ws;
+      wp.piece_max = plan_piece_max(p, item.N);
       if (!(li + 1 < list.size() && items[list[li + 1]].same_points)) wp.sidx = nullptr;
-      launch_points(g, item.theta, item.phi, item.w, item.w_f32, item.N, mode, wp, s,
-                    rt.tc && plan_uses_nufft(p, ws.npts));
+      launch_points(g, item.theta, item.phi, item.w, item.w_f32, item.N, mode, wp, s, plan_uses_nufft(p, item.N));
       *sorted_item = i;
     }
     prof_mark(p, DSHT_STAGE_BIN_SUMS, s);
     DSHT_CUDA_OK(cudaMemcpyAsync(w2.flags, ws.flags, sizeof(unsigned), cudaMemcpyDeviceToDevice, s));
     if (rt.tc) {
-      if (int rc = launch_bin_sums_mixed(p, w2, s)) return rc;
+      if (int rc = launch_bin_sums_mixed(p, w2, item.N, s)) return rc;
     } else {
       launch_piece_maxima(w2, s);
       launch_bin_sums_fp64(g, w2, s);
@@ -424,15 +451,15 @@ int run_items(dsht_plan_s* p, const Item* items, int n, int mode, const Workspac
         prof_mark(p, DSHT_STAGE_POINTS, s);
         // The sort keeps the input index of every slot when later items share it.
         Workspace wp = ws;
+        wp.piece_max = plan_piece_max(p, item.N);
         if (!(li + 1 < list.size() && items[list[li + 1]].same_points)) wp.sidx = nullptr;
-        launch_points(g, item.theta, item.phi, item.w, item.w_f32, item.N, mode, wp, s,
-                      mixed && plan_uses_nufft(p, ws.npts));
+        launch_points(g, item.theta, item.phi, item.w, item.w_f32, item.N, mode, wp, s, plan_uses_nufft(p, item.N));
         sorted_item = i;
       }
       prof_mark(p, DSHT_STAGE_BIN_SUMS, s);
       DSHT_CUDA_OK(cudaMemcpyAsync(w2.flags, ws.flags, sizeof(unsigned), cudaMemcpyDeviceToDevice, s));
       if (mixed) {
-        if (int rc = launch_bin_sums_mixed(p, w2, s)) return rc;
+        if (int rc = launch_bin_sums_mixed(p, w2, item.N, s)) return rc;
       } else {
         launch_bin_sums_fp64(g, w2, s);
         w2.partial_f32 = 0;
@@ -632,8 +659,8 @@ int dsht_plan_tune(dsht_plan_t p, int param, int value) {
       p->tune_piece_max = value;
       return DSHT_OK;
     case DSHT_TUNE_BIN_SUMS:
-      if (value != DSHT_BIN_SUMS_AUTO && value != DSHT_BIN_SUMS_NUFFT && value != DSHT_BIN_SUMS_TC)
-        return set_error(DSHT_ERR_INVALID, "bin-sum method %d: AUTO (0), NUFFT (1) or TC (2)", value);
+      if (value < DSHT_BIN_SUMS_AUTO || value > DSHT_BIN_SUMS_FP64)
+        return set_error(DSHT_ERR_INVALID, "bin-sum method %d: AUTO (0), NUFFT (1), TC (2) or FP64 (3)", value);
       p->tune_bin_sums = value;
       return DSHT_OK;
     case DSHT_TUNE_MAPS_PER_PASS:

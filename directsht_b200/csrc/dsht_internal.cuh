@@ -133,6 +133,7 @@ int launch_bin_sums_nufft(const Geometry& g, const Workspace& ws, int logn, cons
                           cudaStream_t s);
 constexpr int kNufftPiece = 8192;  // default points per piece of the NUFFT sums
 constexpr int kNufftMinPerKey = 512;  // AUTO bin sums: NUFFT from this many points per key on average
+constexpr int kFp64MaxPerKey = 28;    // AUTO bin sums: FP64 direct sums below this many per key
 int tc_inner_factor(int Nl);
 // FP64 fold of the current map into ws.fold, and the live-tile flags of the contractions.
 void launch_fold(const Geometry& g, const Workspace& ws, cudaStream_t s);
@@ -263,7 +264,8 @@ struct Item {
 };
 // Bin sums of a tensor-core-route transform: the NUFFT (default) or the tensor-core direct
 // sums; sets w2.partial_f32 to the layout written.
-int launch_bin_sums_mixed(const dsht_plan_s* p, Workspace& w2, cudaStream_t s);
+int launch_bin_sums_mixed(const dsht_plan_s* p, Workspace& w2, int64_t N, cudaStream_t s);
+int plan_bin_method(const dsht_plan_s* p, int64_t N);
 bool plan_uses_nufft(const dsht_plan_s* p, int64_t N);
 // Runs the items in order; every finished item's flags are OR-ed into ws.all_flags.
 int run_items(dsht_plan_s* p, const Item* items, int n, int mode, const Workspace& ws, cudaStream_t s);

@@ -15,8 +15,8 @@
 // The array's name in host code is only a host-side stand-in for the device symbol, not a
 // device address, so it is never handed to a kernel: the device address is looked up once
 // per device with cudaGetSymbolAddress, with that device current, on the first call made
-// on that device (this first call should therefore happen before any stream capture), and
-// cached.  All calls share the one array and it keeps the last call's contents; the
+// on that device, and cached.  Every call waits for its stream at the end to read the error
+// flags, so no call can be captured into a CUDA graph.  All calls share the one array and it keeps the last call's contents; the
 // pipeline clears what must start at zero (the bin counts and the error flags) and
 // overwrites everything else it reads, so stale contents never leak into a result.  Calls
 // whose kernels overlap on the GPU (on different streams or host threads) race on the

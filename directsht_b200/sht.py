@@ -97,12 +97,14 @@ class DirectSHT:
         self.precision = precision
 
     # -- tables ---------------------------------------------------------------------
-    _BIN_SUMS = {"auto": L.DSHT_BIN_SUMS_AUTO, "nufft": L.DSHT_BIN_SUMS_NUFFT, "tc": L.DSHT_BIN_SUMS_TC}
+    _BIN_SUMS = {"auto": L.DSHT_BIN_SUMS_AUTO, "nufft": L.DSHT_BIN_SUMS_NUFFT, "tc": L.DSHT_BIN_SUMS_TC,
+                 "fp64": L.DSHT_BIN_SUMS_FP64}
 
     def tune(self, piece_max=None, maps_per_pass=None, bin_sums=None):
         """Set tuning parameters (``dsht_plan_tune``); None leaves one unchanged, 0 (or
         'auto') restores the automatic choice.  bin_sums picks the mixed levels' per-bin sums:
-        'nufft' (the default) or 'tc' (direct tensor-core sums).  Returns the current values
+        'nufft', 'tc' (direct tensor-core sums), 'fp64' (direct FP64 sums) or 'auto' (the
+        default).  Returns the current values
         as a dict (bin_sums as its name)."""
         if piece_max is not None:
             L.check(self._lib.dsht_plan_tune(self._plan, L.DSHT_TUNE_PIECE_MAX, int(piece_max)))

@@ -112,14 +112,18 @@ int dsht_get_precision(dsht_plan_t plan, int* precision);
  * tensor-core, cap it at 2048; the NUFFT sums default to 8192).  DSHT_TUNE_MAPS_PER_PASS:
  * maps or point sets that share one read of the tables in a multi-transform call, 1..8,
  * 0 = the most (8; the tensor-core contraction only: the FP64 one reads the tables once per
- * map).  DSHT_TUNE_BIN_SUMS: the bin sums of the mixed levels, DSHT_BIN_SUMS_NUFFT or
- * DSHT_BIN_SUMS_TC (the direct int8-slice tensor-core sums); AUTO (the default) takes the
- * NUFFT sums when a call has at least 512 points per bin key on average (N >= 2048 (Nx - 1)),
- * where its fixed cost per bin piece pays off, and the tensor-core sums below.  Workspace
- * sizes depend on all three: query them after tuning. */
+ * map).  DSHT_TUNE_BIN_SUMS: the bin sums of the mixed levels, DSHT_BIN_SUMS_NUFFT,
+ * DSHT_BIN_SUMS_TC (the direct int8-slice tensor-core sums) or DSHT_BIN_SUMS_FP64 (the direct
+ * FP64 CUDA-core sums of the fp64 level); AUTO (the default) chooses per transform (so the
+ * transforms of one batch call may differ) from its points per bin key on average: the
+ * NUFFT sums from 512 (N >= 2048 (Nx - 1)), where their fixed cost per bin piece pays off,
+ * the FP64 direct sums below 28 (N < 112 (Nx - 1): pieces of a few points, where the
+ * tensor-core sums' per-piece GEMM tile costs more than FP64 work per point), and the
+ * tensor-core sums in between.  Workspace sizes depend on all three: query them after
+ * tuning. */
 enum { DSHT_TUNE_PIECE_MAX = 1, DSHT_TUNE_MAPS_PER_PASS = 2, DSHT_TUNE_BIN_SUMS = 3 };
 /* Values of DSHT_TUNE_BIN_SUMS: the bin-sum method of the mixed levels. */
-enum { DSHT_BIN_SUMS_AUTO = 0, DSHT_BIN_SUMS_NUFFT = 1, DSHT_BIN_SUMS_TC = 2 };
+enum { DSHT_BIN_SUMS_AUTO = 0, DSHT_BIN_SUMS_NUFFT = 1, DSHT_BIN_SUMS_TC = 2, DSHT_BIN_SUMS_FP64 = 3 };
 int dsht_plan_tune(dsht_plan_t plan, int param, int value);
 int dsht_plan_get_tune(dsht_plan_t plan, int param, int* value);
 
@@ -214,8 +218,8 @@ int dsht_rotate_back(dsht_plan_t plan, const double* alm_rot, const double* alm_
  * a plan tuned to smaller pieces (DSHT_TUNE_PIECE_MAX) needs more: check a problem with
  * dsht_workspace_size(plan, N) <= dsht_noalloc_scratch_bytes() beforehand.  Like
  * dsht_execute, each call waits for its stream once at the end to read the error flags,
- * and N is limited to 0xfffffff0 points.  The first call on a device
- * looks up the array's device address and should come before any stream capture.  All
+ * and N is limited to 0xfffffff0 points; because of that wait a call can never be captured
+ * into a CUDA graph (dsht_enqueue_maps is the capturable entry point).  All
  * calls share the array (it keeps the last call's contents; what must start at zero is
  * cleared), so calls that overlap on the GPU race and must be serialised by the caller. */
 int dsht_execute_noalloc(dsht_plan_t plan, const double* theta, const double* phi, const double* w,

@@ -45,7 +45,10 @@ def test_batch_equals_single_calls(precision):
     tab = O.build_tables(Nl, Nx)
     for i, (th, ph, w) in enumerate(sets):
         single = d(th, ph, w)
-        if precision == "fp64" or len(th) < 1024:
+        # the NUFFT and tensor-core bin sums (from 28 points per bin key on average) are exact
+        # integer sums, so a batch item repeats its single call bit for bit; the FP64 sums
+        # (fp64 level, transforms under 1024 points, sparse transforms) add in the sort's order
+        if precision == "fp64" or len(th) < 28 * 4 * (Nx - 1):
             assert _rel(got[i], single) <= 1e-13 or not np.any(single), i
         else:
             assert np.array_equal(got[i], single), i
@@ -125,9 +128,10 @@ def test_enqueue_batch_in_cuda_graph():
             a.zero_()
         g.replay()
         torch.cuda.synchronize()
-        for i in range(n):  # N < 1024 runs the FP64 bin sums, whose order inside a bin varies
+        for i in range(n):  # under 28 points per bin key the FP64 bin sums run: their order varies
             got = alms[i].cpu().numpy()
-            assert np.array_equal(got, eager[i]) if len(sets[i][0]) >= 1024 else _rel(got, eager[i]) <= 1e-13
+            exact = len(sets[i][0]) >= 28 * 4 * (Nx - 1)
+            assert np.array_equal(got, eager[i]) if exact else _rel(got, eager[i]) <= 1e-13
     assert all(d._lib.dsht_status(int(f), L.DSHT_MODE_CALL) == L.DSHT_OK for f in status.cpu().numpy())
 
 

@@ -132,7 +132,7 @@ def test_tune_rejects_bad_values():
     d = DirectSHT(16, 32)
     for param, value in ((L.DSHT_TUNE_PIECE_MAX, 100), (L.DSHT_TUNE_PIECE_MAX, 70000),
                          (L.DSHT_TUNE_PIECE_MAX, 4100), (L.DSHT_TUNE_MAPS_PER_PASS, 9),
-                         (L.DSHT_TUNE_BIN_SUMS, 3), (77, 1)):
+                         (L.DSHT_TUNE_BIN_SUMS, 4), (L.DSHT_TUNE_BIN_SUMS, -1), (77, 1)):
         assert d._lib.dsht_plan_tune(d._plan, param, value) == L.DSHT_ERR_INVALID
     assert d.tune() == {"piece_max": 0, "maps_per_pass": 0, "bin_sums": "auto"}
 

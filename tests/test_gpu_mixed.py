@@ -46,7 +46,7 @@ def test_mixed_matches_fp64(Nl, Nx, N, seed):
     w = rng.lognormal(0, 0.5, N)
     d = DirectSHT(Nl, Nx)
     ref = d(th, ph, w)
-    for bin_sums in ("nufft", "tc"):
+    for bin_sums in ("nufft", "tc", "fp64"):
         d.tune(bin_sums=bin_sums)
         for level in ("mixed", "mixed_f64_tables"):
             d.set_precision(level)
@@ -86,7 +86,7 @@ def test_mixed_heavy_bin_and_wide_weights():
     ref = d.basic_sht(th, ph, w.copy(), verbose=False)
     # Half of the weight sits in one bin: the digit tables' fixed point is relative to each
     # row's and fold column's scale, so both levels hold 1e-7.
-    for bin_sums in ("nufft", "tc"):
+    for bin_sums in ("nufft", "tc", "fp64"):
         d.tune(bin_sums=bin_sums)
         for level in ("mixed_f64_tables", "mixed"):
             d.set_precision(level)
@@ -125,7 +125,7 @@ def test_mixed_concentrated_weight_vs_oracle(case):
     ref = _oracle_basic(Nl, Nx, th, ph, w)
     for kwargs in (dict(precision="mixed"), dict(compact_tables=True)):
         d = DirectSHT(Nl, Nx, **kwargs)
-        for bin_sums in ("nufft", "tc"):
+        for bin_sums in ("nufft", "tc", "fp64"):
             d.tune(bin_sums=bin_sums)
             a = d.basic_sht(th, ph, w.copy(), verbose=False)
             assert _rel(a, ref) <= TOL_MIXED, (case, kwargs, bin_sums)
@@ -176,7 +176,7 @@ def test_mixed_c2_full_size():
     d = DirectSHT(1024, 2048)
     ref = d(th, ph, w)
     d.set_precision("mixed")
-    for bin_sums in ("nufft", "tc"):
+    for bin_sums in ("nufft", "tc", "fp64"):
         d.tune(bin_sums=bin_sums)
         a = d(th, ph, w)
         assert _rel(a, ref) <= TOL_MIXED, bin_sums

@@ -105,10 +105,12 @@ def test_nufft_many_maps_match_single_calls():
 
 
 def test_auto_bin_sums_follow_points_per_key():
-    """AUTO takes the NUFFT sums from 512 points per bin key on average and the tensor-core
-    sums below: the two calls here agree with the forced methods bit for bit (pieces of up to
-    2048 points keep every bin one piece, so both methods' sums are exact and repeatable)."""
-    Nl, Nx = 64, 32  # 4 x 31 = 124 keys: the NUFFT from 63488 points
+    """AUTO takes the NUFFT sums from 512 points per bin key on average, the FP64 direct sums
+    below 28 and the tensor-core sums in between: each call here agrees with its forced
+    method (bit for bit for the NUFFT and tensor-core sums, whose per-piece sums are exact
+    integers when pieces of up to 2048 points keep every bin one piece; to FP64 rounding for
+    the FP64 sums, whose order of adds follows the sort) and not with the tensor-core sums."""
+    Nl, Nx = 64, 32  # 4 x 31 = 124 keys: the NUFFT from 63488 points, FP64 below 3472
     th, ph, w = _sky(100000, 31)
     d = DirectSHT(Nl, Nx, precision="mixed")
     d.tune(piece_max=2048)
@@ -117,3 +119,32 @@ def test_auto_bin_sums_follow_points_per_key():
         d.tune(bin_sums=method)
         assert np.array_equal(a, d(th[:N], ph[:N], w[:N])), (N, method)
         d.tune(bin_sums="auto")
+    N = 2500
+    a = d(th[:N], ph[:N], w[:N])
+    d.tune(bin_sums="fp64")
+    a64 = d(th[:N], ph[:N], w[:N])
+    d.tune(bin_sums="tc")
+    atc = d(th[:N], ph[:N], w[:N])
+    d.tune(bin_sums="auto")
+    scale = np.abs(a64).max()
+    assert np.abs(a - a64).max() <= 1e-13 * scale
+    assert np.abs(a - atc).max() > 1e-11 * scale
+
+
+def test_batch_items_choose_their_own_bin_sums():
+    """In a batch call each transform takes the bin-sum method its own size selects (not the
+    one of the batch's largest transform).  With pieces of up to 2048 points every bin here
+    is one piece and each item equals the same transform run alone to FP64 rounding; with the
+    default piece sizes (a workspace laid out for the NUFFT's large pieces, smaller pieces
+    for the direct sums of the smaller items) each item agrees with it within the mixed
+    tolerance (pieces cut from the sort's order quantise differently)."""
+    Nl, Nx = 64, 32  # 124 keys: NUFFT from 63488 points, FP64 sums below 3472
+    th, ph, w = _sky(100000, 37)
+    d = DirectSHT(Nl, Nx, precision="mixed")
+    sets = [(th[:N], ph[:N], w[:N]) for N in (100000, 20000, 2500)]
+    for piece, tol in ((2048, 1e-12), (0, 1e-8)):
+        d.tune(piece_max=piece)
+        batch = d.call_batch(sets)
+        for (t, p, ww), a in zip(sets, batch):
+            alone = d(t, p, ww)
+            assert np.abs(a - alone).max() <= tol * np.abs(alone).max(), (piece, len(t))
