@@ -114,6 +114,7 @@ size_t workspace_layout(const Geometry& g, int64_t N, int piece_max, uint8_t* ba
   w.fold = reinterpret_cast<double*>(take(std::max(fold_bytes, fdig_bytes)));
   w.cexp = reinterpret_cast<int16_t*>(take(sizeof(int16_t) * 2 * w.tc_maps));
   w.cmax = reinterpret_cast<unsigned long long*>(take(sizeof(unsigned long long) * 2 * w.tc_maps));
+  w.tc_next = reinterpret_cast<unsigned*>(take(sizeof(unsigned)));
   w.tile_live = reinterpret_cast<uint8_t*>(take(2 * (size_t)ntile));
   w.tile_live2 = reinterpret_cast<uint8_t*>(take(2 * (size_t)((g.Nx + 255) / 256)));
   w.alm_equ = reinterpret_cast<double*>(take(sizeof(double) * 2 * (size_t)g.Nlm));
@@ -290,7 +291,7 @@ int run_after_sort(dsht_plan_s* p, int64_t N, int mode, double* alm, const Works
     out.equ[0] = ws.alm_equ;
     out.pol[0] = ws.alm_pol;
     if (int rc = launch_contract_tc(g, p->tmDig, p->tc_items, p->tc_nitems, p->rexp, fdig, 4, ws.cexp, 1, out,
-                                    ws.flags, s))
+                                    ws.flags, ws.tc_next, s))
       return rc;
   } else {
     mark(DSHT_STAGE_FOLD);
@@ -380,7 +381,7 @@ static int run_class_digits(dsht_plan_s* p, const Item* items, const std::vector
     }
     prof_mark(p, DSHT_STAGE_CONTRACT, s);
     if (int rc = launch_contract_tc(g, p->tmDig, p->tc_items, p->tc_nitems, p->rexp, fdig, fcols, ws.cexp,
-                                    (int)pass.size(), out, ws.slot_flags, s))
+                                    (int)pass.size(), out, ws.slot_flags, ws.tc_next, s))
       return rc;
     prof_mark(p, DSHT_STAGE_ROTATE, s);
     if (mode == DSHT_MODE_CALL) launch_rotate_back_maps(g, rm, (int)pass.size(), s);

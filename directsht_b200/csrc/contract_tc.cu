@@ -18,12 +18,19 @@
 // epilogue forms V = W_0 2^32 + W_1 2^24 + W_2 2^16 + W_3 2^8 + W_4 in int64 and the
 // value 2^(er+ec-46) V.
 //
-// Warp roles: warp 0 (one thread) issues TMA loads -- one 3D box of 4 digit planes x 128
-// rows x 64 bytes of the table and one of 4 planes x NC columns x 64 bytes of the fold per
-// stage -- into a ring of stages; warp 1 allocates TMEM and issues the MMAs from one thread;
+// Warp roles: warp 0 (one thread) claims work items from a global counter and issues TMA
+// loads -- one 3D box of 4 digit planes x 128 rows x 64 bytes of the table and one of 4
+// planes x NC columns x 64 bytes of the fold per stage -- into a ring of stages; warp 1
+// allocates TMEM and issues the MMAs from one thread;
 // warps 2-5 read the accumulators (TMEM lanes 32 (w % 4) ..) and write the alm, while the
 // next tile accumulates into the other TMEM buffer.  Every wait is bounded and records
 // kFlagTimeout instead of hanging.  No cluster multicast anywhere.
+//
+// Items are claimed in order (m, parity, row tile) by whichever CTA is free, so the row tiles
+// of one (m, parity) block run at about the same time on different SMs and the block's fold
+// slice (NC x 32 bytes per node) comes from DRAM once and from L2 for the other tiles.  (A
+// fixed round-robin assignment let the CTAs drift apart, and the slice was read from DRAM
+// about once per tile: +25 % of DRAM traffic at Nl = 2048 with 32 columns.)
 //
 // Bound: HBM (the table digits, 8 B per (l, m, node), half the FP64 pair) while N is
 // small; each table byte is read once per pass however many maps the pass holds.
@@ -42,6 +49,7 @@ constexpr int kChunk = 64;    // K bytes per stage: one 64-byte swizzled row per
 constexpr int kTileRows = 128;
 constexpr int kEpiWarps = 4;
 constexpr int kTcThreads = 32 * (2 + kEpiWarps);
+constexpr int kItemRing = 16;  // claimed items in flight: the producer leads the epilogue by <= kStages + 3
 
 template <int NC>
 struct TcLayout {
@@ -54,7 +62,7 @@ struct TcLayout {
   static constexpr uint32_t kTmemCols = kBufs * kAcc <= 32 ? 32 : kBufs * kAcc <= 64 ? 64
                                         : kBufs * kAcc <= 128 ? 128 : kBufs * kAcc <= 256 ? 256 : 512;
   static constexpr int kBarOff = kStages * kStage;
-  static constexpr int kBytes = kBarOff + 256 + 1024;  // barriers, TMEM address, alignment slack
+  static constexpr int kBytes = kBarOff + 512 + 1024;  // barriers, TMEM address, item ring, alignment slack
 };
 
 // Work item i: (m, parity, row tile) packed as m | par << 16 | tile << 17.
@@ -69,7 +77,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 contract_tc_kernel(int Nl, int nchunks, const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                    const uint32_t* __restrict__ items, int nitems, const int16_t* __restrict__ rexp,
                    const int16_t* __restrict__ cexp, int ncols, const TcOut out, unsigned* __restrict__ err,
-                   int stall) {
+                   unsigned* __restrict__ next_item, int stall) {
   using L = TcLayout<NC>;
   constexpr int S = L::kStages;
   extern __shared__ uint8_t smem_raw[];
@@ -79,8 +87,10 @@ contract_tc_kernel(int Nl, int nchunks, const __grid_constant__ CUtensorMap tmA,
   uint64_t* tfull = empty + S;       // [2] MMA -> epilogue
   uint64_t* tempty = tfull + 2;      // [2] epilogue -> MMA
   uint64_t* drain = tempty + 2;      // [1] every MMA issued has completed
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+  uint64_t* item_full = drain + 1;   // [kItemRing] producer -> MMA issuer and epilogue
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(item_full + kItemRing);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  int* item_ring = reinterpret_cast<int*>(tmem_slot + 2);  // [kItemRing] claimed item, -1 = none left
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0) {
     for (int s = 0; s < S; ++s) {
@@ -92,6 +102,7 @@ contract_tc_kernel(int Nl, int nchunks, const __grid_constant__ CUtensorMap tmA,
       tc::mbar_init(&tempty[b], kEpiWarps);
     }
     tc::mbar_init(drain, 1);
+    for (int r = 0; r < kItemRing; ++r) tc::mbar_init(&item_full[r], 1);
     *abort_flag = 0;
     tc::mbar_fence_init();
   }
@@ -108,9 +119,15 @@ contract_tc_kernel(int Nl, int nchunks, const __grid_constant__ CUtensorMap tmA,
   if (warp == 0) {
     // ---- TMA producer (one thread) --------------------------------------------------------
     if (lane == 0) {
-      uint32_t n = 0;
+      uint32_t n = 0, j = 0;
       bool ok = true;
-      for (int it = blockIdx.x; it < nitems && ok; it += gridDim.x) {
+      while (ok) {
+        int it = (int)atomicAdd(next_item, 1u);
+        if (it >= nitems) it = -1;
+        item_ring[j % kItemRing] = it;
+        tc::mbar_arrive(&item_full[j % kItemRing]);  // releases the ring entry
+        ++j;
+        if (it < 0) break;
         int m, par, tile;
         item_decode(items[it], &m, &par, &tile);
         const int ne = (Nl - m + 1) / 2;
@@ -152,9 +169,14 @@ contract_tc_kernel(int Nl, int nchunks, const __grid_constant__ CUtensorMap tmA,
       constexpr uint32_t i2 = tc::idesc_i8(kTileRows, 2 * NC, true, true);
       constexpr uint32_t i1 = tc::idesc_i8(kTileRows, NC, true, true);
       constexpr uint32_t kPlaneA = kTileRows * kChunk, kPlaneB = NC * kChunk;
-      uint32_t n = 0, iter = 0;
+      uint32_t n = 0;
       bool ok = true;
-      for (int it = blockIdx.x; it < nitems && ok; it += gridDim.x, ++iter) {
+      for (uint32_t iter = 0; ok; ++iter) {
+        if (!tc::mbar_wait(&item_full[iter % kItemRing], (iter / kItemRing) & 1, abort_flag)) {
+          fail();
+          break;
+        }
+        if (item_ring[iter % kItemRing] < 0) break;
         const uint32_t b = L::kBufs == 2 ? (iter & 1) : 0;
         const uint32_t use_b = L::kBufs == 2 ? (iter >> 1) : iter;
         if (use_b > 0 && !tc::mbar_wait(&tempty[b], (use_b - 1) & 1, abort_flag)) {
@@ -207,8 +229,13 @@ contract_tc_kernel(int Nl, int nchunks, const __grid_constant__ CUtensorMap tmA,
   } else {
     // ---- epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 -----------------------------
     const int q = warp & 3;
-    uint32_t iter = 0;
-    for (int it = blockIdx.x; it < nitems; it += gridDim.x, ++iter) {
+    for (uint32_t iter = 0;; ++iter) {
+      if (*abort_flag || !tc::mbar_wait(&item_full[iter % kItemRing], (iter / kItemRing) & 1, abort_flag)) {
+        if (lane == 0) fail();
+        break;
+      }
+      const int it = item_ring[iter % kItemRing];
+      if (it < 0) break;
       const uint32_t b = L::kBufs == 2 ? (iter & 1) : 0;
       const uint32_t use_b = L::kBufs == 2 ? (iter >> 1) : iter;
       if (*abort_flag || !tc::mbar_wait(&tfull[b], use_b & 1, abort_flag)) {
@@ -291,7 +318,7 @@ int make_digit_tmap(CUtensorMap* tm, const void* base, int64_t kp, int64_t rows,
 template <int NC>
 int tc_launch(const Geometry& g, const CUtensorMap& tmA, const uint8_t* fdig, int fdig_cols, const uint32_t* items,
               int nitems, const int16_t* rexp, const int16_t* cexp, int ncols, const TcOut& out, unsigned* flags,
-              cudaStream_t s) {
+              unsigned* next_item, cudaStream_t s) {
   using L = TcLayout<NC>;
   alignas(64) CUtensorMap tmB;
   const int kp = digit_kp(g.Nx);
@@ -306,8 +333,9 @@ int tc_launch(const Geometry& g, const CUtensorMap& tmA, const uint8_t* fdig, in
   auto kern = contract_tc_kernel<NC>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kBytes);
   const int stall = g_stall_next.exchange(0);
+  cudaMemsetAsync(next_item, 0, sizeof(unsigned), s);
   kern<<<grid, kTcThreads, L::kBytes, s>>>(g.Nl, kp / kChunk, tmA, tmB, items, nitems, rexp, cexp, ncols, out, flags,
-                                           stall);
+                                           next_item, stall);
   count_launches(1);
   return DSHT_OK;
 }
@@ -332,14 +360,17 @@ std::vector<uint32_t> tc_items(int Nl) {
 
 int launch_contract_tc(const Geometry& g, const CUtensorMap& tmA, const uint32_t* items, int nitems,
                        const int16_t* rexp, const uint8_t* fdig, int fdig_cols, const int16_t* cexp, int nmaps,
-                       const TcOut& out, unsigned* flags, cudaStream_t s) {
+                       const TcOut& out, unsigned* flags, unsigned* next_item, cudaStream_t s) {
   if (nmaps < 1 || nmaps > kTcMaxMaps || 4 * nmaps > fdig_cols)
     return set_error(DSHT_ERR_INVALID, "tensor-core pass of %d maps (%d fold columns)", nmaps, fdig_cols);
   const int nc = tc_fold_cols(nmaps);
   const int ncols = 4 * nmaps;
-  if (nc == 16) return tc_launch<16>(g, tmA, fdig, fdig_cols, items, nitems, rexp, cexp, ncols, out, flags, s);
-  if (nc == 32) return tc_launch<32>(g, tmA, fdig, fdig_cols, items, nitems, rexp, cexp, ncols, out, flags, s);
-  return tc_launch<64>(g, tmA, fdig, fdig_cols, items, nitems, rexp, cexp, ncols, out, flags, s);
+  auto go = [&](auto launch) {
+    return launch(g, tmA, fdig, fdig_cols, items, nitems, rexp, cexp, ncols, out, flags, next_item, s);
+  };
+  if (nc == 16) return go(tc_launch<16>);
+  if (nc == 32) return go(tc_launch<32>);
+  return go(tc_launch<64>);
 }
 
 }  // namespace dsht

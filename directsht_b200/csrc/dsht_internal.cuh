@@ -87,6 +87,7 @@ struct Workspace {
                         // [Nl][2][4][4 tc_maps][Kp] (int8) share this region
   int16_t* cexp;        // [tc_maps][2] fold column scale exponents (tensor-core route)
   unsigned long long* cmax;  // [tc_maps][2] largest node |w| sum per half (bits of a double)
+  unsigned* tc_next;    // [1] work counter of the tensor-core contraction
   int tc_maps;          // maps one tensor-core contraction pass can hold
   uint8_t* tile_live;   // [2][ceil(Nx/128)] tiles of the fallback contraction
   uint8_t* tile_live2;  // [2][ceil(Nx/256)] tiles of the streaming contraction
@@ -155,7 +156,7 @@ int make_table_digit_tmap(CUtensorMap* tm, const uint8_t* dig, int Nx, int64_t N
 std::vector<uint32_t> tc_items(int Nl);
 int launch_contract_tc(const Geometry& g, const CUtensorMap& tmA, const uint32_t* items, int nitems,
                        const int16_t* rexp, const uint8_t* fdig, int fdig_cols, const int16_t* cexp, int nmaps,
-                       const TcOut& out, unsigned* flags, cudaStream_t s);
+                       const TcOut& out, unsigned* flags, unsigned* next_item, cudaStream_t s);
 
 void launch_contract_fp64(const Geometry& g, const double* Yv, const double* Yd,
                           const Workspace& ws, cudaStream_t s);
