@@ -655,8 +655,19 @@ def main(argv=None):
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             total_ms = float(t.item())
         ms_b = total_ms / args.steps
+        # Stage times of one headline step (untimed, after the timed steps): the library's
+        # stage events around every launch of one batched call.
+        stage_ms = (ct.c_double * 5)()
+        calls = ct.c_int64()
+        L.check(lib.dsht_profile_enable(d._plan, 1))
+        L.check(lib.dsht_profile_read(d._plan, stage_ms, ct.byref(calls), 1))
+        step_batch()
+        torch.cuda.synchronize()
+        L.check(lib.dsht_profile_read(d._plan, stage_ms, ct.byref(calls), 1))
+        L.check(lib.dsht_profile_enable(d._plan, 0))
+        bstages = {n: stage_ms[i] for i, n in enumerate(L.STAGES)}
         main = {"ms_per_step": ms_b, "value": world * batch * N * Nl / (ms_b / 1e3), "per_step": per_step,
-                "stages": single["stages"], "launches": int(launches), "clocks": clk, "alm": balm[0:1].clone()}
+                "stages": bstages, "launches": int(launches), "clocks": clk, "alm": balm[0:1].clone()}
     other = None
     if args.precision == "mixed" and not args.no_fp64_compare:
         other = timed("fp64", sample_clocks=False)
@@ -681,6 +692,9 @@ def main(argv=None):
     # the FP64 CUDA-core contraction one
     per_pass = (d.tune()["maps_per_pass"] or (8 if args.precision == "mixed" else 1)) if maps > 1 else 1
     passes = -(-maps // per_pass)
+    # point sets per step: the headline step's stage times cover `batch` sets (points, bin
+    # sums, fold and rotation once per set; one contraction pass serves all of them)
+    nsets = batch
 
     def stage_roof(name, ms):
         """Roofline of one stage: algorithmic bytes or flops of the whole step (the per-unit
@@ -698,7 +712,7 @@ def main(argv=None):
                     "algorithmic": f"{2 * eb} B of {'digit' if f32_tables else 'FP64'} table (Yv, Yd) per "
                                    f"(l, m, node) per pass ({passes} passes)"}
         if name == "points":
-            alg = 56.0 * N
+            alg = 56.0 * N * nsets
             a = alg / (ms * 1e-3) / 1e9
             return {"kernel": "count/scan/scatter (counting sort by bin)", "bound": "hbm", "achieved": a,
                     "peak": hbm_peak, "unit": "GB/s", "frac": a / hbm_peak, "peak_source": peak_src,
@@ -709,19 +723,21 @@ def main(argv=None):
             # Hermite weights; per piece two complex FFTs of n cells (5 n log2 n each)
             logn = nufft_logn(Nl)
             pieces = nufft_pieces(th, ph, Nx, 0.75, 8192)
-            alg = (400.0 * N + pieces * 2 * 5.0 * (1 << logn) * logn * (2 if logn > 12 else 1)) * maps
+            alg = (400.0 * N + pieces * 2 * 5.0 * (1 << logn) * logn * (2 if logn > 12 else 1)) * maps * nsets
             a = alg / (ms * 1e-3) / 1e12
             return {"kernel": "nufft_sums_kernel (FP64 spread, shared-memory FFT)", "bound": "fp64",
                     "achieved": a, "peak": 40.0, "unit": "TFLOP/s", "frac": a / 40.0,
                     "peak_source": "nominal (no measured FP64 figure)",
-                    "algorithmic": f"400 flop per point + 10 n log2 n per piece ({pieces} pieces, n = {1 << logn})",
-                    "equivalent_direct": {"value": 24.0 * N * Nl * maps / (ms * 1e-3) / 1e12, "unit": "TFLOP/s",
+                    "algorithmic": f"400 flop per point + 10 n log2 n per piece ({pieces} pieces, n = {1 << logn}) "
+                                   f"x {nsets} point sets",
+                    "equivalent_direct": {"value": 24.0 * N * Nl * maps * nsets / (ms * 1e-3) / 1e12,
+                                          "unit": "TFLOP/s",
                                           "what": "24 flop per (point, m, map) of the direct sums over the "
                                                   "stage time: the rate the direct method would need"}}
         if name == "bin_sums" and args.precision != "fp64" and bin_method == "tc":
-            alg = 24.0 * N * Nl * maps
+            alg = 24.0 * N * Nl * maps * nsets
             a = alg / (ms * 1e-3) / 1e12
-            ops = 2.0 * 128 * (2 * C) * 8 * N * maps
+            ops = 2.0 * 128 * (2 * C) * 8 * N * maps * nsets
             a_ops = ops / (ms * 1e-3) / 1e12
             return {"kernel": "bin_sums_tc_kernel (tcgen05 kind::i8)", "bound": "tensor", "achieved": a,
                     "peak": bf16_peak, "unit": "TFLOP/s", "frac": a / bf16_peak,
@@ -732,13 +748,13 @@ def main(argv=None):
                                        "what": f"8 int8 slice products of a 128 x {2 * C} x (points) GEMM, "
                                                f"2 op per MAC, against 2 x the bf16 rate (dense int8 on B200)"}}
         if name == "bin_sums":
-            alg = 24.0 * N * Nl * maps
+            alg = 24.0 * N * Nl * maps * nsets
             a = alg / (ms * 1e-3) / 1e12
             return {"kernel": "bin_sums_fp64_kernel", "bound": "fp64", "achieved": a, "peak": 40.0,
                     "unit": "TFLOP/s", "frac": a / 40.0, "peak_source": "nominal (no measured FP64 figure)",
                     "algorithmic": "24 flop per (point, m, map): 8 FMA sums + 4 FMA angle step"}
         if name == "rotate":
-            alg = 2.0 * 5 * sum((l + 1) ** 2 for l in range(Nl)) * maps
+            alg = 2.0 * 5 * sum((l + 1) ** 2 for l in range(Nl)) * maps * nsets
             a = alg / (ms * 1e-3) / 1e12
             return {"kernel": "rotate_back_kernel", "bound": "fp64", "achieved": a, "peak": 40.0,
                     "unit": "TFLOP/s", "frac": a / 40.0, "peak_source": "nominal (no measured FP64 figure)",
@@ -749,7 +765,7 @@ def main(argv=None):
     top = max(stages, key=stages.get)
     roof = dict(roofs[top] or {"kernel": top, "bound": None})
     roof["traffic"] = dram_traffic(top, args.precision + (":tc" if top == "bin_sums" and bin_method == "tc" else ""),
-                                   N, d.Nlm, Nx)
+                                   N * nsets, d.Nlm, Nx)
     roof["stage_ms"] = stages[top]
 
     # End to end from pinned host buffers: inputs copied in and alm copied out every step.
@@ -881,13 +897,15 @@ def main(argv=None):
             "stages_ms": stages, "plan_build_s": t_plan, "roofline": roof,
             "stages_note": ("one sort (points) for all maps; bin_sums, fold and rotate summed over all maps "
                             "(bin_sums includes the payload gathers), contract over all passes") if maps > 1 else (
-                "stages of one single-transform step (the headline step holds %d point sets)" % batch
-                if batch > 1 else "all stages of one step"),
+                "stages of one headline step (%d point sets: points, bin_sums, fold and rotate for each, one "
+                "contraction pass for all), from the library's stage events in an untimed step after the timed "
+                "ones" % batch if batch > 1 else "all stages of one step"),
             "stage_rooflines": {k: v for k, v in roofs.items() if v}, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(launches), "clocks": clk,
         }
         if batch > 1:
             line["mixed_single_transform"] = {"value": single["value"], "ms_per_step": single["ms_per_step"],
+                                              "stages_ms": single["stages"],
                                               "p50_ms": float(np.percentile(single["per_step"], 50))}
         if other is not None:
             line["fp64_plain"] = {"value": other["value"], "ms_per_step": other["ms_per_step"],

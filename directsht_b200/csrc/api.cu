@@ -703,6 +703,8 @@ int dsht_profile_enable(dsht_plan_t p, int enable) {
 int dsht_profile_read(dsht_plan_t p, double* ms, int64_t* calls, int reset) {
   if (!p) return set_error(DSHT_ERR_INVALID, "plan is NULL");
   std::lock_guard<std::mutex> lock(p->mu);
+  // stage marks of the last asynchronous call (dsht_enqueue_*), once its stream has finished
+  if (p->ev_n > 0) collect_profile(p);
   if (ms)
     for (int i = 0; i < DSHT_STAGE_COUNT; ++i) ms[i] = p->prof_ms[i];
   if (calls) *calls = p->prof_calls;

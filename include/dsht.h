@@ -279,9 +279,10 @@ int dsht_do_transform(int Nl, int Nx, double xmax, double* Yv, double* Yd, int N
  * Stages: 0 points+sort, 1 bin sums, 2 fold, 3 contraction, 4 rotation.  Each stage's time
  * is the sum over all its launches in the call: for multi-map and batch calls stage 0 is
  * every sort, stage 1 every bin-sum launch (with the weight gathers of later maps), stage 2
- * every fold, stage 3 every contraction pass and stage 4 every rotation.  Timed only for
- * the synchronising entry points (dsht_execute*, not dsht_enqueue_*); calls on one plan must
- * not overlap while profiling. */
+ * every fold, stage 3 every contraction pass and stage 4 every rotation.  The synchronising
+ * entry points (dsht_execute*) add their stages when they return; the stages of the last
+ * dsht_enqueue_* call are added by the next dsht_profile_read once the caller has
+ * synchronised that call's stream.  Calls on one plan must not overlap while profiling. */
 enum { DSHT_STAGE_POINTS = 0, DSHT_STAGE_BIN_SUMS = 1, DSHT_STAGE_FOLD = 2, DSHT_STAGE_CONTRACT = 3,
        DSHT_STAGE_ROTATE = 4, DSHT_STAGE_COUNT = 5 };
 int dsht_profile_enable(dsht_plan_t plan, int enable);
