@@ -12,9 +12,8 @@
 // reserves a contiguous range per key and block with one global add, recomputes each
 // point's 32-byte record (cos phi, sin phi, w, t) -- one DRAM sector -- from its inputs and
 // writes it to its sorted slot; the bin-sum kernels form w h_k(t) themselves (the NUFFT bin
-// sums take the record (phi, 0, w, t) instead).  HBM bytes
-// per point: 12-16 read + 4 written (count), 28 read + 32 written (scatter), against the
-// algorithmic 24 read + 32 written.
+// sums take the record (phi, 0, w, t) instead).  HBM bytes per point: 16 read + 4 written
+// (count), 28 read + 32 written (scatter), against the algorithmic 24 read + 32 written.
 #include "dsht_internal.cuh"
 
 namespace dsht {
@@ -86,19 +85,23 @@ __device__ __forceinline__ KeyOut point_key(const Geometry& g, double inv_dx, in
 // FP32 screen of point_key: the same decisions (polar or not, rotated range, sign of x, bin)
 // from FP32 sines and cosines, accepted only when no decision lies within the screen of its
 // boundary; otherwise (and for every point that raises a flag or is NaN) false, and the
-// FP64 path decides.  Bound on the FP32 x: theta, phi rounded to float move cos, sin by at
-// most 1.2e-7 and 2.4e-7 (theta in [0, 3.2], |phi| <= 8; other angles go to FP64); sincosf errs by at most 2 ulp (2.4e-7 here); the product rounds
-// once: |x32 - x| < 9e-7, and the screen is 3e-6.  The bin coordinate u = |x| / dx errs by
-// at most screen / dx plus its own rounding (nbins 2^-24 per operation): bin_guard bounds
-// both.  So an accepted key is the FP64 key.
+// FP64 path decides.  The sines and cosines are the hardware approximations __sincosf,
+// whose absolute error is at most 2^-21.41 (3.6e-7) for arguments in [-pi, pi] (CUDA C
+// Programming Guide, intrinsic functions).  Bound on the FP32 x: theta in [0, 3.14] rounds
+// to float within 1.2e-7, so |sin, cos error| <= 4.8e-7; phi (|phi| <= 8) rounds within
+// 2.4e-7 and is brought into [-pi, pi] by one subtraction of the float 2 pi (1.7e-7 from
+// 2 pi, the difference rounded within 1.2e-7), so its cosine errs by at most 8.9e-7; the
+// product rounds once: |x32 - x| < 1.5e-6, and the screen is 3e-6.  The bin coordinate
+// u = |x| / dx errs by at most screen / dx plus its own rounding (nbins 2^-24 per
+// operation): bin_guard bounds both.  So an accepted key is the FP64 key.
 constexpr float kScreenX = 3e-6f;
 
 __device__ __forceinline__ bool screen_key(const Geometry& g, float inv_dx_f, float bin_guard, float xmax_f, int mode,
-                                           double th, const double* phi_p, uint32_t* key, unsigned* flag) {
-  // the bounds below hold for theta in [0, 3.2] and |phi| <= 8 (float rounding of the angles)
-  if (!(th >= 0.0 && th <= 3.2)) return false;
+                                           double th, double ph, uint32_t* key, unsigned* flag) {
+  // the bounds below hold for theta in [0, 3.14] and |phi| <= 8
+  if (!(th >= 0.0 && th <= 3.14)) return false;
   float sf, cf;
-  sincosf((float)th, &sf, &cf);
+  __sincosf((float)th, &sf, &cf);
   float x;
   int set;
   *flag = 0;
@@ -106,10 +109,13 @@ __device__ __forceinline__ bool screen_key(const Geometry& g, float inv_dx_f, fl
     const float xv = fabsf(cf);
     if (!(fabsf(xv - xmax_f) >= kScreenX)) return false;  // near the polar boundary, or NaN
     if (xv > xmax_f) {
-      const double ph = *phi_p;
       if (!(fabs(ph) <= 8.0)) return false;
+      constexpr float kTwoPiF = 6.28318548f;  // the float nearest 2 pi
+      float pf = (float)ph;
+      if (pf > 3.14f) pf -= kTwoPiF;
+      else if (pf < -3.14f) pf += kTwoPiF;
       float sp, cp;
-      sincosf((float)ph, &sp, &cp);
+      __sincosf(pf, &sp, &cp);
       x = -sf * cp;
       if (!(fabsf(x) <= xmax_f - kScreenX)) return false;  // near or beyond the rotated range
       set = 2;
@@ -135,17 +141,21 @@ __device__ __forceinline__ bool screen_key(const Geometry& g, float inv_dx_f, fl
 }
 
 // Count pass: the key of every point (4 bytes written) and a shared-memory histogram of the
-// keys (one global add per live key and block).  Reads theta, and phi of polar points only.
-// Keys come from the FP32 screen; the points it leaves undecided (~2 % at Nx = 2048) are
-// queued in shared memory and decided by the FP64 path a few rounds later by whole warps,
-// so the FP64 sines and cosines run for those points only.
-constexpr int kQueueRounds = 8;  // rounds of blockDim points between queue flushes
+// keys (one global add per live key and block).  Reads theta and phi (phi for every point in
+// __call__ mode: polar candidates are a third of a survey footprint, so their phi loads
+// touch most sectors anyway, and loading every phi alongside theta keeps the loads
+// independent).  Four points per thread per round, all their loads issued first.  Keys come
+// from the FP32 screen; the points it leaves undecided (~2 % at Nx = 2048) are queued in
+// shared memory and decided by the FP64 path a few rounds later by whole warps, so the FP64
+// sines and cosines run for those points only.
+constexpr int kCountUnroll = 4;
+constexpr int kQueueRounds = 2;  // rounds of kCountUnroll * blockDim points between queue flushes
 
 __global__ void __launch_bounds__(kPointThreads)
 count_kernel(Geometry g, int mode, const double* __restrict__ theta, const double* __restrict__ phi,
              int64_t N, uint32_t* __restrict__ keys, uint32_t* __restrict__ count, unsigned* __restrict__ flags,
              float bin_guard) {
-  extern __shared__ uint32_t hist[];  // [nkeys], then the queue [kQueueRounds * blockDim]
+  extern __shared__ uint32_t hist[];  // [nkeys], then the queue [kQueueRounds * kCountUnroll * blockDim]
   uint32_t* queue = hist + g.nkeys;
   __shared__ int qn;
   for (int k = threadIdx.x; k < g.nkeys; k += blockDim.x) hist[k] = 0;
@@ -154,20 +164,36 @@ count_kernel(Geometry g, int mode, const double* __restrict__ theta, const doubl
   unsigned fl = 0;
   const double inv_dx = 1.0 / g.dx;
   const float inv_dx_f = (float)inv_dx, xmax_f = (float)g.xmax;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t span = (int64_t)kCountUnroll * blockDim.x;
+  const int64_t stride = (int64_t)gridDim.x * span;
+  const bool call = mode == DSHT_MODE_CALL;
   int round = 0;
   // block-uniform trip count: every thread reaches every flush
-  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < N; base += stride) {
-    const int64_t i = base + threadIdx.x;
-    if (i < N) {
-      uint32_t key;
-      unsigned f;
-      if (screen_key(g, inv_dx_f, bin_guard, xmax_f, mode, theta[i], phi + i, &key, &f)) {
-        keys[i] = key;
-        fl |= f;
-        atomicAdd(&hist[key], 1u);
-      } else {
-        queue[atomicAdd(&qn, 1)] = (uint32_t)i;
+  for (int64_t base = (int64_t)blockIdx.x * span; base < N; base += stride) {
+    double th[kCountUnroll], ph[kCountUnroll];
+#pragma unroll
+    for (int u = 0; u < kCountUnroll; ++u) {
+      const int64_t i = base + (int64_t)u * blockDim.x + threadIdx.x;
+      th[u] = 0.0;
+      ph[u] = 0.0;
+      if (i < N) {
+        th[u] = theta[i];
+        if (call) ph[u] = phi[i];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kCountUnroll; ++u) {
+      const int64_t i = base + (int64_t)u * blockDim.x + threadIdx.x;
+      if (i < N) {
+        uint32_t key;
+        unsigned f;
+        if (screen_key(g, inv_dx_f, bin_guard, xmax_f, mode, th[u], ph[u], &key, &f)) {
+          keys[i] = key;
+          fl |= f;
+          atomicAdd(&hist[key], 1u);
+        } else {
+          queue[atomicAdd(&qn, 1)] = (uint32_t)i;
+        }
       }
     }
     if (++round == kQueueRounds || base + stride >= N) {
@@ -176,10 +202,10 @@ count_kernel(Geometry g, int mode, const double* __restrict__ theta, const doubl
       const int nq = qn;
       for (int q = threadIdx.x; q < nq; q += blockDim.x) {
         const int64_t k = queue[q];
-        const double th = theta[k];
+        const double t = theta[k];
         double st, c;
-        sincos(th, &st, &c);
-        const KeyOut o = point_key(g, inv_dx, mode, th, st, c, phi + k);
+        sincos(t, &st, &c);
+        const KeyOut o = point_key(g, inv_dx, mode, t, st, c, phi + k);
         keys[k] = o.key;
         fl |= o.flag;
         if (o.key != DSHT_KEY_DROP) atomicAdd(&hist[o.key], 1u);
@@ -306,19 +332,19 @@ scatter_kernel(Geometry g, const double* __restrict__ theta, const double* __res
       if (k[u] != DSHT_KEY_DROP) atomicAdd(&loc[k[u]], 1u);
   }
   __syncthreads();
-  // one global reservation per (block, key); four of a thread's in flight at once
-  for (int k0 = threadIdx.x; k0 < g.nkeys; k0 += 4 * blockDim.x) {
-    uint32_t c[4], r[4];
+  // one global reservation per (block, key); eight of a thread's in flight at once
+  for (int k0 = threadIdx.x; k0 < g.nkeys; k0 += 8 * blockDim.x) {
+    uint32_t c[8], r[8];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
+    for (int u = 0; u < 8; ++u) {
       const int k = k0 + u * blockDim.x;
       c[u] = k < g.nkeys ? loc[k] : 0u;
     }
 #pragma unroll
-    for (int u = 0; u < 4; ++u)
+    for (int u = 0; u < 8; ++u)
       if (c[u]) r[u] = atomicAdd(&cursor[k0 + u * blockDim.x], c[u]);
 #pragma unroll
-    for (int u = 0; u < 4; ++u)
+    for (int u = 0; u < 8; ++u)
       if (c[u]) loc[k0 + u * blockDim.x] = r[u];
   }
   __syncthreads();
@@ -373,7 +399,8 @@ scatter_kernel(Geometry g, const double* __restrict__ theta, const double* __res
           }
         }
       }
-      const int j = (int)(k[u] % (uint32_t)g.nbins);
+      const int kk = (int)k[u];  // bin j = key - set nbins, without an integer division
+      const int j = kk - g.nbins * ((kk >= g.nbins) + (kk >= 2 * g.nbins) + (kk >= 3 * g.nbins));
       // t = (|x| - x_j) / dx in the reference's rounding (sht/sht.py:221); the NUFFT route
       // (mixed levels) takes the product with 1/dx, within an ulp of it
       const double t = PHI ? (fabs(x) - (double)j * g.dx) * inv_dx
@@ -462,10 +489,10 @@ void launch_points(const Geometry& g, const double* theta, const double* phi, co
   cudaMemsetAsync(ws.count, 0, sizeof(uint32_t) * (g.nkeys + 1), s);
   cudaMemsetAsync(ws.flags, 0, sizeof(unsigned), s);
   const size_t hsmem = sizeof(uint32_t) * g.nkeys;
-  const size_t csmem = hsmem + sizeof(uint32_t) * kQueueRounds * kPointThreads;
+  const size_t csmem = hsmem + sizeof(uint32_t) * kQueueRounds * kCountUnroll * kPointThreads;
   cudaFuncSetAttribute(count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csmem);
   if (N > 0) {
-    int64_t blocks = (N + kPointThreads * 8 - 1) / (kPointThreads * 8);
+    int64_t blocks = (N + kPointThreads * 2 * kCountUnroll - 1) / (kPointThreads * 2 * kCountUnroll);
     if (blocks > 148 * 4) blocks = 148 * 4;  // fewer, longer blocks: fewer per-block key flushes
     // fraction-of-bin guard of the FP32 screen: the x bound over dx, plus the rounding of
     // u = |x| / dx (four roundings of a value below nbins)
