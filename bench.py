@@ -34,6 +34,9 @@ WORKLOADS = {
     # Smaller tables for Nsight Compute captures of the same kernels (inputs still exceed L2).
     "c2prof": dict(Nl=1024, Nx=256, N=4_000_000, kind="c2", wkind="lognormal",
                    name="profiling case: Nl=1024, Nx=256, N=4e6, C2 point distribution"),
+    # The sort at the full size (Nx=2048: 8188 bin keys, N=1e7) with small tables (Nl=64).
+    "c2sort": dict(Nl=64, Nx=2048, N=10_000_000, kind="c2", wkind="lognormal",
+                   name="sort profiling case: Nl=64, Nx=2048, N=1e7, C2 point distribution"),
     "c1": dict(Nl=256, Nx=512, N=100_000, kind="full", wkind="ones",
                name="full sky: Nl=256, Nx=512, N=1e5, cos(theta)~U[-1,1], phi~U[0,2pi), w=1 f64"),
     "c3": dict(Nl=1024, Nx=2048, N=2_000_000, kind="full", wkind="normal", maps=64,

@@ -351,7 +351,7 @@ scatter_kernel(Geometry g, const double* __restrict__ theta, const double* __res
   const int polar_key0 = 2 * g.nbins;
   const double inv_dx = 1.0 / g.dx;
   for (int64_t b = lo + threadIdx.x; b < hi; b += step) {
-    uint32_t k[kUnroll];
+    uint32_t k[kUnroll], pos[kUnroll];
     double th[kUnroll], ph[kUnroll], wi[kUnroll];
 #pragma unroll
     for (int u = 0; u < kUnroll; ++u) {
@@ -364,6 +364,10 @@ scatter_kernel(Geometry g, const double* __restrict__ theta, const double* __res
         wi[u] = (double)w[i];
       }
     }
+    // the slots first: their shared-memory round trips overlap the record arithmetic
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u)
+      if (k[u] != DSHT_KEY_DROP) pos[u] = atomicAdd(&loc[k[u]], 1u);
 #pragma unroll
     for (int u = 0; u < kUnroll; ++u) {
       if (k[u] == DSHT_KEY_DROP) continue;
@@ -405,11 +409,10 @@ scatter_kernel(Geometry g, const double* __restrict__ theta, const double* __res
       // (mixed levels) takes the product with 1/dx, within an ulp of it
       const double t = PHI ? (fabs(x) - (double)j * g.dx) * inv_dx
                            : __ddiv_rn(__dadd_rn(fabs(x), -(double)j * g.dx), g.dx);
-      const uint32_t pos = atomicAdd(&loc[k[u]], 1u);
-      double2* out = reinterpret_cast<double2*>(pay + (size_t)kRec * pos);  // one 32-byte sector
+      double2* out = reinterpret_cast<double2*>(pay + (size_t)kRec * pos[u]);  // one 32-byte sector
       out[0] = make_double2(cphi, sphi);
       out[1] = make_double2(wi[u], t);
-      if (sidx) sidx[pos] = (uint32_t)(b + (int64_t)u * blockDim.x);
+      if (sidx) sidx[pos[u]] = (uint32_t)(b + (int64_t)u * blockDim.x);
     }
   }
 }
