@@ -757,11 +757,16 @@ def main(argv=None):
                     "unit": "TFLOP/s", "frac": a / 40.0, "peak_source": "nominal (no measured FP64 figure)",
                     "algorithmic": "24 flop per (point, m, map): 8 FMA sums + 4 FMA angle step"}
         if name == "rotate":
-            alg = 2.0 * 5 * sum((l + 1) ** 2 for l in range(Nl)) * maps * nsets
+            # the products themselves: a real Wigner element d^l_{m m'} (m, m' >= 0, the m' < 0
+            # terms folded in by the symmetry of d(pi/2)) times a complex coefficient, 2 FMA per
+            # map; the recursion that forms d (shared by the maps of a launch) is not counted
+            alg = 2.0 * 2 * sum((l + 1) ** 2 for l in range(Nl)) * maps * nsets
             a = alg / (ms * 1e-3) / 1e12
-            return {"kernel": "rotate_back_kernel", "bound": "fp64", "achieved": a, "peak": 40.0,
+            return {"kernel": "rotate_back_kernel" if maps * nsets == 1 else "rotate_back_maps_kernel",
+                    "bound": "fp64", "achieved": a, "peak": 40.0,
                     "unit": "TFLOP/s", "frac": a / 40.0, "peak_source": "nominal (no measured FP64 figure)",
-                    "algorithmic": "5 FMA per (l, m, m', map) of the Wigner-d recursion and product"}
+                    "algorithmic": "2 FMA per (l, m >= 0, m' >= 0, map): real d^l_{mm'}(pi/2) times a complex "
+                                   "coefficient (the recursion forming d is not counted)"}
         return None
 
     roofs = {n: stage_roof(n, ms) for n, ms in stages.items()}
