@@ -174,6 +174,21 @@ void launch_rotate_back(const Geometry& g, const double* alm_rot, const double* 
 // alm io[k] += R(rot[k]) for k < nmaps <= kMaxRot (a map without polar points is left as it is).
 void launch_rotate_back_maps(const Geometry& g, const RotMaps& maps, int nmaps, cudaStream_t s);
 
+// Hint: bring [p, p + bytes) into L2 (cp.async.bulk.prefetch.L2, 16-byte aligned chunks of at
+// most 32 KB; the unaligned ends are left out).  lane, nlanes: the calling threads share the
+// chunks.  A prefetch only warms the cache: it reads nothing into registers and cannot fault
+// on the addresses of a live buffer.
+__device__ __forceinline__ void prefetch_l2(const void* p, size_t bytes, int lane, int nlanes) {
+  const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+  const uintptr_t a0 = (a + 15) & ~uintptr_t(15);
+  if (bytes <= a0 - a) return;
+  const size_t n = (bytes - (a0 - a)) & ~size_t(15);
+  for (size_t off = (size_t)lane * 32768; off < n; off += (size_t)nlanes * 32768) {
+    const size_t sz = n - off < 32768 ? n - off : 32768;
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a0 + off), "r"((unsigned)sz) : "memory");
+  }
+}
+
 // Hermite weights w * {(2t+1)(1-t)^2, t(1-t)^2, t^2(3-2t), t^2(t-1)} of one point, in the
 // rounding order of sht/sht.py:239-240.
 __device__ __forceinline__ void hermite(double t, double wi, double* out4) {

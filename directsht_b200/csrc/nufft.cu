@@ -259,15 +259,10 @@ nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* _
     const int64_t start = piece_start[piece];
     const int len = piece_len[piece];
     const double* rec0 = pay + (size_t)kRec * start;
-    // The next piece's records into L2 while this one is summed (warp 0, 32 KB per lane).
+    // The next piece's records into L2 while this one is summed (warp 0).
     if (warp == 0 && piece + (int)gridDim.x < npieces) {
       const int nxt = piece + (int)gridDim.x;
-      const size_t bytes = sizeof(double) * kRec * (size_t)piece_len[nxt];
-      const char* src = reinterpret_cast<const char*>(pay + (size_t)kRec * piece_start[nxt]);
-      for (size_t off = (size_t)lane * 32768; off < bytes; off += (size_t)32 * 32768) {
-        const size_t sz = bytes - off < 32768 ? bytes - off : 32768;
-        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src + off), "r"((unsigned)sz) : "memory");
-      }
+      prefetch_l2(pay + (size_t)kRec * piece_start[nxt], sizeof(double) * kRec * (size_t)piece_len[nxt], lane, 32);
     }
     // sum |w| of the piece (one pass, four loads in flight) with a margin for its own rounding,
     // and max |w| (only to detect non-finite weights).  The bound 2^e above it bounds every

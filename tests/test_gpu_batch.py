@@ -95,6 +95,40 @@ def test_enqueue_batch_status_words():
                                      ct.c_void_p(s)) == L.DSHT_ERR_INVALID
 
 
+def test_stage_times_of_an_enqueued_batch():
+    """dsht_profile_read adds the stage events of the last dsht_enqueue_batch call once its
+    stream has finished: every stage of a mixed batch with polar points is timed, once."""
+    d = DirectSHT(64, 128, precision="mixed")
+    sets = _sets(6, [40000, 30000, 50000])
+    dev = [tuple(torch.tensor(a, device="cuda") for a in s) for s in sets]
+    alms = [torch.empty(d.Nlm, dtype=torch.complex128, device="cuda") for _ in sets]
+    n = len(sets)
+    arr = lambda xs: (ct.c_void_p * n)(*[x.data_ptr() for x in xs])
+    Ns = (ct.c_int64 * n)(*[len(s[0]) for s in sets])
+    nb = ct.c_size_t()
+    L.check(d._lib.dsht_workspace_size_batch(d._plan, 50000, n, ct.byref(nb)))
+    ws = torch.empty(nb.value, dtype=torch.uint8, device="cuda")
+    s = ct.c_void_p(torch.cuda.current_stream().cuda_stream)
+    ms = (ct.c_double * 5)()
+    calls = ct.c_int64()
+    L.check(d._lib.dsht_profile_enable(d._plan, 1))
+    L.check(d._lib.dsht_profile_read(d._plan, ms, ct.byref(calls), 1))
+    L.check(d._lib.dsht_enqueue_batch(d._plan, n, arr([x[0] for x in dev]), arr([x[1] for x in dev]),
+                                      arr([x[2] for x in dev]), Ns, L.DSHT_MODE_CALL, arr(alms), None,
+                                      L.ptr(ws), ws.numel(), s))
+    torch.cuda.synchronize()
+    L.check(d._lib.dsht_profile_read(d._plan, ms, ct.byref(calls), 1))
+    L.check(d._lib.dsht_profile_enable(d._plan, 0))
+    assert calls.value == 1
+    assert all(v > 0.0 for v in ms), list(ms)
+    # read again: nothing new was enqueued, nothing is added twice
+    L.check(d._lib.dsht_profile_read(d._plan, ms, ct.byref(calls), 0))
+    assert calls.value == 0 and all(v == 0.0 for v in ms)
+    for (th, ph, w), a in zip(sets, alms):
+        ref = O.direct_sht(O.build_tables(64, 128), th, ph, w)
+        assert _rel(a.cpu().numpy(), ref) <= 1e-7
+
+
 def test_enqueue_batch_in_cuda_graph():
     """The enqueued batch captures into a CUDA graph; replays give the eager results."""
     Nl, Nx = 48, 96
