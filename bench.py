@@ -509,7 +509,7 @@ def main(argv=None):
                          "library's choice by points per bin key (default)")
     ap.add_argument("--maps-per-pass", type=int, default=0, help="DSHT_TUNE_MAPS_PER_PASS (0: automatic)")
     ap.add_argument("--batch", type=int, default=None,
-                    help="point sets per step for the headline (dsht_enqueue_batch); default 4 for c2, else 1")
+                    help="point sets per step for the headline (dsht_enqueue_batch); default 8 for c2, else 1")
     args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3)
     spec = WORKLOADS[args.workload]
@@ -605,7 +605,9 @@ def main(argv=None):
     # FP64 direct sums below 28 and the tensor-core sums in between (DSHT_TUNE_BIN_SUMS)
     bin_method = args.bin_sums if args.bin_sums != "auto" else (
         "nufft" if N >= 512 * 4 * (Nx - 1) else "fp64" if N < 28 * 4 * (Nx - 1) else "tc")
-    batch = args.batch if args.batch is not None else (4 if args.workload == "c2" else 1)
+    # eight point sets per headline step: one contraction pass holds up to eight (32 fold
+    # columns), so the table read is shared by all of them
+    batch = args.batch if args.batch is not None else (8 if args.workload == "c2" else 1)
     if maps > 1 or w_dtype != L.DSHT_W_F64:
         batch = 1
     single = timed(args.precision, sample_clocks=batch == 1)

@@ -335,10 +335,13 @@ static void rotate_maps_launch(const Geometry& g, const RotMaps& maps, int nmaps
 
 void launch_rotate_back_maps(const Geometry& g, const RotMaps& maps, int nmaps, cudaStream_t s) {
   if (nmaps <= 0) return;
-  // As many maps per CTA (8, 4, 2, 1) as the shared-memory limit allows for this Nl.
+  // As many maps per CTA (8, 4, 2, 1) as the shared-memory limit allows for this Nl; eight
+  // only while two such CTAs still fit an SM (at Nl=1024 one 8-map CTA per SM took 0.131 ms
+  // per map, two 4-map CTAs per SM 0.107: the recurrence is latency-bound, so residency wins
+  // over sharing it between more maps).
   auto bytes = [&](int k) { return (size_t)g.Nl * ((5 + 2 * k) * sizeof(double) + sizeof(int)) + 64; };
   const size_t lim = 227 * 1024;
-  if (nmaps > 4 && bytes(8) <= lim)
+  if (nmaps > 4 && 2 * (bytes(8) + 1024) <= 228 * 1024)
     rotate_maps_launch<8>(g, maps, nmaps, bytes(8), s);
   else if (nmaps > 2 && bytes(4) <= lim)
     rotate_maps_launch<4>(g, maps, nmaps, bytes(4), s);
