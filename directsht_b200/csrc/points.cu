@@ -88,10 +88,11 @@ __device__ __forceinline__ KeyOut point_key(const Geometry& g, double inv_dx, in
 // FP64 path decides.  The sines and cosines are the hardware approximations __sincosf,
 // whose absolute error is at most 2^-21.41 (3.6e-7) for arguments in [-pi, pi] (CUDA C
 // Programming Guide, intrinsic functions).  Bound on the FP32 x: theta in [0, 3.14] rounds
-// to float within 1.2e-7, so |sin, cos error| <= 4.8e-7; phi (|phi| <= 8) rounds within
-// 2.4e-7 and is brought into [-pi, pi] by one subtraction of the float 2 pi (1.7e-7 from
-// 2 pi, the difference rounded within 1.2e-7), so its cosine errs by at most 8.9e-7; the
-// product rounds once: |x32 - x| < 1.5e-6, and the screen is 3e-6.  The bin coordinate
+// to float within 1.2e-7 (and stays below pi), so |sin, cos error| <= 4.8e-7; phi (|phi| <=
+// 8) rounds within 2.4e-7 and is brought into [-pi, pi] by one exact (Sterbenz) subtraction
+// of the float 2 pi (1.75e-7 from 2 pi) and a clamp to the largest float below pi (at most
+// 2.6e-7), so its cosine errs by at most 1.03e-6; the product rounds once: |x32 - x| <
+// 1.6e-6, and the screen is 3e-6.  The bin coordinate
 // u = |x| / dx errs by at most screen / dx plus its own rounding (nbins 2^-24 per
 // operation): bin_guard bounds both.  So an accepted key is the FP64 key.
 constexpr float kScreenX = 3e-6f;
@@ -111,9 +112,11 @@ __device__ __forceinline__ bool screen_key(const Geometry& g, float inv_dx_f, fl
     if (xv > xmax_f) {
       if (!(fabs(ph) <= 8.0)) return false;
       constexpr float kTwoPiF = 6.28318548f;  // the float nearest 2 pi
+      constexpr float kPiBelow = 3.14159250f;  // the largest float below pi
       float pf = (float)ph;
-      if (pf > 3.14f) pf -= kTwoPiF;
-      else if (pf < -3.14f) pf += kTwoPiF;
+      if (pf > kPiBelow) pf -= kTwoPiF;
+      else if (pf < -kPiBelow) pf += kTwoPiF;
+      pf = fminf(fmaxf(pf, -kPiBelow), kPiBelow);
       float sp, cp;
       __sincosf(pf, &sp, &cp);
       x = -sf * cp;
