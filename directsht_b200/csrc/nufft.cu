@@ -255,40 +255,47 @@ nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* _
   __syncthreads();
   const double u_per_rad = (double)n * 0.15915494309189533577;  // n / (2 pi)
   const int npieces = (int)min((int64_t)*npieces_p, pmax);
+  // sum |w| of a piece with a margin for its own rounding, and max |w| (only to detect
+  // non-finite weights).  The bound 2^e above it bounds every grid value (|h_k| <= 1,
+  // psi <= 1), so the spread runs in fixed point of step 2^(e - 46) with integer reductions:
+  // the grid does not depend on the order of the adds.  The sum itself is summed in whatever
+  // order the sort left the points; e can only differ between runs when the sum lies within
+  // its rounding (~len 2^-53 relative) of a power of two.  This thread's share of a piece,
+  // from its point pfrom on, four loads in flight:
+  auto bound_part = [&](const double* r0, int l, int pfrom, double& wa, unsigned long long& mb) {
+    const int bd = blockDim.x;
+    int p = pfrom;
+    for (; p + 3 * bd < l; p += 4 * bd) {
+      const double a0 = fabs(r0[(size_t)kRec * p + 2]), a1 = fabs(r0[(size_t)kRec * (p + bd) + 2]);
+      const double a2 = fabs(r0[(size_t)kRec * (p + 2 * bd) + 2]), a3 = fabs(r0[(size_t)kRec * (p + 3 * bd) + 2]);
+      wa += (a0 + a1) + (a2 + a3);
+      mb = max(max(mb, (unsigned long long)__double_as_longlong(a0)),
+               max((unsigned long long)__double_as_longlong(a1),
+                   max((unsigned long long)__double_as_longlong(a2), (unsigned long long)__double_as_longlong(a3))));
+    }
+    for (; p < l; p += bd) {
+      const double a = fabs(r0[(size_t)kRec * p + 2]);
+      wa += a;
+      mb = max(mb, (unsigned long long)__double_as_longlong(a));
+    }
+  };
+  // The shares of the CTA's first piece here; those of every later piece while the piece
+  // before it is summed (the first four loads are issued before that piece's extraction
+  // phase and summed after it).
+  double wabs_n = 0.0;
+  unsigned long long mbits_n = 0ull;
+  if ((int)blockIdx.x < npieces)
+    bound_part(pay + (size_t)kRec * piece_start[blockIdx.x], piece_len[blockIdx.x], threadIdx.x, wabs_n, mbits_n);
   for (int piece = blockIdx.x; piece < npieces; piece += gridDim.x) {
     const int64_t start = piece_start[piece];
     const int len = piece_len[piece];
     const double* rec0 = pay + (size_t)kRec * start;
+    const int nxt = piece + (int)gridDim.x;
     // The next piece's records into L2 while this one is summed (warp 0).
-    if (warp == 0 && piece + (int)gridDim.x < npieces) {
-      const int nxt = piece + (int)gridDim.x;
+    if (warp == 0 && nxt < npieces)
       prefetch_l2(pay + (size_t)kRec * piece_start[nxt], sizeof(double) * kRec * (size_t)piece_len[nxt], lane, 32);
-    }
-    // sum |w| of the piece (one pass, four loads in flight) with a margin for its own rounding,
-    // and max |w| (only to detect non-finite weights).  The bound 2^e above it bounds every
-    // grid value (|h_k| <= 1, psi <= 1), so the spread runs in fixed point of step 2^(e - 46)
-    // with integer reductions: the grid does not depend on the order of the adds.  The sum
-    // itself is summed in whatever order the sort left the points; e can only differ between
-    // runs when the sum lies within its rounding (~len 2^-53 relative) of a power of two.
-    unsigned long long mbits = 0ull;
-    double wabs = 0.0;
-    {
-      const int bd = blockDim.x;
-      int p = threadIdx.x;
-      for (; p + 3 * bd < len; p += 4 * bd) {
-        const double a0 = fabs(rec0[(size_t)kRec * p + 2]), a1 = fabs(rec0[(size_t)kRec * (p + bd) + 2]);
-        const double a2 = fabs(rec0[(size_t)kRec * (p + 2 * bd) + 2]), a3 = fabs(rec0[(size_t)kRec * (p + 3 * bd) + 2]);
-        wabs += (a0 + a1) + (a2 + a3);
-        mbits = max(max(mbits, (unsigned long long)__double_as_longlong(a0)),
-                    max((unsigned long long)__double_as_longlong(a1),
-                        max((unsigned long long)__double_as_longlong(a2), (unsigned long long)__double_as_longlong(a3))));
-      }
-      for (; p < len; p += bd) {
-        const double a = fabs(rec0[(size_t)kRec * p + 2]);
-        wabs += a;
-        mbits = max(mbits, (unsigned long long)__double_as_longlong(a));
-      }
-    }
+    unsigned long long mbits = mbits_n;
+    double wabs = wabs_n;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       mbits = max(mbits, __shfl_xor_sync(0xffffffffu, mbits, o));
@@ -417,6 +424,20 @@ nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* _
         __syncthreads();
       }
       fft_all<NSEQ>(zs, seq_stride, logn, tws);
+      // the next piece's first four weights per thread, in flight during the extraction
+      const bool last_pass = kp + KP >= 4;
+      const double* nrec = nullptr;
+      int nlen = 0;
+      double nq[4] = {0.0, 0.0, 0.0, 0.0};
+      if (last_pass && nxt < npieces) {
+        nrec = pay + (size_t)kRec * piece_start[nxt];
+        nlen = piece_len[nxt];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int p = threadIdx.x + u * (int)blockDim.x;
+          if (p < nlen) nq[u] = fabs(nrec[(size_t)kRec * p + 2]);
+        }
+      }
       // v_k0 = (Z[m] + conj Z[-m]) / 2, v_k1 = (Z[m] - conj Z[-m]) / 2i, each over Psi(m)
       for (int m = threadIdx.x; m < Nl; m += blockDim.x) {
         const int pm = padi(fft_pos(m, logn)), pn = padi(fft_pos((n - m) & (n - 1), logn));
@@ -433,6 +454,12 @@ nufft_sums_kernel(int Nl, int logn, const double* __restrict__ pay, const int* _
         }
       }
       __syncthreads();
+      if (last_pass) {
+        wabs_n = (nq[0] + nq[1]) + (nq[2] + nq[3]);
+        mbits_n = max(max((unsigned long long)__double_as_longlong(nq[0]), (unsigned long long)__double_as_longlong(nq[1])),
+                      max((unsigned long long)__double_as_longlong(nq[2]), (unsigned long long)__double_as_longlong(nq[3])));
+        if (nrec) bound_part(nrec, nlen, threadIdx.x + 4 * (int)blockDim.x, wabs_n, mbits_n);
+      }
     }
   }
 }
