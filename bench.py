@@ -735,6 +735,10 @@ def main(argv=None):
                     "peak_source": "nominal (no measured FP64 figure)",
                     "algorithmic": f"400 flop per point + 10 n log2 n per piece ({pieces} pieces, n = {1 << logn}) "
                                    f"x {nsets} point sets",
+                    "bound_note": "the kernel's own limit is its shared-memory pipe (96 32-bit reductions per "
+                                  "point for the spread, the in-place FFT): L1/TEX throughput 79 % of peak in the "
+                                  "ncu capture summarised in profiles/nufft_sums_c2prof.md; no FP64 peak is "
+                                  "measured here, so the fp64 fraction uses the nominal 40 TFLOP/s",
                     "equivalent_direct": {"value": 24.0 * N * Nl * maps * nsets / (ms * 1e-3) / 1e12,
                                           "unit": "TFLOP/s",
                                           "what": "24 flop per (point, m, map) of the direct sums over the "
